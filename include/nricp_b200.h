@@ -1,0 +1,238 @@
+/*
+ * nricp_b200 -- C-ABI of the B200-native non-rigid ICP wrapping path.
+ *
+ * The reference ships its solve routes only as the pybind11 module `nricp_dp`
+ * (src/python/bindings.cpp:714); it has no C ABI.  Every entry point below is
+ * what that module's route B / route C surface binds, flattened to plain
+ * pointers and sizes so that a cgo / JNI / ctypes / pybind11 caller can bind it
+ * directly.  Each declaration names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every function returns an int status (NRICP_OK on success).  The message
+ *     of the last failure on the calling thread is nricp_last_error().
+ *   - Outputs are caller-allocated.  Sizes are known up front from
+ *     nricp_plan() (node counts per level) and the input sizes.
+ *   - Points are double precision, row-major (n, 3); faces are int32 (m, 3).
+ *   - Distances (distance_threshold, robust_threshold) are in the caller's
+ *     units, exactly as the reference's route functions take them
+ *     (src/python/bindings.cpp:631-639).
+ */
+#ifndef NRICP_B200_H
+#define NRICP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  INVALID maps to the reference's py::value_error /
+ * std::invalid_argument (ValueError), CUDA and DEVICE to std::runtime_error
+ * (RuntimeError), see src/cuda/cuda_error.h:14-19 and
+ * src/python/bindings.cpp:557-570. */
+enum {
+    NRICP_OK = 0,
+    NRICP_ERR_INVALID = 1,   /* caller error: shapes, indices, settings */
+    NRICP_ERR_CUDA = 2,      /* a CUDA call failed */
+    NRICP_ERR_NO_DEVICE = 3, /* no usable sm_100 device */
+    NRICP_ERR_CAPACITY = 4,  /* output buffer too small / budget exceeded */
+    NRICP_ERR_STATE = 5,     /* call not valid in the object's current state */
+    NRICP_ERR_TIMEOUT = 6    /* a bounded device wait gave up */
+};
+
+/* Maximum binding support per vertex.  The reference hard-codes 4
+ * (src/core/sampling.h:17); the BASELINE configs ask for 6 and 8. */
+#define NRICP_MAX_SLOTS 8
+
+/* Robust kernels, src/energy/robust.h:9-13. */
+enum { NRICP_ROBUST_NONE = 0, NRICP_ROBUST_HUBER = 1, NRICP_ROBUST_GEMAN_MCCLURE = 2 };
+
+/* Device routes, src/cuda/gpu_solver.cuh:19-26. */
+enum { NRICP_ROUTE_B = 0, NRICP_ROUTE_C = 1 };
+
+/* One level of the coarse-to-fine schedule: LevelSettings,
+ * src/solver/route_a.h:17-25, parsed from the level dict at
+ * src/python/bindings.cpp:181-196 (same defaults). */
+typedef struct NricpLevelSettings {
+    double point_to_point;   /* 1.0 */
+    double point_to_plane;   /* 1.0 */
+    double smoothness;       /* 1.0 */
+    double anchor;           /* 0.0 */
+    double landmark;         /* 1.0 */
+    int robust_kernel;       /* NRICP_ROBUST_HUBER */
+    double robust_threshold; /* 0.0 (caller units; 0 disables reweighting) */
+    int max_outer_iterations;  /* 10 */
+    int max_inner_iterations;  /* 10 */
+    double outer_tolerance;    /* 1e-3 */
+    double inner_tolerance;    /* 1e-4 */
+} NricpLevelSettings;
+
+/* Everything one wrap needs: the arguments of solve_route_b/solve_route_c
+ * (src/python/bindings.cpp:1426-1481), same meaning and defaults, plus the
+ * extensions the BASELINE configs need (k > 4 bindings, k-NN edges). */
+typedef struct NricpSolveDesc {
+    const double* template_points; /* (template_vertex_count, 3) */
+    int template_vertex_count;
+    const int32_t* template_faces; /* (template_face_count, 3) */
+    int template_face_count;
+    const double* target_points;   /* (target_vertex_count, 3) */
+    int target_vertex_count;
+    const int32_t* target_faces;   /* (target_face_count, 3) */
+    int target_face_count;
+    const NricpLevelSettings* levels; /* one per level; last reused */
+    int level_setting_count;
+    const uint8_t* mask;            /* (template_vertex_count,) or NULL */
+    const int32_t* landmark_indices; /* (landmark_count,) or NULL */
+    const double* landmark_targets;  /* (landmark_count, 3) or NULL */
+    int landmark_count;
+    double distance_threshold;  /* +inf */
+    double min_normal_cosine;   /* -1 */
+    double min_slope;           /* 0 */
+    double initial_damping;     /* 1e-3 */
+    double damping_decrease;    /* 0.3 */
+    double damping_increase;    /* 4 */
+    int max_damping_attempts;   /* 6 */
+    int diagonal_damping;       /* 1 */
+    int graph_levels;           /* 4 */
+    int nodes_initial;          /* 100 */
+    int growth;                 /* 2 */
+    double pcg_tolerance;       /* 1e-5 */
+    int pcg_max_iterations;     /* 60 */
+    /* extensions (0 selects the reference default of 4 for both) */
+    int max_nodes_per_vertex;   /* binding support k, <= NRICP_MAX_SLOTS */
+    int edge_neighbours;        /* k-NN graph edges */
+    int route;                  /* NRICP_ROUTE_B or NRICP_ROUTE_C */
+} NricpSolveDesc;
+
+/* Fills `desc` with the reference's defaults; pointers and counts zeroed. */
+void nricp_default_desc(NricpSolveDesc* desc);
+void nricp_default_level(NricpLevelSettings* level);
+
+/* The result dict of route_result_to_dict (src/python/bindings.cpp:674-710),
+ * caller-allocated.  Sizes: vertices template_vertex_count*3; rotations,
+ * translations and node_positions use the finest level's node count from
+ * nricp_plan(); level_nodes holds one entry per level.  report_json receives
+ * the run report (src/core/report.cpp:46-105 format), NUL-terminated;
+ * report_length is set to the full length even when it was truncated. */
+typedef struct NricpResult {
+    double* vertices;
+    double* rotations;
+    double* translations;
+    double* node_positions;
+    int32_t* level_nodes;
+    char* report_json;
+    size_t report_capacity;
+    size_t report_length;
+} NricpResult;
+
+/* Per-step progress, WrapProgress (src/cuda/gpu_solver.cuh:60-68). */
+typedef struct NricpProgress {
+    int level;
+    int outer;
+    int inner;
+    int finished;
+    int level_converged;
+    double energy;
+    double correspondence_mean;
+} NricpProgress;
+
+/* ---- identity and devices --------------------------------------------- */
+
+/* Message of the last failing call on this thread (the text the reference
+ * raises as ValueError / RuntimeError). */
+const char* nricp_last_error(void);
+
+/* device_info(), src/python/bindings.cpp:1614-1622. */
+int nricp_device_info(int* available, char* description, size_t capacity);
+
+/* Node count per level for a descriptor (src/core/graph.cpp:52-57): sizes the
+ * caller's result buffers.  `level_count` receives the number of levels. */
+int nricp_plan(const NricpSolveDesc* desc, int32_t* level_nodes, int capacity,
+               int* level_count);
+
+/* ---- the route functions ------------------------------------------------ */
+
+/* solve_route_b / solve_route_c (src/python/bindings.cpp:1422-1492 ->
+ * src/cuda/gpu_solver.cu:14-39): one wrap, start to finish, on the current
+ * device.  desc->route selects the route. */
+int nricp_solve(const NricpSolveDesc* desc, NricpResult* out);
+
+/* ---- the session (RouteBSession, bindings.cpp:1510-1612) ---------------- */
+
+typedef struct NricpSession NricpSession;
+
+/* RouteBSession(...) constructor (bindings.cpp:1513-1561): validates,
+ * prepares the template graph, uploads, builds the target hierarchy. */
+int nricp_session_create(const NricpSolveDesc* desc, NricpSession** out);
+/* .step() (bindings.cpp:1562-1580): advances the schedule by one unit of
+ * work -- a correspondence refresh or one damped solve attempt. */
+int nricp_session_step(NricpSession* session, NricpProgress* progress);
+/* Steps until finished, without host round trips between steps. */
+int nricp_session_run(NricpSession* session);
+/* .finished() (bindings.cpp:1581-1582). */
+int nricp_session_finished(NricpSession* session, int* finished);
+/* .vertices() (bindings.cpp:1583-1592): the current fit, caller units,
+ * template_vertex_count x 3. */
+int nricp_session_vertices(NricpSession* session, double* out);
+/* .result() (bindings.cpp:1600-1611): the solve_route_b payload for the state
+ * reached so far; .report() is result->report_json. */
+int nricp_session_result(NricpSession* session, NricpResult* out);
+/* Schedule ticks run and kernels launched so far. */
+int nricp_session_ticks(NricpSession* session, long* ticks, long* launches);
+void nricp_session_destroy(NricpSession* session);
+
+/* ---- batches: many uneven wraps advanced by the same launches ----------- */
+
+typedef struct NricpBatch NricpBatch;
+
+/* No reference counterpart (the reference solves one wrap per call,
+ * src/cuda/gpu_solver.cu:14-39): prepares and uploads `count` wraps. */
+int nricp_batch_create(const NricpSolveDesc* descs, int count, NricpBatch** out);
+/* Puts every wrap back at the start of its schedule, inputs kept resident. */
+int nricp_batch_reset(NricpBatch* batch);
+/* Runs every wrap to completion in one stream of shared launches. */
+int nricp_batch_run(NricpBatch* batch);
+int nricp_batch_result(NricpBatch* batch, int index, NricpResult* out);
+int nricp_batch_counters(NricpBatch* batch, long* ticks, long* launches);
+/* Re-runs the batch with CUDA events around the closest-point query, the
+ * linear solve and the assembly of every tick; totals in milliseconds. */
+int nricp_batch_profile(NricpBatch* batch, double* query_ms, double* pcg_ms,
+                        double* assemble_ms, long* ticks);
+void nricp_batch_destroy(NricpBatch* batch);
+/* One call: create, run, results, destroy. */
+int nricp_batch_solve(const NricpSolveDesc* descs, int count, NricpResult* results);
+
+/* ---- components ---------------------------------------------------------- */
+
+/* build_template_graph(...) (bindings.cpp:886-925), one level: the
+ * normalisation, the sampled nodes, the bindings (stride NRICP_MAX_SLOTS) and
+ * the k-NN edges of `level`. */
+int nricp_template_graph_level(const double* points, int count, int levels,
+                               int nodes_initial, int growth, int max_nodes,
+                               int edge_neighbours, int level, double* center,
+                               double* scale, int32_t* template_indices,
+                               double* node_positions, int32_t* bind_nodes,
+                               double* bind_weights, int32_t* bind_counts,
+                               int32_t* edges, int edge_capacity, int* edge_count);
+
+/* closest_points(...) (bindings.cpp:1004-1044 -> src/cuda/lbvh.cu:439-533):
+ * nearest target point, interpolated normal, distance and triangle per query,
+ * through the device hierarchy. */
+int nricp_closest_points(const double* target_points, int vertex_count,
+                         const int32_t* faces, int face_count, const double* queries,
+                         int query_count, double* out_points, double* out_normals,
+                         double* out_distances, int32_t* out_triangles);
+
+/* The hierarchy's canonical arrays (src/cuda/lbvh.cu:553-668): sorted 30-bit
+ * Morton codes, the sort permutation, and each internal node's Karras
+ * children (child < face_count: leaf; else face_count + internal index). */
+int nricp_lbvh_export(const double* target_points, int vertex_count,
+                      const int32_t* faces, int face_count, uint32_t* codes,
+                      uint32_t* order, int32_t* left, int32_t* right, float* bounds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NRICP_B200_H */

@@ -1,0 +1,532 @@
+// Host-side preparation of a wrap.  See host.hpp.
+//
+// Compiled with -ffp-contract=off so that every FP64 expression rounds the way
+// the reference's host code does: the template graph (seeds, bindings, edges)
+// then comes out bit-identical to src/core/graph.cpp's.
+#include "host.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <iomanip>
+#include <limits>
+#include <numeric>
+#include <sstream>
+#include <unordered_set>
+#include <utility>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace nricp_b200 {
+
+namespace {
+
+inline double sqdist(const double* a, const double* b) {  // sampling.cpp:17-19
+    const double x = a[0] - b[0], y = a[1] - b[1], z = a[2] - b[2];
+    return x * x + y * y + z * z;
+}
+
+void keep_nearest(double* sq, int* idx, int& held, int capacity, double value, int entry) {
+    // sampling.cpp:23-42
+    if (held == capacity) {
+        const bool beats = value < sq[capacity - 1] ||
+                           (value == sq[capacity - 1] && entry < idx[capacity - 1]);
+        if (!beats) return;
+    }
+    int at = held < capacity ? held++ : capacity - 1;
+    while (at > 0 && (sq[at - 1] > value || (sq[at - 1] == value && idx[at - 1] > entry))) {
+        sq[at] = sq[at - 1];
+        idx[at] = idx[at - 1];
+        --at;
+    }
+    sq[at] = value;
+    idx[at] = entry;
+}
+
+}  // namespace
+
+void validate_mesh(const double* p, int n, const int32_t* f, int m, const char* what) {
+    std::vector<std::string> problems;  // mesh.cpp:90-116
+    if (n <= 0) problems.push_back("mesh has no vertices");
+    if (m <= 0) problems.push_back("mesh has no faces; closest-point queries need a surface");
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(p[i * 3]) || !std::isfinite(p[i * 3 + 1]) || !std::isfinite(p[i * 3 + 2]))
+            problems.push_back("vertex " + std::to_string(i) + " is not finite");
+    for (int i = 0; i < m; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const int index = f[i * 3 + k];
+            if (index < 0 || index >= n)
+                problems.push_back("face " + std::to_string(i) + " corner " + std::to_string(k) +
+                                   " index " + std::to_string(index) + " is out of range");
+        }
+    if (problems.empty()) return;
+    std::string message = std::string("invalid ") + what + " mesh: ";
+    for (size_t i = 0; i < problems.size(); ++i) message += (i ? "; " : "") + problems[i];
+    throw InvalidArgument(message);
+}
+
+void validate_settings(const NricpSolveDesc& d) {
+    validate_mesh(d.template_points, d.template_vertex_count, d.template_faces,
+                  d.template_face_count, "template");
+    validate_mesh(d.target_points, d.target_vertex_count, d.target_faces, d.target_face_count,
+                  "target");
+    const int k = d.max_nodes_per_vertex > 0 ? d.max_nodes_per_vertex : 4;
+    if (k > NRICP_MAX_SLOTS)
+        throw InvalidArgument("max_nodes_per_vertex is " + std::to_string(k) + "; at most " +
+                              std::to_string(NRICP_MAX_SLOTS) + " nodes can bind a vertex");
+    if (d.graph_levels > 16)
+        throw InvalidArgument("graph_levels is " + std::to_string(d.graph_levels) +
+                              "; at most 16 levels are supported");
+    if (d.route != NRICP_ROUTE_B && d.route != NRICP_ROUTE_C)
+        throw InvalidArgument("the device session runs 'route_b' or 'route_c'");
+    if (d.mask) {  // constraints.cpp:34-58
+        int active = 0;
+        for (int i = 0; i < d.template_vertex_count; ++i) active += d.mask[i] ? 1 : 0;
+        if (active == 0)
+            throw InvalidArgument(
+                "invalid mask: mask excludes every vertex; the fit would be unconstrained");
+    }
+    if (d.landmark_count > 0) {  // constraints.cpp:8-32
+        std::vector<std::string> problems;
+        std::unordered_set<int> seen;
+        for (int i = 0; i < d.landmark_count; ++i) {
+            const int v = d.landmark_indices[i];
+            if (v < 0 || v >= d.template_vertex_count) {
+                problems.push_back("landmark " + std::to_string(i) + " points at template vertex " +
+                                   std::to_string(v) + " but the template has " +
+                                   std::to_string(d.template_vertex_count) + " vertices");
+                continue;
+            }
+            const double* t = d.landmark_targets + i * 3;
+            if (!std::isfinite(t[0]) || !std::isfinite(t[1]) || !std::isfinite(t[2]))
+                problems.push_back("landmark " + std::to_string(i) + " has a non-finite target");
+            if (!seen.insert(v).second)
+                problems.push_back("landmark " + std::to_string(i) + " marks template vertex " +
+                                   std::to_string(v) + " twice");
+        }
+        if (!problems.empty()) {
+            std::string message = "invalid landmarks: ";
+            for (size_t i = 0; i < problems.size(); ++i) message += (i ? "; " : "") + problems[i];
+            throw InvalidArgument(message);
+        }
+    }
+}
+
+void compute_normalization(const double* p, int n, double center[3], double* scale) {
+    // mesh.cpp:47-64, 174-181
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (n > 0)
+        for (int k = 0; k < 3; ++k) lo[k] = hi[k] = p[k];
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], p[i * 3 + k]);
+            hi[k] = std::max(hi[k], p[i * 3 + k]);
+        }
+    for (int k = 0; k < 3; ++k) center[k] = (lo[k] + hi[k]) * 0.5;
+    const double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    const double diagonal = std::sqrt(dx * dx + dy * dy + dz * dz);
+    *scale = diagonal > 0.0 ? 1.0 / diagonal : 1.0;
+}
+
+std::vector<double> normalized(const double* p, int n, const double center[3], double scale) {
+    std::vector<double> out(static_cast<size_t>(n) * 3);  // mesh.cpp:183-187
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) out[i * 3 + k] = (p[i * 3 + k] - center[k]) * scale;
+    return out;
+}
+
+std::vector<double> vertex_normals(const std::vector<double>& p, const int32_t* f, int m) {
+    const size_t n = p.size() / 3;  // mesh.cpp:71-88
+    std::vector<double> out(n * 3, 0.0);
+    for (int i = 0; i < m; ++i) {
+        const double* a = &p[f[i * 3] * 3];
+        const double* b = &p[f[i * 3 + 1] * 3];
+        const double* c = &p[f[i * 3 + 2] * 3];
+        const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        const double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        const double w[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                             e1[0] * e2[1] - e1[1] * e2[0]};
+        for (int k = 0; k < 3; ++k) {
+            double* t = &out[f[i * 3 + k] * 3];
+            t[0] = t[0] + w[0];
+            t[1] = t[1] + w[1];
+            t[2] = t[2] + w[2];
+        }
+    }
+    for (size_t i = 0; i < n; ++i) {
+        double* v = &out[i * 3];
+        const double length = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        if (length > 0.0) {
+            v[0] = v[0] / length; v[1] = v[1] / length; v[2] = v[2] / length;
+        } else {
+            v[0] = v[1] = v[2] = 0.0;
+        }
+    }
+    return out;
+}
+
+// sampling.cpp:47-88.  Ties go to the lowest index; a parallel sweep keeps
+// that rule by combining per-thread maxima in thread order.
+std::vector<int> farthest_point_seeds(const std::vector<double>& pts, int count, int first) {
+    const int n = static_cast<int>(pts.size() / 3);
+    std::vector<int> seeds;
+    if (n <= 0 || count <= 0) return seeds;
+    count = std::min(count, n);
+    first = std::clamp(first, 0, n - 1);
+    std::vector<double> nearest(static_cast<size_t>(n));
+    seeds.reserve(count);
+    seeds.push_back(first);
+    const double* chosen = &pts[first * 3];
+    int best = first;
+    double best_sq = -1.0;
+    for (int i = 0; i < n; ++i) {
+        nearest[i] = sqdist(&pts[i * 3], chosen);
+        if (nearest[i] > best_sq) { best_sq = nearest[i]; best = i; }
+    }
+#ifdef _OPENMP
+    const int threads = n >= 20000 ? std::min(omp_get_max_threads(), 16) : 1;
+#else
+    const int threads = 1;
+#endif
+    std::vector<double> t_best(threads);
+    std::vector<int> t_idx(threads);
+    while (static_cast<int>(seeds.size()) < count) {
+        seeds.push_back(best);
+        chosen = &pts[best * 3];
+#pragma omp parallel num_threads(threads)
+        {
+#ifdef _OPENMP
+            const int t = omp_get_thread_num();
+#else
+            const int t = 0;
+#endif
+            const int begin = static_cast<int>((long)n * t / threads);
+            const int end = static_cast<int>((long)n * (t + 1) / threads);
+            double bs = -1.0;
+            int bi = begin;
+            for (int i = begin; i < end; ++i) {
+                const double d = sqdist(&pts[i * 3], chosen);
+                nearest[i] = nearest[i] < d ? nearest[i] : d;
+                if (nearest[i] > bs) { bs = nearest[i]; bi = i; }
+            }
+            t_best[t] = bs;
+            t_idx[t] = bi;
+        }
+        best_sq = -1.0;
+        for (int t = 0; t < threads; ++t)
+            if (t_best[t] > best_sq) { best_sq = t_best[t]; best = t_idx[t]; }
+    }
+    return seeds;
+}
+
+std::vector<Binding> bind_vertices(const std::vector<double>& vertices,
+                                   const std::vector<double>& nodes, int max_nodes, int slot_cap) {
+    const int vc = static_cast<int>(vertices.size() / 3);  // sampling.cpp:90-143
+    const int nc = static_cast<int>(nodes.size() / 3);
+    std::vector<Binding> out(static_cast<size_t>(vc));
+    for (Binding& b : out) {
+        for (int s = 0; s < NRICP_MAX_SLOTS; ++s) { b.nodes[s] = -1; b.weights[s] = 0.0; }
+        b.count = 0;
+    }
+    if (nc <= 0) return out;
+    const int support = std::max(1, std::min({max_nodes, nc, slot_cap}));
+#pragma omp parallel for schedule(static) if (static_cast<long>(vc) * nc > 2000000)
+    for (int v = 0; v < vc; ++v) {
+        double best_sq[NRICP_MAX_SLOTS];
+        int best_idx[NRICP_MAX_SLOTS];
+        int held = 0;
+        const double* p = &vertices[v * 3];
+        for (int n = 0; n < nc; ++n) keep_nearest(best_sq, best_idx, held, support, sqdist(p, &nodes[n * 3]), n);
+        Binding b;
+        for (int s = 0; s < NRICP_MAX_SLOTS; ++s) { b.nodes[s] = -1; b.weights[s] = 0.0; }
+        b.count = support;
+        const double dmax = std::sqrt(best_sq[support - 1]);
+        double total = 0.0;
+        for (int s = 0; s < support; ++s) {
+            const double distance = std::sqrt(best_sq[s]);
+            const double ratio = dmax > 0.0 ? distance / dmax : 0.0;
+            const double falloff = 1.0 - ratio;
+            b.nodes[s] = best_idx[s];
+            b.weights[s] = falloff * falloff;
+            total += b.weights[s];
+        }
+        for (int s = 0; s < support; ++s)
+            b.weights[s] = total > 0.0 ? b.weights[s] / total : 1.0 / static_cast<double>(support);
+        out[v] = b;
+    }
+    return out;
+}
+
+std::vector<int32_t> node_edges(const std::vector<double>& nodes, int neighbours) {
+    const int n = static_cast<int>(nodes.size() / 3);  // graph.cpp:11-39
+    if (n <= 1 || neighbours <= 0) return {};
+    const int taken = std::min(neighbours, n - 1);
+    std::vector<std::pair<int, int>> pairs(static_cast<size_t>(n) * taken);
+#pragma omp parallel for schedule(static) if (n > 512)
+    for (int i = 0; i < n; ++i) {
+        std::vector<std::pair<double, int>> d;
+        d.reserve(n - 1);
+        for (int o = 0; o < n; ++o) {
+            if (o == i) continue;
+            const double x = nodes[i * 3] - nodes[o * 3], y = nodes[i * 3 + 1] - nodes[o * 3 + 1],
+                         z = nodes[i * 3 + 2] - nodes[o * 3 + 2];
+            d.push_back({std::sqrt(x * x + y * y + z * z), o});
+        }
+        std::partial_sort(d.begin(), d.begin() + taken, d.end());
+        for (int k = 0; k < taken; ++k) {
+            const int o = d[k].second;
+            pairs[static_cast<size_t>(i) * taken + k] = {std::min(i, o), std::max(i, o)};
+        }
+    }
+    std::sort(pairs.begin(), pairs.end());
+    pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+    std::vector<int32_t> out;
+    out.reserve(pairs.size() * 2);
+    for (auto& p : pairs) { out.push_back(p.first); out.push_back(p.second); }
+    return out;
+}
+
+int level_node_count(int level, int nodes_initial, int growth, int vertex_count) {
+    const double g = std::pow(static_cast<double>(std::max(1, growth)), static_cast<double>(level));
+    const int requested = std::max(1, static_cast<int>(std::lround(nodes_initial * g)));
+    return std::min(requested, vertex_count);  // graph.cpp:52-57
+}
+
+TemplateGraph build_template_graph(const double* points, int count, int levels, int nodes_initial,
+                                   int growth, int max_nodes, int edge_neighbours) {
+    TemplateGraph graph;  // graph.cpp:41-76
+    compute_normalization(points, count, graph.center, &graph.scale);
+    const std::vector<double> norm = normalized(points, count, graph.center, graph.scale);
+    const int level_count = std::max(1, levels);
+    // The greedy sampling does not depend on how many seeds it is asked for,
+    // so every level's seeds are a prefix of the largest level's.
+    int most = 0;
+    for (int l = 0; l < level_count; ++l)
+        most = std::max(most, level_node_count(l, nodes_initial, growth, count));
+    const std::vector<int> seeds = farthest_point_seeds(norm, most, 0);
+    for (int l = 0; l < level_count; ++l) {
+        GraphLevel level;
+        const int n = std::min<int>(level_node_count(l, nodes_initial, growth, count),
+                                    static_cast<int>(seeds.size()));
+        level.template_index.assign(seeds.begin(), seeds.begin() + n);
+        level.rest.resize(static_cast<size_t>(n) * 3);
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < 3; ++k) level.rest[i * 3 + k] = norm[seeds[i] * 3 + k];
+        level.bindings = bind_vertices(norm, level.rest, max_nodes, NRICP_MAX_SLOTS);
+        level.edges = node_edges(level.rest, edge_neighbours);
+        graph.levels.push_back(std::move(level));
+    }
+    return graph;
+}
+
+LevelLayout build_layout(const TemplateGraph& graph, int level, int V) {
+    const GraphLevel& g = graph.levels[level];
+    LevelLayout L;
+    const int N = g.node_count();
+    L.node_count = N;
+    L.rest = g.rest;
+    L.bind_nodes.assign(static_cast<size_t>(V) * NRICP_MAX_SLOTS, -1);
+    L.bind_weights.assign(static_cast<size_t>(V) * NRICP_MAX_SLOTS, 0.0);
+    L.bind_counts.assign(V, 0);
+    // usable_binding (fused_assembly.cpp:85-98): only slots that contribute
+    for (int v = 0; v < V; ++v) {
+        const Binding& b = g.bindings[v];
+        int c = 0;
+        for (int s = 0; s < b.count; ++s) {
+            if (b.nodes[s] < 0 || b.nodes[s] >= N || b.weights[s] == 0.0) continue;
+            L.bind_nodes[v * NRICP_MAX_SLOTS + c] = b.nodes[s];
+            L.bind_weights[v * NRICP_MAX_SLOTS + c] = b.weights[s];
+            ++c;
+        }
+        L.bind_counts[v] = c;
+    }
+    // node -> (vertex, slot)
+    std::vector<int32_t> count(N + 1, 0);
+    for (int v = 0; v < V; ++v)
+        for (int s = 0; s < L.bind_counts[v]; ++s) count[L.bind_nodes[v * NRICP_MAX_SLOTS + s] + 1]++;
+    L.gather_begin.assign(N + 1, 0);
+    for (int n = 0; n < N; ++n) L.gather_begin[n + 1] = L.gather_begin[n] + count[n + 1];
+    L.gather_entry.assign(L.gather_begin[N], 0);
+    {
+        std::vector<int32_t> cursor(L.gather_begin.begin(), L.gather_begin.end() - 1);
+        for (int v = 0; v < V; ++v)
+            for (int s = 0; s < L.bind_counts[v]; ++s) {
+                const int n = L.bind_nodes[v * NRICP_MAX_SLOTS + s];
+                L.gather_entry[cursor[n]++] = v * NRICP_MAX_SLOTS + s;
+            }
+    }
+    // smoothness edges and node -> edge lists
+    L.edges = g.edges;
+    L.edge_count = static_cast<int>(g.edges.size() / 2);
+    L.node_edge_begin.assign(N + 1, 0);
+    for (int e = 0; e < L.edge_count; ++e) {
+        L.node_edge_begin[L.edges[e * 2] + 1]++;
+        L.node_edge_begin[L.edges[e * 2 + 1] + 1]++;
+    }
+    for (int n = 0; n < N; ++n) L.node_edge_begin[n + 1] += L.node_edge_begin[n];
+    L.node_edge_list.assign(L.node_edge_begin[N], 0);
+    {
+        std::vector<int32_t> cursor(L.node_edge_begin.begin(), L.node_edge_begin.end() - 1);
+        for (int e = 0; e < L.edge_count; ++e) {
+            L.node_edge_list[cursor[L.edges[e * 2]]++] = e;
+            L.node_edge_list[cursor[L.edges[e * 2 + 1]]++] = e;
+        }
+    }
+    // node pairs sharing a vertex (the interactions_ map of
+    // fused_assembly.cpp:68-79), grouped by (a, b)
+    struct PairEntry { int a, b, code; };
+    std::vector<PairEntry> entries;
+    for (int v = 0; v < V; ++v) {
+        const int c = L.bind_counts[v];
+        for (int x = 0; x < c; ++x)
+            for (int y = x + 1; y < c; ++y) {
+                const int nx = L.bind_nodes[v * NRICP_MAX_SLOTS + x];
+                const int ny = L.bind_nodes[v * NRICP_MAX_SLOTS + y];
+                if (nx == ny) continue;
+                const bool xf = nx < ny;
+                entries.push_back({xf ? nx : ny, xf ? ny : nx,
+                                   v * 64 + (xf ? x : y) * 8 + (xf ? y : x)});
+            }
+    }
+    std::stable_sort(entries.begin(), entries.end(), [](const PairEntry& l, const PairEntry& r) {
+        return l.a != r.a ? l.a < r.a : l.b < r.b;
+    });
+    L.pair_begin.push_back(0);
+    for (size_t i = 0; i < entries.size(); ++i) {
+        if (i == 0 || entries[i].a != entries[i - 1].a || entries[i].b != entries[i - 1].b) {
+            if (i > 0) L.pair_begin.push_back(static_cast<int32_t>(i));
+            L.pair_nodes.push_back(entries[i].a);
+            L.pair_nodes.push_back(entries[i].b);
+        }
+        L.pair_entry.push_back(entries[i].code);
+    }
+    L.pair_count = static_cast<int>(L.pair_nodes.size() / 2);
+    L.pair_begin.resize(L.pair_count + 1);
+    L.pair_begin[L.pair_count] = static_cast<int32_t>(entries.size());
+    // off-diagonal blocks: smoothness edges, then pair groups
+    L.offdiag_nodes = L.edges;
+    L.offdiag_nodes.insert(L.offdiag_nodes.end(), L.pair_nodes.begin(), L.pair_nodes.end());
+    const int B = L.edge_count + L.pair_count;
+    L.row_begin.assign(N + 1, 0);
+    for (int k = 0; k < B; ++k) {
+        L.row_begin[L.offdiag_nodes[k * 2] + 1]++;
+        L.row_begin[L.offdiag_nodes[k * 2 + 1] + 1]++;
+    }
+    for (int n = 0; n < N; ++n) L.row_begin[n + 1] += L.row_begin[n];
+    L.row_entry.assign(L.row_begin[N], 0);
+    {
+        std::vector<int32_t> cursor(L.row_begin.begin(), L.row_begin.end() - 1);
+        for (int k = 0; k < B; ++k) {
+            L.row_entry[cursor[L.offdiag_nodes[k * 2]]++] = k * 2;
+            L.row_entry[cursor[L.offdiag_nodes[k * 2 + 1]]++] = k * 2 + 1;
+        }
+    }
+    // warm start from the previous level (deformation.cpp:141-160): the new
+    // nodes bound to the old ones with the reference's four slots
+    L.transfer_nodes.assign(static_cast<size_t>(N) * 4, 0);
+    L.transfer_weights.assign(static_cast<size_t>(N) * 4, 0.0);
+    L.transfer_counts.assign(N, 0);
+    if (level > 0) {
+        const GraphLevel& from = graph.levels[level - 1];
+        const std::vector<Binding> tb = bind_vertices(g.rest, from.rest, 4, 4);
+        for (int n = 0; n < N; ++n) {
+            L.transfer_counts[n] = tb[n].count;
+            for (int s = 0; s < 4; ++s) {
+                L.transfer_nodes[n * 4 + s] = tb[n].nodes[s] < 0 ? 0 : tb[n].nodes[s];
+                L.transfer_weights[n * 4 + s] = tb[n].weights[s];
+            }
+        }
+    }
+    return L;
+}
+
+void vertex_faces(const int32_t* faces, int m, int V, std::vector<int32_t>& begin,
+                  std::vector<int32_t>& list) {
+    begin.assign(V + 1, 0);
+    for (int f = 0; f < m; ++f)
+        for (int k = 0; k < 3; ++k) begin[faces[f * 3 + k] + 1]++;
+    for (int v = 0; v < V; ++v) begin[v + 1] += begin[v];
+    list.assign(begin[V], 0);
+    std::vector<int32_t> cursor(begin.begin(), begin.end() - 1);
+    for (int f = 0; f < m; ++f)
+        for (int k = 0; k < 3; ++k) list[cursor[faces[f * 3 + k]]++] = f;
+}
+
+namespace {
+std::string number(double value) {  // report.cpp:36-43
+    if (!std::isfinite(value)) return "null";
+    std::ostringstream out;
+    out << std::setprecision(17) << value;
+    return out.str();
+}
+}  // namespace
+
+std::string report_json(const char* route, const char* precision, const double e[5],
+                        const StatsView& c, const std::vector<LevelView>& levels,
+                        const NricpSolveDesc& desc, double units, double setup_seconds,
+                        double solve_seconds) {
+    std::ostringstream out;  // report.cpp:46-105
+    out << std::setprecision(17);
+    out << "{\n";
+    out << "  \"version\": \"0.1.0\",\n";
+    out << "  \"route\": \"" << route << "\",\n";
+    out << "  \"precision\": \"" << precision << "\",\n";
+    out << "  \"setup_seconds\": " << number(setup_seconds) << ",\n";
+    out << "  \"solve_seconds\": " << number(solve_seconds) << ",\n";
+    out << "  \"energy\": {\n";
+    out << "    \"point_to_point\": " << number(e[0]) << ",\n";
+    out << "    \"point_to_plane\": " << number(e[1]) << ",\n";
+    out << "    \"smoothness\": " << number(e[2]) << ",\n";
+    out << "    \"anchor\": " << number(e[3]) << ",\n";
+    out << "    \"landmark\": " << number(e[4]) << ",\n";
+    out << "    \"total\": " << number(e[0] + e[1] + e[2] + e[3] + e[4]) << "\n";
+    out << "  },\n";
+    out << "  \"correspondence\": {\n";
+    out << "    \"total\": " << c.total << ",\n";
+    out << "    \"accepted\": " << c.accepted << ",\n";
+    out << "    \"rejected_distance\": " << c.rejected_distance << ",\n";
+    out << "    \"rejected_normal\": " << c.rejected_normal << ",\n";
+    out << "    \"rejected_slope\": " << c.rejected_slope << ",\n";
+    out << "    \"rejected_masked\": " << c.rejected_masked << ",\n";
+    out << "    \"distance_mean\": " << number(c.mean) << ",\n";
+    out << "    \"distance_p95\": " << number(c.p95) << ",\n";
+    out << "    \"distance_max\": " << number(c.max) << "\n";
+    out << "  },\n";
+    out << "  \"levels\": [";
+    for (size_t i = 0; i < levels.size(); ++i) {
+        const LevelView& l = levels[i];
+        out << (i == 0 ? "\n" : ",\n");
+        out << "    {\"level\": " << l.level << ", \"nodes\": " << l.nodes
+            << ", \"outer_iterations\": " << l.outer_iterations
+            << ", \"inner_iterations\": " << l.inner_iterations
+            << ", \"energy_start\": " << number(l.energy_start)
+            << ", \"energy_end\": " << number(l.energy_end)
+            << ", \"correspondence_mean\": " << number(l.correspondence_mean)
+            << ", \"converged\": " << (l.converged ? "true" : "false") << "}";
+    }
+    out << (levels.empty() ? "],\n" : "\n  ],\n");
+    out << "  \"settings\": {";
+    bool first = true;
+    const char* keys[6] = {"point_to_point", "point_to_plane", "smoothness", "anchor",
+                           "landmark", "robust_threshold"};
+    for (size_t l = 0; l < levels.size(); ++l) {
+        NricpLevelSettings s;
+        nricp_default_level(&s);
+        if (desc.level_setting_count > 0)
+            s = desc.levels[std::min<int>(static_cast<int>(l), desc.level_setting_count - 1)];
+        const double robust = s.robust_threshold > 0.0 ? s.robust_threshold * units : s.robust_threshold;
+        const double values[6] = {s.point_to_point, s.point_to_plane, s.smoothness, s.anchor,
+                                  s.landmark, robust};
+        for (int k = 0; k < 6; ++k) {
+            out << (first ? "\n" : ",\n");
+            first = false;
+            out << "    \"level" << l << "_" << keys[k] << "\": " << number(values[k]);
+        }
+    }
+    out << (first ? "}\n" : "\n  }\n");
+    out << "}\n";
+    return out.str();
+}
+
+}  // namespace nricp_b200

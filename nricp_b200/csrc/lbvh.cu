@@ -1,0 +1,768 @@
+// The target's Morton-code LBVH: build and closest-point query.
+//
+// Build (once per target, all on the device): FP32 triangle centroids and
+// scene bounds, 30-bit Morton codes with the reference's quantisation
+// (src/cuda/lbvh.cu:146-168), a stable LSD radix sort of (code, index) written
+// here (4-bit digits, per-tile ranking in shared memory), Karras' split search
+// with index tie-breaking (lbvh.cu:177-245), and a bottom-up box fit with the
+// fence + arrival-counter protocol (no waiting: the second child to arrive
+// merges).  The hierarchy is then packed for traversal with each child's box
+// stored in its parent (64 B per internal node = one L2 line pair), so a
+// visit costs one 64-byte load instead of three dependent ones.
+//
+// Query (thread per template vertex): the previous correspondence's triangle
+// seeds the search radius, the traversal walks FP32 boxes and triangles with
+// a fixed-depth stack whose overflow is reported (never silently pruned), and
+// the winning triangle is re-evaluated in FP64 so that the correspondence
+// point, normal and distance are those of the reference's FP64 closest-point
+// routine (src/geometry/closest_point.cpp:24-121).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nricp_b200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSortItems = 8;                       // keys per thread per tile
+constexpr int kSortTile = kThreads * kSortItems;    // 2048 keys
+constexpr int kRadixBits = 4;
+constexpr int kRadix = 1 << kRadixBits;             // 16 bins
+
+__device__ inline uint32_t expand_bits(uint32_t v) {  // lbvh.cu:132-139
+    v &= 0x000003ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// FP32 copies of the target corners, triangle centroids ((a+b+c)/3 with each
+// operation rounded on its own, as lbvh.cu:44-45 evaluates it).
+__global__ void k_centroids(const double* __restrict__ points, const int32_t* __restrict__ faces,
+                            int count, float* __restrict__ centroids) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int32_t* f = faces + (long)t * 3;
+    for (int k = 0; k < 3; ++k) {
+        const float a = __double2float_rn(points[(long)f[0] * 3 + k]);
+        const float b = __double2float_rn(points[(long)f[1] * 3 + k]);
+        const float c = __double2float_rn(points[(long)f[2] * 3 + k]);
+        centroids[(long)t * 3 + k] = __fdiv_rn(__fadd_rn(__fadd_rn(a, b), c), 3.0f);
+    }
+}
+
+// Scene bounds of the centroids: per-block partials, then one block folds
+// them.  min/max are exact, so the order does not matter.
+__global__ void k_bounds_partial(const float* __restrict__ centroids, int count,
+                                 float* __restrict__ partial) {
+    __shared__ float lo[3][kThreads], hi[3][kThreads];
+    float l[3] = {3.4e38f, 3.4e38f, 3.4e38f}, h[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; ++k) {
+            l[k] = fminf(l[k], centroids[(long)i * 3 + k]);
+            h[k] = fmaxf(h[k], centroids[(long)i * 3 + k]);
+        }
+    for (int k = 0; k < 3; ++k) { lo[k][threadIdx.x] = l[k]; hi[k][threadIdx.x] = h[k]; }
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int k = 0; k < 3; ++k) {
+                lo[k][threadIdx.x] = fminf(lo[k][threadIdx.x], lo[k][threadIdx.x + s]);
+                hi[k][threadIdx.x] = fmaxf(hi[k][threadIdx.x], hi[k][threadIdx.x + s]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 3; ++k) {
+            partial[blockIdx.x * 6 + k] = lo[k][0];
+            partial[blockIdx.x * 6 + 3 + k] = hi[k][0];
+        }
+}
+
+__global__ void k_bounds_final(const float* __restrict__ partial, int blocks,
+                               float* __restrict__ bounds) {
+    if (threadIdx.x != 0) return;
+    float l[3] = {3.4e38f, 3.4e38f, 3.4e38f}, h[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    for (int b = 0; b < blocks; ++b)
+        for (int k = 0; k < 3; ++k) {
+            l[k] = fminf(l[k], partial[b * 6 + k]);
+            h[k] = fmaxf(h[k], partial[b * 6 + 3 + k]);
+        }
+    for (int k = 0; k < 3; ++k) { bounds[k] = l[k]; bounds[3 + k] = h[k]; }
+}
+
+__global__ void k_morton(const float* __restrict__ centroids, int count,
+                         const float* __restrict__ bounds, uint32_t* __restrict__ codes,
+                         uint32_t* __restrict__ order) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    uint32_t q[3];
+    for (int k = 0; k < 3; ++k) {
+        const float extent = __fsub_rn(bounds[3 + k], bounds[k]);
+        const float scale = extent > 1e-10f ? __fdiv_rn(1023.0f, extent) : 0.0f;
+        const float v = __fmul_rn(__fsub_rn(centroids[(long)t * 3 + k], bounds[k]), scale);
+        q[k] = (uint32_t)fminf(1023.0f, fmaxf(0.0f, v));
+    }
+    codes[t] = (expand_bits(q[2]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[0]);
+    order[t] = (uint32_t)t;
+}
+
+// ---- stable LSD radix sort of (key, value), 4-bit digits --------------------
+
+__global__ void k_radix_histogram(const uint32_t* __restrict__ keys, int count, int shift,
+                                  uint32_t* __restrict__ counts, int tiles) {
+    __shared__ uint32_t bins[kRadix];
+    if (threadIdx.x < kRadix) bins[threadIdx.x] = 0;
+    __syncthreads();
+    const long base = (long)blockIdx.x * kSortTile;
+    for (int i = threadIdx.x; i < kSortTile; i += blockDim.x) {
+        const long at = base + i;
+        if (at < count) atomicAdd(&bins[(keys[at] >> shift) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < kRadix) counts[threadIdx.x * tiles + blockIdx.x] = bins[threadIdx.x];
+}
+
+// Exclusive scan of the digit-major count matrix in one block.
+__global__ void k_radix_scan(uint32_t* __restrict__ counts, int total) {
+    __shared__ uint32_t sums[1024];
+    const int per = (total + blockDim.x - 1) / blockDim.x;
+    const int begin = threadIdx.x * per;
+    uint32_t local = 0;
+    for (int i = begin; i < begin + per && i < total; ++i) local += counts[i];
+    sums[threadIdx.x] = local;
+    __syncthreads();
+    for (int s = 1; s < blockDim.x; s <<= 1) {
+        const uint32_t v = threadIdx.x >= s ? sums[threadIdx.x - s] : 0;
+        __syncthreads();
+        sums[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t running = threadIdx.x == 0 ? 0 : sums[threadIdx.x - 1];
+    for (int i = begin; i < begin + per && i < total; ++i) {
+        const uint32_t c = counts[i];
+        counts[i] = running;
+        running += c;
+    }
+}
+
+// Each thread owns kSortItems consecutive keys of the tile, so ranking by
+// (digit, thread, position) preserves the input order within a digit.
+__global__ void k_radix_scatter(const uint32_t* __restrict__ keys_in,
+                                const uint32_t* __restrict__ values_in, int count, int shift,
+                                const uint32_t* __restrict__ offsets, int tiles,
+                                uint32_t* __restrict__ keys_out,
+                                uint32_t* __restrict__ values_out) {
+    __shared__ uint32_t grid_counts[kRadix * kThreads];  // [digit][thread]
+    __shared__ uint32_t partial[kThreads];
+    const long base = (long)blockIdx.x * kSortTile + (long)threadIdx.x * kSortItems;
+    uint32_t k[kSortItems], v[kSortItems];
+    int digit[kSortItems];
+    uint32_t mine[kRadix];
+    for (int d = 0; d < kRadix; ++d) mine[d] = 0;
+    for (int i = 0; i < kSortItems; ++i) {
+        const long at = base + i;
+        digit[i] = -1;
+        if (at < count) {
+            k[i] = keys_in[at];
+            v[i] = values_in[at];
+            digit[i] = (k[i] >> shift) & (kRadix - 1);
+            mine[digit[i]]++;
+        }
+    }
+    for (int d = 0; d < kRadix; ++d) grid_counts[d * kThreads + threadIdx.x] = mine[d];
+    __syncthreads();
+    // exclusive scan of the [digit][thread] matrix: each thread sums a run of
+    // kRadix consecutive entries, a block scan of the runs, then write-back.
+    uint32_t run = 0;
+    for (int i = 0; i < kRadix; ++i) run += grid_counts[threadIdx.x * kRadix + i];
+    partial[threadIdx.x] = run;
+    __syncthreads();
+    for (int s = 1; s < kThreads; s <<= 1) {
+        const uint32_t add = threadIdx.x >= s ? partial[threadIdx.x - s] : 0;
+        __syncthreads();
+        partial[threadIdx.x] += add;
+        __syncthreads();
+    }
+    uint32_t running = threadIdx.x == 0 ? 0 : partial[threadIdx.x - 1];
+    for (int i = 0; i < kRadix; ++i) {
+        const uint32_t c = grid_counts[threadIdx.x * kRadix + i];
+        grid_counts[threadIdx.x * kRadix + i] = running;
+        running += c;
+    }
+    __syncthreads();
+    uint32_t local[kRadix];
+    for (int d = 0; d < kRadix; ++d)
+        local[d] = grid_counts[d * kThreads + threadIdx.x] - grid_counts[d * kThreads] +
+                   offsets[d * tiles + blockIdx.x];
+    for (int i = 0; i < kSortItems; ++i) {
+        if (digit[i] < 0) continue;
+        const uint32_t at = local[digit[i]]++;
+        keys_out[at] = k[i];
+        values_out[at] = v[i];
+    }
+}
+
+// ---- Karras build --------------------------------------------------------
+
+__device__ inline int lcp(const uint32_t* codes, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = codes[i], b = codes[j];
+    if (a == b) return 32 + __clz((uint32_t)(i ^ j));
+    return __clz(a ^ b);
+}
+
+// Internal node i covers a range and splits it (lbvh.cu:190-245).  Children
+// are written in the reference's numbering: a leaf is its sorted position
+// (< n), an internal node is n + index.
+__global__ void k_karras(const uint32_t* __restrict__ codes, int n, int32_t* __restrict__ left,
+                         int32_t* __restrict__ right, int32_t* __restrict__ parent) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int pp = lcp(codes, n, i, i - 1);
+    const int pn = lcp(codes, n, i, i + 1);
+    const int dir = pn > pp ? 1 : -1;
+    const int pmin = pp < pn ? pp : pn;
+    int span = 2;
+    while (lcp(codes, n, i, i + span * dir) > pmin) span *= 2;
+    int last = 0;
+    for (int step = span / 2; step >= 1; step /= 2)
+        if (lcp(codes, n, i, i + (last + step) * dir) > pmin) last += step;
+    const int j = i + last * dir;
+    const int rl = i < j ? i : j, rr = i < j ? j : i;
+    const int np = lcp(codes, n, rl, rr);
+    int offset = 0, step = rr - rl;
+    do {
+        step = (step + 1) / 2;
+        if (lcp(codes, n, rl, rl + offset + step) > np) offset += step;
+    } while (step > 1);
+    const int split = rl + offset;
+    const int lc = rl == split ? rl : n + split;
+    const int rc = split + 1 == rr ? rr : n + split + 1;
+    left[i] = lc;
+    right[i] = rc;
+    parent[lc] = n + i;
+    parent[rc] = n + i;
+}
+
+struct Box { float lo[3], hi[3]; };
+
+// Leaf boxes from the FP32 corners, then the bottom-up merge: the fence makes
+// a child's box visible before its arrival is counted, and only the second
+// arrival at a parent carries on -- nothing ever waits.
+__global__ void k_refit(const double* __restrict__ points, const int32_t* __restrict__ faces,
+                        const uint32_t* __restrict__ order, int n,
+                        const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+                        const int32_t* __restrict__ parent, uint32_t* __restrict__ arrivals,
+                        float* __restrict__ boxes) {
+    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    const int32_t* f = faces + (long)order[leaf] * 3;
+    Box b;
+    for (int k = 0; k < 3; ++k) {
+        const float x = __double2float_rn(points[(long)f[0] * 3 + k]);
+        const float y = __double2float_rn(points[(long)f[1] * 3 + k]);
+        const float z = __double2float_rn(points[(long)f[2] * 3 + k]);
+        b.lo[k] = fminf(x, fminf(y, z));
+        b.hi[k] = fmaxf(x, fmaxf(y, z));
+    }
+    for (int k = 0; k < 3; ++k) {
+        boxes[(long)leaf * 6 + k] = b.lo[k];
+        boxes[(long)leaf * 6 + 3 + k] = b.hi[k];
+    }
+    int node = leaf;
+    for (int depth = 0; depth < 2 * n + 2; ++depth) {
+        const int p = parent[node];
+        if (p < 0) return;
+        __threadfence();
+        if (atomicAdd(&arrivals[p - n], 1u) != 1u) return;
+        __threadfence();
+        const int l = left[p - n], r = right[p - n];
+        for (int k = 0; k < 3; ++k) {
+            const float a = __ldcg(&boxes[(long)l * 6 + k]);
+            const float c = __ldcg(&boxes[(long)r * 6 + k]);
+            boxes[(long)p * 6 + k] = fminf(a, c);
+            const float a2 = __ldcg(&boxes[(long)l * 6 + 3 + k]);
+            const float c2 = __ldcg(&boxes[(long)r * 6 + 3 + k]);
+            boxes[(long)p * 6 + 3 + k] = fmaxf(a2, c2);
+        }
+        node = p;
+    }
+}
+
+
+__device__ inline uint32_t encode_child(int child, int n) {
+    return child < n ? (kLeafBit | (uint32_t)child) : (uint32_t)(child - n);
+}
+
+// Traversal layout: internal node i = 4 float4 = (left box lo, left hi.x),
+// (left hi.yz, right lo.xy), (right lo.z, right hi), (children, unused).
+__global__ void k_pack_nodes(const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+                             const float* __restrict__ boxes, int n, float4* __restrict__ nodes) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int l = left[i], r = right[i];
+    const float* bl = boxes + (long)l * 6;
+    const float* br = boxes + (long)r * 6;
+    nodes[(long)i * 4 + 0] = make_float4(bl[0], bl[1], bl[2], bl[3]);
+    nodes[(long)i * 4 + 1] = make_float4(bl[4], bl[5], br[0], br[1]);
+    nodes[(long)i * 4 + 2] = make_float4(br[2], br[3], br[4], br[5]);
+    nodes[(long)i * 4 + 3] = make_float4(__uint_as_float(encode_child(l, n)),
+                                         __uint_as_float(encode_child(r, n)), 0.0f, 0.0f);
+}
+
+__global__ void k_pack_leaves(const double* __restrict__ points, const int32_t* __restrict__ faces,
+                              const uint32_t* __restrict__ order, int n,
+                              float4* __restrict__ leaves) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int tri = (int)order[i];
+    const int32_t* f = faces + (long)tri * 3;
+    float c[9];
+    for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) c[k * 3 + a] = __double2float_rn(points[(long)f[k] * 3 + a]);
+    leaves[(long)i * 3 + 0] = make_float4(c[0], c[1], c[2], c[3]);
+    leaves[(long)i * 3 + 1] = make_float4(c[4], c[5], c[6], c[7]);
+    leaves[(long)i * 3 + 2] = make_float4(c[8], __int_as_float(tri), 0.0f, 0.0f);
+}
+
+int blocks_for(long n, int threads = kThreads) { return (int)((n + threads - 1) / threads); }
+
+}  // namespace
+
+size_t lbvh_scratch_bytes(int n) {
+    // the carve sequence of lbvh_build, each piece rounded up to 256 bytes
+    const size_t tiles = (size_t)((n + kSortTile - 1) / kSortTile);
+    const size_t pieces[] = {
+        sizeof(float) * 3 * (size_t)n,                 // centroids
+        sizeof(float) * 6 * 1024,                      // bound partials
+        64,                                            // bounds
+        sizeof(uint32_t) * (size_t)n, sizeof(uint32_t) * (size_t)n,  // keys x2
+        sizeof(uint32_t) * (size_t)n, sizeof(uint32_t) * (size_t)n,  // values x2
+        sizeof(uint32_t) * kRadix * (tiles + 1),       // digit counts
+        sizeof(int32_t) * (size_t)n, sizeof(int32_t) * (size_t)n,    // left, right
+        sizeof(int32_t) * 2 * (size_t)n,               // parent
+        sizeof(uint32_t) * (size_t)n,                  // arrivals
+        sizeof(float) * 6 * 2 * (size_t)n,             // boxes
+    };
+    size_t total = 0;
+    for (size_t bytes : pieces) total += (bytes + 255) & ~size_t(255);
+    return total + 256;
+}
+
+// Builds the hierarchy over `n` target triangles into `nodes` ((n-1) x 4
+// float4) and `leaves` (n x 3 float4) using `scratch`; optionally exports the
+// canonical arrays (sorted codes, permutation, Karras children) for parity
+// tests.  Returns the encoded root.
+uint32_t lbvh_build(const double* points, const int32_t* faces, int n, void* scratch,
+                    float4* nodes, float4* leaves, cudaStream_t stream, LbvhExport* out) {
+    char* base = static_cast<char*>(scratch);
+    auto carve = [&base](size_t bytes) {
+        char* p = base;
+        base += (bytes + 255) & ~size_t(255);
+        return p;
+    };
+    float* centroids = reinterpret_cast<float*>(carve(sizeof(float) * 3 * n));
+    float* bound_partial = reinterpret_cast<float*>(carve(sizeof(float) * 6 * 1024));
+    float* bounds = reinterpret_cast<float*>(carve(64));
+    uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n)),
+                         reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n))};
+    uint32_t* values[2] = {reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n)),
+                           reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n))};
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* counts = reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * kRadix * (tiles + 1)));
+    int32_t* left = reinterpret_cast<int32_t*>(carve(sizeof(int32_t) * n));
+    int32_t* right = reinterpret_cast<int32_t*>(carve(sizeof(int32_t) * n));
+    int32_t* parent = reinterpret_cast<int32_t*>(carve(sizeof(int32_t) * 2 * n));
+    uint32_t* arrivals = reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n));
+    float* boxes = reinterpret_cast<float*>(carve(sizeof(float) * 6 * 2 * n));
+
+    k_centroids<<<blocks_for(n), kThreads, 0, stream>>>(points, faces, n, centroids);
+    const int bound_blocks = blocks_for(n) < 1024 ? blocks_for(n) : 1024;
+    k_bounds_partial<<<bound_blocks, kThreads, 0, stream>>>(centroids, n, bound_partial);
+    k_bounds_final<<<1, 32, 0, stream>>>(bound_partial, bound_blocks, bounds);
+    k_morton<<<blocks_for(n), kThreads, 0, stream>>>(centroids, n, bounds, keys[0], values[0]);
+    int cur = 0;
+    for (int shift = 0; shift < 32; shift += kRadixBits) {
+        k_radix_histogram<<<tiles, kThreads, 0, stream>>>(keys[cur], n, shift, counts, tiles);
+        k_radix_scan<<<1, 1024, 0, stream>>>(counts, kRadix * tiles);
+        k_radix_scatter<<<tiles, kThreads, 0, stream>>>(keys[cur], values[cur], n, shift, counts,
+                                                        tiles, keys[1 - cur], values[1 - cur]);
+        cur = 1 - cur;
+    }
+    const uint32_t* codes = keys[cur];
+    const uint32_t* order = values[cur];
+    cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream);
+    cudaMemsetAsync(arrivals, 0, sizeof(uint32_t) * n, stream);
+    if (n > 1) {
+        k_karras<<<blocks_for(n - 1), kThreads, 0, stream>>>(codes, n, left, right, parent);
+    }
+    k_refit<<<blocks_for(n), kThreads, 0, stream>>>(points, faces, order, n, left, right, parent,
+                                                    arrivals, boxes);
+    if (n > 1) k_pack_nodes<<<blocks_for(n - 1), kThreads, 0, stream>>>(left, right, boxes, n, nodes);
+    k_pack_leaves<<<blocks_for(n), kThreads, 0, stream>>>(points, faces, order, n, leaves);
+    if (out) {
+        cudaMemcpyAsync(out->codes, codes, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(out->order, order, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream);
+        if (n > 1) {
+            cudaMemcpyAsync(out->left, left, sizeof(int32_t) * (n - 1), cudaMemcpyDeviceToHost, stream);
+            cudaMemcpyAsync(out->right, right, sizeof(int32_t) * (n - 1), cudaMemcpyDeviceToHost, stream);
+        }
+        cudaMemcpyAsync(out->bounds, bounds, sizeof(float) * 6, cudaMemcpyDeviceToHost, stream);
+    }
+    return n > 1 ? 0u : (kLeafBit | 0u);
+}
+
+// ---------------------------------------------------------------------------
+// Closest-point query
+// ---------------------------------------------------------------------------
+
+__device__ inline float box_distance(F3 p, float lx, float ly, float lz, float hx, float hy,
+                                     float hz) {
+    const float dx = fmaxf(fmaxf(lx - p.x, p.x - hx), 0.0f);
+    const float dy = fmaxf(fmaxf(ly - p.y, p.y - hy), 0.0f);
+    const float dz = fmaxf(fmaxf(lz - p.z, p.z - hz), 0.0f);
+    return dx * dx + dy * dy + dz * dz;
+}
+
+// Squared distance from p to a triangle (Voronoi-region closest point,
+// closest_point.cpp:24-121), FP32, for ranking candidates.
+__device__ inline float triangle_distance(F3 p, F3 a, F3 b, F3 c) {
+    const F3 ab = b - a, ac = c - a, ap = p - a;
+    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
+    F3 q;
+    if (d1 <= 0.0f && d2 <= 0.0f) {
+        q = a;
+    } else {
+        const F3 bp = p - b;
+        const float d3 = dot(ab, bp), d4 = dot(ac, bp);
+        if (d3 >= 0.0f && d4 <= d3) {
+            q = b;
+        } else {
+            const float vc = d1 * d4 - d3 * d2;
+            if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+                const float den = d1 - d3;
+                q = a + ab * (den != 0.0f ? d1 / den : 0.0f);
+            } else {
+                const F3 cp = p - c;
+                const float d5 = dot(ab, cp), d6 = dot(ac, cp);
+                if (d6 >= 0.0f && d5 <= d6) {
+                    q = c;
+                } else {
+                    const float vb = d5 * d2 - d1 * d6;
+                    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+                        const float den = d2 - d6;
+                        q = a + ac * (den != 0.0f ? d2 / den : 0.0f);
+                    } else {
+                        const float va = d3 * d6 - d5 * d4;
+                        if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+                            const float den = (d4 - d3) + (d5 - d6);
+                            q = b + (c - b) * (den != 0.0f ? (d4 - d3) / den : 0.0f);
+                        } else {
+                            const float den = va + vb + vc;
+                            if (fabsf(den) < 1e-30f) {
+                                q = a;
+                            } else {
+                                const float v = vb / den, w = vc / den;
+                                q = a + ab * v + ac * w;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    const F3 d = q - p;
+    return dot(d, d);
+}
+
+// FP64 closest point with barycentrics, the reference routine's exact steps
+// (closest_point.cpp:24-121), with every product and sum rounded on its own so
+// the result matches the host build bit for bit.
+__device__ inline double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ inline double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ inline double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ inline D3 vsub(D3 a, D3 b) { return {ds(a.x, b.x), ds(a.y, b.y), ds(a.z, b.z)}; }
+__device__ inline D3 vadd(D3 a, D3 b) { return {da(a.x, b.x), da(a.y, b.y), da(a.z, b.z)}; }
+__device__ inline D3 vmul(D3 a, double s) { return {dm(a.x, s), dm(a.y, s), dm(a.z, s)}; }
+__device__ inline double vdot(D3 a, D3 b) { return da(da(dm(a.x, b.x), dm(a.y, b.y)), dm(a.z, b.z)); }
+
+__device__ D3 closest_point_fp64(D3 p, D3 a, D3 b, D3 c, double* bary) {
+    const D3 ab = vsub(b, a), ac = vsub(c, a), ap = vsub(p, a);
+    const double d1 = vdot(ab, ap), d2 = vdot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) { bary[0] = 1; bary[1] = 0; bary[2] = 0; return a; }
+    const D3 bp = vsub(p, b);
+    const double d3 = vdot(ab, bp), d4 = vdot(ac, bp);
+    if (d3 >= 0.0 && d4 <= d3) { bary[0] = 0; bary[1] = 1; bary[2] = 0; return b; }
+    const double vc = ds(dm(d1, d4), dm(d3, d2));
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double den = ds(d1, d3);
+        const double v = den != 0.0 ? __ddiv_rn(d1, den) : 0.0;
+        bary[0] = ds(1.0, v); bary[1] = v; bary[2] = 0.0;
+        return vadd(a, vmul(ab, v));
+    }
+    const D3 cp = vsub(p, c);
+    const double d5 = vdot(ab, cp), d6 = vdot(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) { bary[0] = 0; bary[1] = 0; bary[2] = 1; return c; }
+    const double vb = ds(dm(d5, d2), dm(d1, d6));
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double den = ds(d2, d6);
+        const double w = den != 0.0 ? __ddiv_rn(d2, den) : 0.0;
+        bary[0] = ds(1.0, w); bary[1] = 0.0; bary[2] = w;
+        return vadd(a, vmul(ac, w));
+    }
+    const double va = ds(dm(d3, d6), dm(d5, d4));
+    if (va <= 0.0 && ds(d4, d3) >= 0.0 && ds(d5, d6) >= 0.0) {
+        const double den = da(ds(d4, d3), ds(d5, d6));
+        const double w = den != 0.0 ? __ddiv_rn(ds(d4, d3), den) : 0.0;
+        bary[0] = 0.0; bary[1] = ds(1.0, w); bary[2] = w;
+        return vadd(b, vmul(vsub(c, b), w));
+    }
+    const double den = da(da(va, vb), vc);
+    if (fabs(den) < 1e-300) { bary[0] = 1; bary[1] = 0; bary[2] = 0; return a; }
+    const double v = __ddiv_rn(vb, den), w = __ddiv_rn(vc, den);
+    bary[0] = ds(ds(1.0, v), w); bary[1] = v; bary[2] = w;
+    return vadd(vadd(a, vmul(ab, v)), vmul(ac, w));
+}
+
+__device__ inline D3 vnormalized(D3 a) {
+    const double length = __dsqrt_rn(vdot(a, a));
+    if (!(length > 0.0)) return {0.0, 0.0, 0.0};
+    return {__ddiv_rn(a.x, length), __ddiv_rn(a.y, length), __ddiv_rn(a.z, length)};
+}
+
+// Robust weight, src/energy/robust.cpp:30-58.
+__device__ inline double robust_weight(int kernel, double squared, double threshold) {
+    if (squared < 0.0) squared = 0.0;
+    if (kernel == 1) {
+        if (threshold <= 0.0) return 1.0;
+        if (squared <= threshold * threshold) return 1.0;
+        return threshold / sqrt(squared);
+    }
+    if (kernel == 2) {
+        if (threshold <= 0.0) return 1.0;
+        const double ratio = squared / (threshold * threshold);
+        const double den = 1.0 + ratio;
+        return 1.0 / (den * den);
+    }
+    return 1.0;
+}
+
+// FP64 squared distance from q to triangle `tri` of the target.
+__device__ inline double triangle_distance_fp64(const WrapDev& w, D3 q, int tri) {
+    const int32_t* f = w.tgt_faces + (long)tri * 3;
+    double bary[3];
+    const D3 c = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
+                                    load_d3(w.tgt_points, f[2]), bary);
+    const D3 d = vsub(c, q);
+    return vdot(d, d);
+}
+
+// Nearest target triangle for `q`.  The walk ranks boxes and triangles in
+// FP32; whenever a triangle lands within the FP32 error window of the best so
+// far (`w.rank_window`, a distance in the target's units) the two are
+// re-ranked in FP64, and exact FP64 ties go to the lower triangle index -- the
+// rule of an FP64 brute-force scan.  `seed` is a triangle whose distance
+// bounds the search from the start.  Returns the winner, or -1.
+__device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* overflow) {
+    const float window = w.rank_window;
+    float best = 3.4e38f;    // smallest FP32 squared distance seen
+    float bound = 3.4e38f;   // (sqrt(best) + window)^2: prune at or beyond
+    int best_tri = -1;
+    double best64 = 0.0;
+    bool best64_valid = false;
+    auto consider = [&](int tri, float d) {
+        if (!(d < bound)) return;
+        if (best_tri < 0 || sqrtf(d) + window < sqrtf(best)) {
+            best_tri = tri;
+            best64_valid = false;
+        } else {
+            // within the window of the current best: decide in FP64
+            if (!best64_valid) {
+                best64 = triangle_distance_fp64(w, q64, best_tri);
+                best64_valid = true;
+            }
+            const double d64 = triangle_distance_fp64(w, q64, tri);
+            if (d64 < best64 || (d64 == best64 && tri < best_tri)) {
+                best_tri = tri;
+                best64 = d64;
+            }
+        }
+        if (d < best) {
+            best = d;
+            const float r = sqrtf(best) + window;
+            bound = r * r;
+        }
+    };
+    if (seed >= 0 && seed < w.F) {
+        const int32_t* f = w.tgt_faces + (long)seed * 3;
+        F3 c[3];
+        for (int k = 0; k < 3; ++k)
+            c[k] = {__double2float_rn(w.tgt_points[(long)f[k] * 3]),
+                    __double2float_rn(w.tgt_points[(long)f[k] * 3 + 1]),
+                    __double2float_rn(w.tgt_points[(long)f[k] * 3 + 2])};
+        consider(seed, triangle_distance(q, c[0], c[1], c[2]));
+    }
+    uint32_t stack[kStackDepth];
+    float stack_d[kStackDepth];
+    int sp = 0;
+    uint32_t node = (uint32_t)w.bvh_root;
+    // A tree visits each node at most once; the cap only guards against a
+    // corrupt hierarchy, which it reports instead of looping.
+    const long step_limit = 4L * (long)w.F + 1024;
+    long steps = 0;
+    while (true) {
+        if (++steps > step_limit) {
+            *overflow = 1;
+            break;
+        }
+        if (node & kLeafBit) {
+            const int leaf = (int)(node & ~kLeafBit);
+            const float4 l0 = __ldg(&w.bvh_leaves[(long)leaf * 3 + 0]);
+            const float4 l1 = __ldg(&w.bvh_leaves[(long)leaf * 3 + 1]);
+            const float4 l2 = __ldg(&w.bvh_leaves[(long)leaf * 3 + 2]);
+            const int tri = __float_as_int(l2.y);
+            if (tri != seed)
+                consider(tri, triangle_distance(q, {l0.x, l0.y, l0.z}, {l0.w, l1.x, l1.y},
+                                                {l1.z, l1.w, l2.x}));
+        } else {
+            const float4* nd = w.bvh_nodes + (long)node * 4;
+            const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+            const float dl = box_distance(q, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
+            const float dr = box_distance(q, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
+            const uint32_t cl = __float_as_uint(n3.x), cr = __float_as_uint(n3.y);
+            const bool hl = dl < bound, hr = dr < bound;
+            if (hl && hr) {
+                const bool left_first = dl <= dr;
+                if (sp < kStackDepth) {
+                    stack[sp] = left_first ? cr : cl;
+                    stack_d[sp] = left_first ? dr : dl;
+                    ++sp;
+                } else {
+                    *overflow = 1;
+                }
+                node = left_first ? cl : cr;
+                continue;
+            }
+            if (hl) { node = cl; continue; }
+            if (hr) { node = cr; continue; }
+        }
+        // pop the next subtree that can still hold something closer
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stack_d[sp] < bound) { node = stack[sp]; found = true; break; }
+        }
+        if (!found) break;
+    }
+    return best_tri;
+}
+
+// One correspondence per template vertex, with the filters in the order the
+// reference applies them (correspondence.cpp:35-80) and the reweighting of
+// route_a.cpp:19-38.
+__global__ void k_query(const WrapDev* __restrict__ wraps) {
+    const WrapDev& w = wraps[blockIdx.y];
+    const WrapControl c = *w.control;
+    if (!(c.phase == kPhaseTransfer || c.phase == kPhaseRefresh || c.phase == kPhaseFinal)) return;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= w.V) return;
+    uint8_t code = 0;
+    D3 point = {0, 0, 0}, normal = {0, 0, 0};
+    double distance = 0.0, robust = 1.0;
+    int tri = -1;
+    if (w.mask && !w.mask[v]) {
+        code = 4;
+        tri = w.corr_triangle[v];
+    } else {
+        const float4 q32 = w.deformed32[v];
+        int overflow = 0;
+        tri = nearest_triangle(w, {q32.x, q32.y, q32.z}, load_d3(w.deformed, v), w.corr_triangle[v],
+                               &overflow);
+        if (overflow) atomicOr(&w.control->error, 1);
+        if (tri >= 0) {
+            const D3 q = load_d3(w.deformed, v);
+            const int32_t* f = w.tgt_faces + (long)tri * 3;
+            double bary[3];
+            point = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
+                                       load_d3(w.tgt_points, f[2]), bary);
+            const D3 d = vsub(point, q);
+            distance = __dsqrt_rn(vdot(d, d));
+            const D3 n0 = load_d3(w.tgt_normals, f[0]), n1 = load_d3(w.tgt_normals, f[1]),
+                     n2 = load_d3(w.tgt_normals, f[2]);
+            normal = vnormalized(vadd(vadd(vmul(n0, bary[0]), vmul(n1, bary[1])), vmul(n2, bary[2])));
+            if (distance > w.distance_threshold) {
+                code = 1;
+            } else if (vdot(load_d3(w.qnormals, v), normal) < w.min_normal_cosine) {
+                code = 2;
+            } else if (distance > 0.0) {
+                const D3 offset = vsub(q, point);
+                const double slope = __ddiv_rn(fabs(vdot(normal, offset)), distance);
+                if (slope < w.min_slope) code = 3;
+            }
+            if (code == 0) {
+                const D3 o = vsub(q, point);
+                const double squared = vdot(o, o);
+                const double threshold = w.robust_threshold[c.level];
+                robust = threshold > 0.0 ? robust_weight(w.robust_kernel[c.level], squared, threshold) : 1.0;
+            }
+        } else {
+            code = 1;
+        }
+    }
+    store_d3(w.corr_point, v, point);
+    store_d3(w.corr_normal, v, normal);
+    w.corr_distance[v] = distance;
+    w.corr_triangle[v] = tri;
+    w.corr_code[v] = code;
+    w.robust[v] = robust;
+}
+
+// Stand-alone query over a prepared hierarchy (parity tests and the
+// `closest_points` entry point): FP32 ranking, FP64 winner.
+__global__ void k_closest_points(const WrapDev* __restrict__ wraps, const double* __restrict__ queries,
+                                 int count, double* __restrict__ out_points,
+                                 double* __restrict__ out_normals, double* __restrict__ out_distances,
+                                 int32_t* __restrict__ out_triangles, int* __restrict__ overflow_flag) {
+    const WrapDev& w = wraps[0];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const D3 q = load_d3(queries, i);
+    int overflow = 0;
+    const int tri = nearest_triangle(w, {__double2float_rn(q.x), __double2float_rn(q.y),
+                                         __double2float_rn(q.z)}, q, -1, &overflow);
+    if (overflow) atomicOr(overflow_flag, 1);
+    D3 point = {0, 0, 0}, normal = {0, 0, 0};
+    double distance = 0.0;
+    if (tri >= 0) {
+        const int32_t* f = w.tgt_faces + (long)tri * 3;
+        double bary[3];
+        point = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
+                                   load_d3(w.tgt_points, f[2]), bary);
+        const D3 d = vsub(point, q);
+        distance = __dsqrt_rn(vdot(d, d));
+        normal = vnormalized(vadd(vadd(vmul(load_d3(w.tgt_normals, f[0]), bary[0]),
+                                       vmul(load_d3(w.tgt_normals, f[1]), bary[1])),
+                                  vmul(load_d3(w.tgt_normals, f[2]), bary[2])));
+    }
+    store_d3(out_points, i, point);
+    store_d3(out_normals, i, normal);
+    out_distances[i] = distance;
+    out_triangles[i] = tri;
+}
+
+void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaStream_t stream) {
+    dim3 grid(blocks_for(max_vertices, 128), wrap_count);
+    k_query<<<grid, 128, 0, stream>>>(wraps);
+}
+
+void launch_closest_points(const WrapDev* wrap, const double* queries, int count,
+                           double* points, double* normals, double* distances, int32_t* triangles,
+                           int* overflow, cudaStream_t stream) {
+    k_closest_points<<<blocks_for(count, 128), 128, 0, stream>>>(
+        wrap, queries, count, points, normals, distances, triangles, overflow);
+}
+
+}  // namespace nricp_b200

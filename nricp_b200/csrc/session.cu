@@ -1,0 +1,683 @@
+// Host orchestration of the device schedule and the C-ABI (include/nricp_b200.h).
+//
+// A Batch owns one or more wraps: their device arenas, the WrapDev
+// descriptors the kernels index by blockIdx.y, and one stream.  Running a
+// batch means replaying the tick (captured once as a CUDA graph) until every
+// wrap's device-side schedule reaches Done; the host only polls a pinned copy
+// of the schedule scalars every few ticks.  A session is a batch of one that
+// the caller advances one tick at a time.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/nricp_b200.h"
+#include "common.cuh"
+#include "host.hpp"
+#include "kernels.cuh"
+#include "session.hpp"
+
+namespace nricp_b200 {
+
+thread_local std::string g_last_error;
+
+void check(cudaError_t status, const char* what) {
+    if (status != cudaSuccess)
+        throw CudaError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(status));
+}
+
+namespace {
+
+double now_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// One device allocation carved into aligned sub-arrays.
+class Arena {
+public:
+    size_t reserve(size_t bytes) {
+        const size_t at = size_;
+        size_ += (bytes + 255) & ~size_t(255);
+        return at;
+    }
+    void allocate() {
+        if (size_ == 0) size_ = 256;
+        check(cudaMalloc(&base_, size_), "cudaMalloc(wrap arena)");
+    }
+    template <typename T>
+    T* at(size_t offset) const { return reinterpret_cast<T*>(static_cast<char*>(base_) + offset); }
+    size_t size() const { return size_; }
+    void release() {
+        if (base_) cudaFree(base_);
+        base_ = nullptr;
+    }
+
+private:
+    void* base_ = nullptr;
+    size_t size_ = 0;
+};
+
+// Candidates whose FP32 distances are this close (relative to the target's
+// diagonal) are re-ranked in FP64.
+constexpr double kRankWindow = 4e-6;
+
+double target_diagonal(const std::vector<double>& p) {
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (size_t i = 0; i < p.size() / 3; ++i)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = i ? std::min(lo[k], p[i * 3 + k]) : p[k];
+            hi[k] = i ? std::max(hi[k], p[i * 3 + k]) : p[k];
+        }
+    return std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                     (hi[2] - lo[2]) * (hi[2] - lo[2]));
+}
+
+template <typename T>
+void upload(T* dst, const std::vector<T>& src, cudaStream_t stream) {
+    if (!src.empty())
+        check(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, stream),
+              "upload");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Wrap: one template/target pair, prepared on the host, resident on the device
+// ---------------------------------------------------------------------------
+struct Wrap {
+    NricpSolveDesc desc{};
+    std::vector<NricpLevelSettings> level_settings;
+    std::vector<double> template_in, target_in, landmark_targets_in;
+    std::vector<int32_t> template_faces, target_faces, landmark_indices;
+    std::vector<uint8_t> mask;
+    TemplateGraph graph;
+    std::vector<LevelLayout> layouts;
+    int V = 0, T = 0, Vt = 0, F = 0, L = 0, levels = 0;
+    int max_nodes = 0, max_edges = 0, max_pairs = 0, max_offdiag = 0;
+    double setup_seconds = 0.0, solve_started = 0.0, solve_seconds = 0.0;
+    Arena arena;
+    WrapDev dev{};        // host copy of the descriptor
+    WrapControl* control = nullptr;  // device
+    WrapControl initial_control{};   // pinned-free host copy used by reset
+    double* identity_rot = nullptr;  // device: identity rotations + initial records
+    LevelRecord* initial_records = nullptr;
+    ~Wrap() {
+        arena.release();
+        if (identity_rot) cudaFree(identity_rot);
+    }
+};
+
+namespace {
+
+// Copies the caller's arrays: the wrap must not depend on them afterwards
+// (the reference's session copies its inputs too, session.cu:593-596).
+void copy_inputs(Wrap& w, const NricpSolveDesc& d) {
+    w.desc = d;
+    w.V = d.template_vertex_count;
+    w.T = d.template_face_count;
+    w.Vt = d.target_vertex_count;
+    w.F = d.target_face_count;
+    w.L = d.landmark_count > 0 ? d.landmark_count : 0;
+    w.template_in.assign(d.template_points, d.template_points + (size_t)w.V * 3);
+    w.target_in.assign(d.target_points, d.target_points + (size_t)w.Vt * 3);
+    w.template_faces.assign(d.template_faces, d.template_faces + (size_t)w.T * 3);
+    w.target_faces.assign(d.target_faces, d.target_faces + (size_t)w.F * 3);
+    if (d.mask) {
+        w.mask.resize(w.V);
+        for (int i = 0; i < w.V; ++i) w.mask[i] = d.mask[i] ? 1 : 0;
+    }
+    if (w.L > 0) {
+        w.landmark_indices.assign(d.landmark_indices, d.landmark_indices + w.L);
+        w.landmark_targets_in.assign(d.landmark_targets, d.landmark_targets + (size_t)w.L * 3);
+    }
+    if (d.level_setting_count > 0) {
+        w.level_settings.assign(d.levels, d.levels + d.level_setting_count);
+    } else {
+        NricpLevelSettings s;
+        nricp_default_level(&s);
+        w.level_settings.push_back(s);
+    }
+    w.desc.levels = w.level_settings.data();
+    w.desc.level_setting_count = static_cast<int>(w.level_settings.size());
+    w.desc.template_points = w.template_in.data();
+    w.desc.target_points = w.target_in.data();
+    w.desc.template_faces = w.template_faces.data();
+    w.desc.target_faces = w.target_faces.data();
+    w.desc.mask = w.mask.empty() ? nullptr : w.mask.data();
+    w.desc.landmark_indices = w.L ? w.landmark_indices.data() : nullptr;
+    w.desc.landmark_targets = w.L ? w.landmark_targets_in.data() : nullptr;
+    w.desc.landmark_count = w.L;
+}
+
+void prepare_host(Wrap& w) {
+    const NricpSolveDesc& d = w.desc;
+    const int k = d.max_nodes_per_vertex > 0 ? d.max_nodes_per_vertex : 4;
+    const int edge_k = d.edge_neighbours > 0 ? d.edge_neighbours : 4;
+    w.graph = build_template_graph(d.template_points, w.V, d.graph_levels, d.nodes_initial,
+                                   d.growth, k, edge_k);
+    w.levels = static_cast<int>(w.graph.levels.size());
+    w.layouts.clear();
+    for (int l = 0; l < w.levels; ++l) {
+        w.layouts.push_back(build_layout(w.graph, l, w.V));
+        const LevelLayout& L = w.layouts.back();
+        w.max_nodes = std::max(w.max_nodes, L.node_count);
+        w.max_edges = std::max(w.max_edges, L.edge_count);
+        w.max_pairs = std::max(w.max_pairs, L.pair_count);
+        w.max_offdiag = std::max(w.max_offdiag, L.edge_count + L.pair_count);
+    }
+}
+
+size_t bytes_of_layout(const LevelLayout& L) {
+    return 256 * 24 + sizeof(double) * (L.rest.size() + L.bind_weights.size() + L.transfer_weights.size()) +
+           sizeof(int32_t) * (L.bind_nodes.size() + L.bind_counts.size() + L.gather_begin.size() +
+                              L.gather_entry.size() + L.node_edge_begin.size() +
+                              L.node_edge_list.size() + L.edges.size() + L.pair_nodes.size() +
+                              L.pair_begin.size() + L.pair_entry.size() + L.row_begin.size() +
+                              L.row_entry.size() + L.offdiag_nodes.size() + L.transfer_nodes.size() +
+                              L.transfer_counts.size());
+}
+
+// Lays out, allocates and fills the wrap's device arena; builds the target's
+// hierarchy.  `control` is this wrap's slot in the batch's control array.
+void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
+    const NricpSolveDesc& d = w.desc;
+    const int V = w.V, N = std::max(1, w.max_nodes), B = std::max(1, w.max_offdiag);
+    Arena& a = w.arena;
+    // template and target
+    const size_t o_tpl = a.reserve(sizeof(double) * 3 * V);
+    const size_t o_tpl_faces = a.reserve(sizeof(int32_t) * 3 * w.T);
+    std::vector<int32_t> vf_begin, vf_list;
+    vertex_faces(w.template_faces.data(), w.T, V, vf_begin, vf_list);
+    const size_t o_vf_begin = a.reserve(sizeof(int32_t) * vf_begin.size());
+    const size_t o_vf_list = a.reserve(sizeof(int32_t) * std::max<size_t>(1, vf_list.size()));
+    const size_t o_mask = a.reserve(w.mask.empty() ? 0 : V);
+    const size_t o_lm_target = a.reserve(sizeof(double) * 3 * V);
+    const size_t o_lm_flag = a.reserve(V);
+    const size_t o_lm_vertices = a.reserve(sizeof(int32_t) * std::max(1, w.L));
+    const size_t o_tgt = a.reserve(sizeof(double) * 3 * w.Vt);
+    const size_t o_tgt_normals = a.reserve(sizeof(double) * 3 * w.Vt);
+    const size_t o_tgt_faces = a.reserve(sizeof(int32_t) * 3 * w.F);
+    const size_t o_bvh_nodes = a.reserve(sizeof(float4) * 4 * std::max(1, w.F - 1));
+    const size_t o_bvh_leaves = a.reserve(sizeof(float4) * 3 * w.F);
+    // levels
+    std::vector<size_t> level_base(w.levels);
+    for (int l = 0; l < w.levels; ++l) level_base[l] = a.reserve(bytes_of_layout(w.layouts[l]));
+    // state and scratch
+    size_t o_rot[2], o_trans[2], o_diag[2], o_rhs[2], o_off[2];
+    for (int i = 0; i < 2; ++i) {
+        o_rot[i] = a.reserve(sizeof(double) * 9 * N);
+        o_trans[i] = a.reserve(sizeof(double) * 3 * N);
+        o_diag[i] = a.reserve(sizeof(float) * 36 * N);
+        o_rhs[i] = a.reserve(sizeof(float) * 6 * N);
+        o_off[i] = a.reserve(sizeof(float) * 36 * B);
+    }
+    const size_t o_rot32 = a.reserve(sizeof(float) * 9 * N);
+    const size_t o_deformed = a.reserve(sizeof(double) * 3 * V);
+    const size_t o_deformed32 = a.reserve(sizeof(float4) * V);
+    const size_t o_qn = a.reserve(sizeof(double) * 3 * V);
+    const size_t o_cp = a.reserve(sizeof(double) * 3 * V);
+    const size_t o_cn = a.reserve(sizeof(double) * 3 * V);
+    const size_t o_cd = a.reserve(sizeof(double) * V);
+    const size_t o_ct = a.reserve(sizeof(int32_t) * V);
+    const size_t o_cc = a.reserve(V);
+    const size_t o_rb = a.reserve(sizeof(double) * V);
+    const size_t o_r0 = a.reserve(sizeof(float4) * V);
+    const size_t o_r1 = a.reserve(sizeof(float4) * V);
+    const size_t o_r2 = a.reserve(sizeof(float4) * V);
+    const size_t o_factor = a.reserve(sizeof(float) * 36 * N);
+    const size_t o_delta = a.reserve(sizeof(double) * 6 * N);
+    const size_t o_x = a.reserve(sizeof(double) * 6 * N);
+    const size_t o_r = a.reserve(sizeof(double) * 6 * N);
+    const size_t o_p = a.reserve(sizeof(float) * 6 * N);
+    const size_t o_ap = a.reserve(sizeof(float) * 6 * N);
+    const int vblocks = (V + 255) / 256;
+    const size_t o_part = a.reserve(sizeof(double) * kPartialStride * std::max(1, vblocks));
+    const size_t o_epart = a.reserve(sizeof(double) * std::max(1, (w.max_edges + 127) / 128));
+    const size_t o_npart = a.reserve(sizeof(double) * std::max(1, (N + 7) / 8));
+    const size_t o_records = a.reserve(sizeof(LevelRecord) * w.levels);
+    const size_t o_lstats = a.reserve(sizeof(CorrStats) * w.levels);
+    const size_t o_fstats = a.reserve(sizeof(CorrStats));
+    a.allocate();
+
+    // ---- fill the descriptor ----
+    WrapDev& D = w.dev;
+    std::memset(&D, 0, sizeof D);
+    D.V = V; D.T = w.T; D.Vt = w.Vt; D.F = w.F; D.L = w.L;
+    D.max_nodes = w.max_nodes; D.max_offdiag = w.max_offdiag; D.max_pairs = w.max_pairs;
+    D.max_edges = w.max_edges; D.energy_blocks = vblocks;
+    const double units = w.graph.scale;
+    for (int l = 0; l < kMaxLevels; ++l) {
+        const NricpLevelSettings& s =
+            w.level_settings[std::min<size_t>(l, w.level_settings.size() - 1)];
+        D.weights[l][0] = s.point_to_point; D.weights[l][1] = s.point_to_plane;
+        D.weights[l][2] = s.smoothness; D.weights[l][3] = s.anchor; D.weights[l][4] = s.landmark;
+        D.robust_kernel[l] = s.robust_kernel;
+        D.robust_threshold[l] = s.robust_threshold > 0.0 ? s.robust_threshold * units : s.robust_threshold;
+        D.max_outer[l] = std::max(1, s.max_outer_iterations);
+        D.max_inner[l] = std::max(1, s.max_inner_iterations);
+        D.outer_tol[l] = s.outer_tolerance;
+        D.inner_tol[l] = s.inner_tolerance;
+    }
+    D.distance_threshold = d.distance_threshold * units;  // bindings.cpp:631-639
+    D.min_normal_cosine = d.min_normal_cosine;
+    D.min_slope = d.min_slope;
+    D.initial_damping = d.initial_damping;
+    D.damping_decrease = d.damping_decrease;
+    D.damping_increase = d.damping_increase;
+    D.max_attempts = std::max(1, d.max_damping_attempts);
+    D.diagonal_damping = d.diagonal_damping ? 1 : 0;
+    D.pcg_max_iterations = std::max(1, d.pcg_max_iterations);
+    D.pcg_tolerance = d.pcg_tolerance;
+
+    // template and target, normalised with the template's frame
+    const std::vector<double> tpl = normalized(w.template_in.data(), V, w.graph.center, w.graph.scale);
+    const std::vector<double> tgt = normalized(w.target_in.data(), w.Vt, w.graph.center, w.graph.scale);
+    const std::vector<double> tgt_normals = vertex_normals(tgt, w.target_faces.data(), w.F);
+    std::vector<double> lm_target(static_cast<size_t>(V) * 3, 0.0);
+    std::vector<uint8_t> lm_flag(V, 0);
+    for (int i = 0; i < w.L; ++i) {
+        const int v = w.landmark_indices[i];
+        lm_flag[v] = 1;
+        for (int k = 0; k < 3; ++k)
+            lm_target[v * 3 + k] = (w.landmark_targets_in[i * 3 + k] - w.graph.center[k]) * w.graph.scale;
+    }
+    D.tpl = a.at<double>(o_tpl);
+    D.tpl_faces = a.at<int32_t>(o_tpl_faces);
+    D.vf_begin = a.at<int32_t>(o_vf_begin);
+    D.vf_faces = a.at<int32_t>(o_vf_list);
+    D.mask = w.mask.empty() ? nullptr : a.at<uint8_t>(o_mask);
+    D.lm_target = a.at<double>(o_lm_target);
+    D.lm_flag = a.at<uint8_t>(o_lm_flag);
+    D.lm_vertices = a.at<int32_t>(o_lm_vertices);
+    D.tgt_points = a.at<double>(o_tgt);
+    D.tgt_normals = a.at<double>(o_tgt_normals);
+    D.tgt_faces = a.at<int32_t>(o_tgt_faces);
+    D.bvh_nodes = a.at<float4>(o_bvh_nodes);
+    D.bvh_leaves = a.at<float4>(o_bvh_leaves);
+    D.rank_window = static_cast<float>(kRankWindow * target_diagonal(tgt));
+    upload(const_cast<double*>(D.tpl), tpl, stream);
+    upload(const_cast<int32_t*>(D.tpl_faces), w.template_faces, stream);
+    upload(const_cast<int32_t*>(D.vf_begin), vf_begin, stream);
+    upload(const_cast<int32_t*>(D.vf_faces), vf_list, stream);
+    if (D.mask) upload(const_cast<uint8_t*>(D.mask), w.mask, stream);
+    upload(const_cast<double*>(D.lm_target), lm_target, stream);
+    upload(const_cast<uint8_t*>(D.lm_flag), lm_flag, stream);
+    upload(const_cast<int32_t*>(D.lm_vertices), w.landmark_indices, stream);
+    upload(const_cast<double*>(D.tgt_points), tgt, stream);
+    upload(const_cast<double*>(D.tgt_normals), tgt_normals, stream);
+    upload(const_cast<int32_t*>(D.tgt_faces), w.target_faces, stream);
+
+    for (int l = 0; l < w.levels; ++l) {
+        const LevelLayout& L = w.layouts[l];
+        LevelDev& G = D.levels[l];
+        char* base = a.at<char>(level_base[l]);
+        auto put = [&](const auto& vec) {
+            using T = typename std::decay_t<decltype(vec)>::value_type;
+            T* p = reinterpret_cast<T*>(base);
+            base += (sizeof(T) * vec.size() + 255) & ~size_t(255);
+            upload(p, vec, stream);
+            return p;
+        };
+        G.node_count = L.node_count;
+        G.edge_count = L.edge_count;
+        G.pair_count = L.pair_count;
+        G.offdiag_count = L.edge_count + L.pair_count;
+        G.rest = put(L.rest);
+        G.bind_nodes = put(L.bind_nodes);
+        G.bind_weights = put(L.bind_weights);
+        G.bind_counts = put(L.bind_counts);
+        G.gather_begin = put(L.gather_begin);
+        G.gather_entry = put(L.gather_entry);
+        G.node_edge_begin = put(L.node_edge_begin);
+        G.node_edge_list = put(L.node_edge_list);
+        G.edges = put(L.edges);
+        G.pair_nodes = put(L.pair_nodes);
+        G.pair_begin = put(L.pair_begin);
+        G.pair_entry = put(L.pair_entry);
+        G.row_begin = put(L.row_begin);
+        G.row_entry = put(L.row_entry);
+        G.offdiag_nodes = put(L.offdiag_nodes);
+        G.transfer_nodes = put(L.transfer_nodes);
+        G.transfer_weights = put(L.transfer_weights);
+        G.transfer_counts = put(L.transfer_counts);
+    }
+    for (int i = 0; i < 2; ++i) {
+        D.rot[i] = a.at<double>(o_rot[i]);
+        D.trans[i] = a.at<double>(o_trans[i]);
+        D.diag[i] = a.at<float>(o_diag[i]);
+        D.rhs[i] = a.at<float>(o_rhs[i]);
+        D.offdiag[i] = a.at<float>(o_off[i]);
+    }
+    D.rot32 = a.at<float>(o_rot32);
+    D.deformed = a.at<double>(o_deformed);
+    D.deformed32 = a.at<float4>(o_deformed32);
+    D.qnormals = a.at<double>(o_qn);
+    D.corr_point = a.at<double>(o_cp);
+    D.corr_normal = a.at<double>(o_cn);
+    D.corr_distance = a.at<double>(o_cd);
+    D.corr_triangle = a.at<int32_t>(o_ct);
+    D.corr_code = a.at<uint8_t>(o_cc);
+    D.robust = a.at<double>(o_rb);
+    D.residual32 = a.at<float4>(o_r0);
+    D.resid_aux32 = a.at<float4>(o_r1);
+    D.lm_resid32 = a.at<float4>(o_r2);
+    D.factor = a.at<float>(o_factor);
+    D.delta = a.at<double>(o_delta);
+    D.pcg_x = a.at<double>(o_x);
+    D.pcg_r = a.at<double>(o_r);
+    D.pcg_p = a.at<float>(o_p);
+    D.pcg_ap = a.at<float>(o_ap);
+    D.partials = a.at<double>(o_part);
+    D.edge_partials = a.at<double>(o_epart);
+    D.node_partials = a.at<double>(o_npart);
+    D.records = a.at<LevelRecord>(o_records);
+    D.level_stats = a.at<CorrStats>(o_lstats);
+    D.final_stats = a.at<CorrStats>(o_fstats);
+    D.control = control;
+    w.control = control;
+
+}
+
+// Puts a wrap back at the start of its schedule: identity transforms, no
+// previous correspondences, and a freshly built hierarchy of its target.  Runs
+// on the device only (the inputs are already resident).
+void reset_device(Wrap& w, cudaStream_t stream, LbvhExport* lbvh_out) {
+    WrapDev& D = w.dev;
+    const int V = w.V, N = std::max(1, w.max_nodes);
+    if (w.identity_rot == nullptr) {
+        std::vector<double> rot(static_cast<size_t>(N) * 9, 0.0);
+        for (int n = 0; n < N; ++n) rot[n * 9] = rot[n * 9 + 4] = rot[n * 9 + 8] = 1.0;
+        std::vector<LevelRecord> records(w.levels);
+        std::memset(records.data(), 0, sizeof(LevelRecord) * records.size());
+        for (int l = 0; l < w.levels; ++l) {
+            records[l].level = l;
+            records[l].nodes = w.layouts[l].node_count;
+        }
+        check(cudaMalloc(&w.identity_rot, sizeof(double) * rot.size() + sizeof(LevelRecord) * records.size()),
+              "cudaMalloc(initial state)");
+        check(cudaMemcpy(w.identity_rot, rot.data(), sizeof(double) * rot.size(), cudaMemcpyHostToDevice),
+              "initial state");
+        w.initial_records = reinterpret_cast<LevelRecord*>(w.identity_rot + rot.size());
+        check(cudaMemcpy(w.initial_records, records.data(), sizeof(LevelRecord) * records.size(),
+                         cudaMemcpyHostToDevice), "initial records");
+    }
+    check(cudaMemcpyAsync(D.rot[0], w.identity_rot, sizeof(double) * 9 * N, cudaMemcpyDeviceToDevice, stream),
+          "init rot");
+    check(cudaMemsetAsync(D.trans[0], 0, sizeof(double) * 3 * N, stream), "init trans");
+    check(cudaMemsetAsync(D.corr_triangle, 0xff, sizeof(int32_t) * V, stream), "init corr");
+    check(cudaMemsetAsync(D.corr_code, 0, V, stream), "init code");
+    check(cudaMemcpyAsync(D.records, w.initial_records, sizeof(LevelRecord) * w.levels,
+                          cudaMemcpyDeviceToDevice, stream), "init records");
+    check(cudaMemsetAsync(D.level_stats, 0, sizeof(CorrStats) * w.levels, stream), "init stats");
+    check(cudaMemsetAsync(D.final_stats, 0, sizeof(CorrStats), stream), "init stats");
+    WrapControl& c = w.initial_control;
+    std::memset(&c, 0, sizeof c);
+    c.phase = kPhaseRefresh;
+    c.route = w.desc.route;
+    c.level = 0;
+    c.level_count = w.levels;
+    c.damping = w.desc.initial_damping;
+    check(cudaMemcpyAsync(w.control, &c, sizeof c, cudaMemcpyHostToDevice, stream), "init control");
+
+    // the target's hierarchy, in a scratch that lives only for the build
+    void* scratch = nullptr;
+    check(cudaMallocAsync(&scratch, lbvh_scratch_bytes(w.F), stream), "cudaMallocAsync(lbvh scratch)");
+    const uint32_t root = lbvh_build(D.tgt_points, D.tgt_faces, w.F, scratch,
+                                     const_cast<float4*>(D.bvh_nodes), const_cast<float4*>(D.bvh_leaves),
+                                     stream, lbvh_out);
+    check(cudaGetLastError(), "lbvh build");
+    check(cudaFreeAsync(scratch, stream), "cudaFreeAsync(lbvh scratch)");
+    D.bvh_root = static_cast<int>(root);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Batch
+// ---------------------------------------------------------------------------
+Batch::Batch() {
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+Batch::~Batch() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    wraps_.clear();
+    if (dev_wraps_) cudaFree(dev_wraps_);
+    if (dev_controls_) cudaFree(dev_controls_);
+    if (host_controls_) cudaFreeHost(host_controls_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Batch::add(const NricpSolveDesc& desc) {
+    NricpSolveDesc d = desc;
+    validate_settings(d);
+    auto w = std::make_unique<Wrap>();
+    const double t0 = now_seconds();
+    copy_inputs(*w, d);
+    prepare_host(*w);
+    w->setup_seconds = now_seconds() - t0;
+    wraps_.push_back(std::move(w));
+}
+
+void Batch::upload_all(LbvhExport* lbvh_out) {
+    const int W = static_cast<int>(wraps_.size());
+    check(cudaMalloc(&dev_controls_, sizeof(WrapControl) * W), "cudaMalloc(controls)");
+    check(cudaMallocHost(&host_controls_, sizeof(WrapControl) * W), "cudaMallocHost(controls)");
+    shape_ = TickShape{};
+    shape_.wraps = W;
+    for (int i = 0; i < W; ++i) {
+        Wrap& w = *wraps_[i];
+        const double t0 = now_seconds();
+        prepare_device(w, dev_controls_ + i, stream_);
+        reset_device(w, stream_, i == 0 ? lbvh_out : nullptr);
+        w.setup_seconds += now_seconds() - t0;
+        shape_.max_vertices = std::max(shape_.max_vertices, w.V);
+        shape_.max_nodes = std::max(shape_.max_nodes, w.max_nodes);
+        shape_.max_edges = std::max(shape_.max_edges, w.max_edges);
+        shape_.max_pairs = std::max(shape_.max_pairs, w.max_pairs);
+    }
+    check(cudaMalloc(&dev_wraps_, sizeof(WrapDev) * W), "cudaMalloc(wraps)");
+    std::vector<WrapDev> host(W);
+    for (int i = 0; i < W; ++i) host[i] = wraps_[i]->dev;
+    check(cudaMemcpyAsync(dev_wraps_, host.data(), sizeof(WrapDev) * W, cudaMemcpyHostToDevice, stream_),
+          "upload wraps");
+    check(cudaStreamSynchronize(stream_), "prepare");
+    const double t = now_seconds();
+    for (auto& w : wraps_) w->solve_started = t;
+}
+
+void Batch::reset() {
+    check(cudaStreamSynchronize(stream_), "reset");
+    for (auto& w : wraps_) {
+        reset_device(*w, stream_, nullptr);
+        w->solve_seconds = 0.0;
+    }
+    ticks_ = 0;
+    launches_ = 0;
+    const double t = now_seconds();
+    for (auto& w : wraps_) w->solve_started = t;
+}
+
+void Batch::tick(KernelTimers* timers) {
+    launch_tick(dev_wraps_, shape_, stream_, timers);
+    check(cudaGetLastError(), "tick launch");
+    ticks_ += 1;
+    launches_ += tick_kernel_launches(shape_);
+}
+
+void Batch::pull_controls() {
+    check(cudaMemcpyAsync(host_controls_, dev_controls_, sizeof(WrapControl) * wraps_.size(),
+                          cudaMemcpyDeviceToHost, stream_), "pull controls");
+    check(cudaStreamSynchronize(stream_), "tick");
+}
+
+bool Batch::all_done() const {
+    for (size_t i = 0; i < wraps_.size(); ++i)
+        if (host_controls_[i].phase != kPhaseDone) return false;
+    return true;
+}
+
+void Batch::run(int max_ticks) {
+    if (!graph_exec_) {
+        cudaGraph_t graph = nullptr;
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+        launch_tick(dev_wraps_, shape_, stream_, nullptr);
+        check(cudaStreamEndCapture(stream_, &graph), "capture end");
+        check(cudaGraphInstantiate(&graph_exec_, graph, 0), "graph instantiate");
+        cudaGraphDestroy(graph);
+    }
+    pull_controls();
+    int chunk = 4;
+    while (!all_done()) {
+        if (ticks_ >= max_ticks) throw StateError("the schedule did not finish within the tick limit");
+        for (int i = 0; i < chunk; ++i) {
+            check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+            ticks_ += 1;
+            launches_ += tick_kernel_launches(shape_);
+        }
+        pull_controls();
+        chunk = std::min(chunk * 2, 16);
+    }
+    finish();
+}
+
+void Batch::run_timed(KernelTimers* timers, std::vector<float>* query_ms, std::vector<float>* pcg_ms,
+                      std::vector<float>* assemble_ms, int max_ticks) {
+    pull_controls();
+    while (!all_done()) {
+        if (ticks_ >= max_ticks) throw StateError("the schedule did not finish within the tick limit");
+        tick(timers);
+        pull_controls();
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, timers->query_begin, timers->query_end);
+        query_ms->push_back(ms);
+        cudaEventElapsedTime(&ms, timers->pcg_begin, timers->pcg_end);
+        pcg_ms->push_back(ms);
+        cudaEventElapsedTime(&ms, timers->assemble_begin, timers->assemble_end);
+        assemble_ms->push_back(ms);
+    }
+    finish();
+}
+
+void Batch::finish() {
+    const double t = now_seconds();
+    for (size_t i = 0; i < wraps_.size(); ++i) {
+        if (host_controls_[i].error)
+            throw StateError("a closest-point traversal exceeded its stack; the hierarchy is too deep");
+        if (wraps_[i]->solve_seconds == 0.0) wraps_[i]->solve_seconds = t - wraps_[i]->solve_started;
+    }
+}
+
+const WrapControl& Batch::control(int i) const { return host_controls_[i]; }
+
+// Result of wrap `i` in the caller's units (route_result_to_dict,
+// src/python/bindings.cpp:674-710).
+void Batch::result(int i, NricpResult* out) {
+    Wrap& w = *wraps_[i];
+    const WrapControl& c = host_controls_[i];
+    const int level = std::min(c.level, w.levels - 1);
+    const int N = w.layouts[level].node_count;
+    std::vector<double> rot(static_cast<size_t>(N) * 9), trans(static_cast<size_t>(N) * 3);
+    check(cudaMemcpyAsync(rot.data(), w.dev.rot[c.state], sizeof(double) * rot.size(),
+                          cudaMemcpyDeviceToHost, stream_), "download rot");
+    check(cudaMemcpyAsync(trans.data(), w.dev.trans[c.state], sizeof(double) * trans.size(),
+                          cudaMemcpyDeviceToHost, stream_), "download trans");
+    std::vector<LevelRecord> records(w.levels);
+    std::vector<CorrStats> lstats(w.levels);
+    CorrStats fstats;
+    check(cudaMemcpyAsync(records.data(), w.dev.records, sizeof(LevelRecord) * w.levels,
+                          cudaMemcpyDeviceToHost, stream_), "download records");
+    check(cudaMemcpyAsync(lstats.data(), w.dev.level_stats, sizeof(CorrStats) * w.levels,
+                          cudaMemcpyDeviceToHost, stream_), "download stats");
+    check(cudaMemcpyAsync(&fstats, w.dev.final_stats, sizeof(CorrStats), cudaMemcpyDeviceToHost,
+                          stream_), "download stats");
+    check(cudaStreamSynchronize(stream_), "download");
+    const std::vector<double> vertices = evaluate_host(i, rot, trans, level);
+    if (out->vertices) std::memcpy(out->vertices, vertices.data(), sizeof(double) * vertices.size());
+    if (out->rotations) std::memcpy(out->rotations, rot.data(), sizeof(double) * rot.size());
+    if (out->translations) std::memcpy(out->translations, trans.data(), sizeof(double) * trans.size());
+    if (out->node_positions)
+        std::memcpy(out->node_positions, w.layouts[level].rest.data(), sizeof(double) * 3 * N);
+    if (out->level_nodes)
+        for (int l = 0; l < w.levels; ++l) out->level_nodes[l] = w.layouts[l].node_count;
+    // The report: levels run so far, the final correspondence statistics
+    // (route_a.cpp:40-63) and the accepted energy's five parts.
+    std::vector<LevelView> views;
+    const int shown = c.phase == kPhaseDone || c.phase == kPhaseFinal ? w.levels : c.level + 1;
+    for (int l = 0; l < shown && l < w.levels; ++l) {
+        const LevelRecord& r = records[l];
+        views.push_back({l, r.nodes, r.outer_iterations, r.inner_iterations, r.converged,
+                         r.energy_start, r.energy_end, r.correspondence_mean});
+    }
+    const CorrStats& s = c.phase == kPhaseDone ? fstats : lstats[std::max(0, c.level - 1)];
+    const StatsView stats{s.total, s.accepted, s.rejected_distance, s.rejected_normal,
+                          s.rejected_slope, s.rejected_masked, s.mean, s.p95, s.max};
+    const std::string json = report_json(c.route == 0 ? "route_b" : "route_c", "float",
+                                         c.energy_parts, stats, views, w.desc, w.graph.scale,
+                                         w.setup_seconds, w.solve_seconds);
+    out->report_length = json.size();
+    if (out->report_json && out->report_capacity > 0) {
+        const size_t n = std::min(json.size(), out->report_capacity - 1);
+        std::memcpy(out->report_json, json.data(), n);
+        out->report_json[n] = 0;
+    }
+}
+
+// v' = sum w (R (v - g) + g + t), then back to the caller's units
+// (mesh.cpp:189-193).
+std::vector<double> Batch::evaluate_host(int i, const std::vector<double>& rot,
+                                         const std::vector<double>& trans, int level) const {
+    const Wrap& w = *wraps_[i];
+    const LevelLayout& L = w.layouts[level];
+    const std::vector<double> tpl = normalized(w.template_in.data(), w.V, w.graph.center, w.graph.scale);
+    std::vector<double> out(static_cast<size_t>(w.V) * 3);
+    for (int v = 0; v < w.V; ++v) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < L.bind_counts[v]; ++k) {
+            const int j = L.bind_nodes[v * NRICP_MAX_SLOTS + k];
+            const double wt = L.bind_weights[v * NRICP_MAX_SLOTS + k];
+            const double* g = &L.rest[j * 3];
+            const double* R = &rot[j * 9];
+            const double p[3] = {tpl[v * 3] - g[0], tpl[v * 3 + 1] - g[1], tpl[v * 3 + 2] - g[2]};
+            for (int r = 0; r < 3; ++r) {
+                const double a = R[r * 3] * p[0] + R[r * 3 + 1] * p[1] + R[r * 3 + 2] * p[2];
+                s[r] = s[r] + ((a + g[r]) + trans[j * 3 + r]) * wt;
+            }
+        }
+        for (int r = 0; r < 3; ++r) out[v * 3 + r] = s[r] / w.graph.scale + w.graph.center[r];
+    }
+    return out;
+}
+
+int Batch::finest_nodes(int i) const { return wraps_[i]->layouts.back().node_count; }
+int Batch::levels(int i) const { return wraps_[i]->levels; }
+int Batch::vertices(int i) const { return wraps_[i]->V; }
+
+void Batch::current_vertices(int i, double* out) {
+    pull_controls();
+    const WrapControl& c = host_controls_[i];
+    Wrap& w = *wraps_[i];
+    const int level = std::min(c.level, w.levels - 1);
+    // a level whose warm start has not run yet still holds the previous one
+    const int shown = c.phase == kPhaseTransfer ? level - 1 : level;
+    const int N = w.layouts[shown].node_count;
+    std::vector<double> rot(static_cast<size_t>(N) * 9), trans(static_cast<size_t>(N) * 3);
+    check(cudaMemcpyAsync(rot.data(), w.dev.rot[c.state], sizeof(double) * rot.size(),
+                          cudaMemcpyDeviceToHost, stream_), "download rot");
+    check(cudaMemcpyAsync(trans.data(), w.dev.trans[c.state], sizeof(double) * trans.size(),
+                          cudaMemcpyDeviceToHost, stream_), "download trans");
+    check(cudaStreamSynchronize(stream_), "download");
+    const std::vector<double> v = evaluate_host(i, rot, trans, shown);
+    std::memcpy(out, v.data(), sizeof(double) * v.size());
+}
+
+const WrapDev* Batch::device_wrap(int i) const { return dev_wraps_ + i; }
+
+}  // namespace nricp_b200

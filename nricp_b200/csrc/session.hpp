@@ -1,0 +1,83 @@
+// Host orchestration of one batch of wraps on one device stream.
+#pragma once
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/nricp_b200.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nricp_b200 {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t status, const char* what);
+
+struct Wrap;
+
+class Batch {
+public:
+    Batch();
+    ~Batch();
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+
+    // Host preparation of one more wrap (validation, graph, layouts).
+    void add(const NricpSolveDesc& desc);
+    // Device arenas, uploads, hierarchies; after this the batch can tick.
+    void upload_all(LbvhExport* lbvh_out = nullptr);
+    // Back to the start of every wrap's schedule, inputs kept resident
+    // (device work only: state reset and the targets' hierarchies rebuilt).
+    void reset();
+    // One tick for every wrap (eager launches, optional kernel timers).
+    void tick(KernelTimers* timers = nullptr);
+    // Ticks (as a replayed CUDA graph) until every wrap is done.
+    void run(int max_ticks = 1 << 20);
+    // Eager ticks with per-tick kernel timing of the dominant kernels.
+    void run_timed(KernelTimers* timers, std::vector<float>* query_ms, std::vector<float>* pcg_ms,
+                   std::vector<float>* assemble_ms, int max_ticks = 1 << 20);
+    void pull_controls();
+    bool all_done() const;
+    void finish();
+
+    int size() const { return static_cast<int>(wraps_.size()); }
+    const WrapControl& control(int i) const;
+    void result(int i, NricpResult* out);
+    void current_vertices(int i, double* out);
+    int finest_nodes(int i) const;
+    int levels(int i) const;
+    int vertices(int i) const;
+    long ticks() const { return ticks_; }
+    long launches() const { return launches_; }
+    const TickShape& shape() const { return shape_; }
+    cudaStream_t stream() const { return stream_; }
+    const WrapDev* device_wrap(int i) const;
+
+private:
+    std::vector<double> evaluate_host(int i, const std::vector<double>& rot,
+                                      const std::vector<double>& trans, int level) const;
+
+    std::vector<std::unique_ptr<Wrap>> wraps_;
+    cudaStream_t stream_ = nullptr;
+    WrapDev* dev_wraps_ = nullptr;
+    WrapControl* dev_controls_ = nullptr;
+    WrapControl* host_controls_ = nullptr;
+    TickShape shape_{};
+    cudaGraphExec_t graph_exec_ = nullptr;
+    long ticks_ = 0;
+    long launches_ = 0;
+};
+
+extern thread_local std::string g_last_error;
+
+}  // namespace nricp_b200

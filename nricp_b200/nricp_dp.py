@@ -1,0 +1,269 @@
+"""Drop-in for the reference's `nricp_dp` extension module (route B / route C).
+
+Same function names, positional and keyword arguments, defaults, result
+dictionaries and error types as src/python/bindings.cpp:714-1623 for the
+device routes:
+
+* ``solve_route_b`` / ``solve_route_c`` (bindings.cpp:1422-1492)
+* ``RouteBSession`` with ``step``, ``finished``, ``vertices``, ``report``,
+  ``result`` (bindings.cpp:1510-1612)
+* ``device_info``, ``build_info``, ``build_template_graph``, ``closest_points``,
+  ``normalization``, ``bounding_box_diagonal``, ``validate_mesh``
+
+plus, beyond the reference, ``solve_batch`` (many uneven wraps advanced by the
+same kernel launches) and the keyword extensions ``max_nodes_per_vertex``
+(k <= 8 bindings) and ``edge_neighbours`` (k-NN graph edges).
+
+Everything below is argument marshalling; the work happens in the CUDA
+library through its C ABI.  The FP64 route A lives only in the test oracle.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, load
+
+__version__ = "0.1.0"
+
+_ROUTES = {"route_b": _abi.ROUTE_B, "route_c": _abi.ROUTE_C}
+
+
+def _plan(desc: _abi.Desc) -> list[int]:
+    counts = (C.c_int32 * 64)()
+    levels = C.c_int()
+    check(load().nricp_plan(C.byref(desc.struct), counts, 64, C.byref(levels)))
+    return [counts[i] for i in range(levels.value)]
+
+
+def _solve(route: str, template_points, template_faces, target_points, target_faces,
+           level_settings, **kwargs) -> dict:
+    desc = _abi.Desc(template_points, template_faces, target_points, target_faces,
+                     level_settings, route=_ROUTES[route], **kwargs)
+    out = _abi.ResultBuffers(desc.template_points.shape[0], _plan(desc))
+    check(load().nricp_solve(C.byref(desc.struct), C.byref(out.struct)))
+    return out.to_dict()
+
+
+def solve_route_b(template_points, template_faces, target_points, target_faces,
+                  level_settings, **kwargs) -> dict:
+    """Fit the template onto the target and return the result plus the run
+    report.  Distances (distance_threshold, robust_threshold) are given in the
+    caller's units and converted into the solver's normalized frame
+    internally; the caller hands in the template and target already aligned to
+    each other."""
+    return _solve("route_b", template_points, template_faces, target_points, target_faces,
+                  level_settings, **kwargs)
+
+
+def solve_route_c(template_points, template_faces, target_points, target_faces,
+                  level_settings, **kwargs) -> dict:
+    """Route C: the same schedule solved by the global/local alternation."""
+    return _solve("route_c", template_points, template_faces, target_points, target_faces,
+                  level_settings, **kwargs)
+
+
+def solve_batch(cases, route: str = "route_b") -> list[dict]:
+    """Many wraps at once: every case is ``(template_points, template_faces,
+    target_points, target_faces, level_settings, kwargs)``.  The wraps may
+    differ in every size; they share the device launches."""
+    descs = [_abi.Desc(*case[:5], route=_ROUTES[route], **(case[5] if len(case) > 5 else {}))
+             for case in cases]
+    outs = [_abi.ResultBuffers(d.template_points.shape[0], _plan(d)) for d in descs]
+    array = (_abi.SolveDesc * len(descs))(*[d.struct for d in descs])
+    results = (_abi.Result * len(outs))(*[o.struct for o in outs])
+    check(load().nricp_batch_solve(array, len(descs), results))
+    return [o.to_dict() for o in outs]
+
+
+class RouteBSession:
+    """The device schedule with the caller holding the loop: construct the
+    session, then call step() until finished().  `route` selects 'route_b'
+    (the default) or 'route_c'."""
+
+    def __init__(self, template_points, template_faces, target_points, target_faces,
+                 level_settings, route: str = "route_b", **kwargs):
+        if route not in _ROUTES:
+            raise ValueError(f"the device session runs 'route_b' or 'route_c', not '{route}'")
+        self._desc = _abi.Desc(template_points, template_faces, target_points, target_faces,
+                               level_settings, route=_ROUTES[route], **kwargs)
+        self._levels = _plan(self._desc)
+        self._handle = C.c_void_p()
+        check(load().nricp_session_create(C.byref(self._desc.struct), C.byref(self._handle)))
+
+    def __del__(self):
+        handle = getattr(self, "_handle", None)
+        if handle:
+            load().nricp_session_destroy(handle)
+            self._handle = None
+
+    def step(self) -> dict:
+        """Advance the schedule by one unit of work and report where it got to."""
+        p = _abi.Progress()
+        check(load().nricp_session_step(self._handle, C.byref(p)))
+        return {"level": p.level, "outer": p.outer, "inner": p.inner,
+                "finished": bool(p.finished), "level_converged": bool(p.level_converged),
+                "energy": p.energy, "correspondence_mean": p.correspondence_mean}
+
+    def finished(self) -> bool:
+        done = C.c_int()
+        check(load().nricp_session_finished(self._handle, C.byref(done)))
+        return bool(done.value)
+
+    def run(self) -> None:
+        """Steps until finished without a host round trip between steps."""
+        check(load().nricp_session_run(self._handle))
+
+    def vertices(self) -> np.ndarray:
+        """The template as it currently stands, for redrawing between steps."""
+        out = np.zeros_like(self._desc.template_points)
+        check(load().nricp_session_vertices(self._handle, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def result(self) -> dict:
+        out = _abi.ResultBuffers(self._desc.template_points.shape[0], self._levels)
+        check(load().nricp_session_result(self._handle, C.byref(out.struct)))
+        return out.to_dict()
+
+    def report(self) -> str:
+        return self.result()["report"]
+
+    def ticks(self) -> tuple[int, int]:
+        t, l = C.c_long(), C.c_long()
+        check(load().nricp_session_ticks(self._handle, C.byref(t), C.byref(l)))
+        return t.value, l.value
+
+
+def device_info() -> dict:
+    """Report whether the accelerated path can run here, and on what."""
+    available = C.c_int()
+    text = C.create_string_buffer(256)
+    check(load().nricp_device_info(C.byref(available), text, 256))
+    return {"available": bool(available.value), "device": text.value.decode()}
+
+
+def build_info() -> dict:
+    return {"version": __version__, "build_type": "Release", "cxx_compiler": "GNU (via nvcc)",
+            "cuda_toolkit": "12.9", "cuda_architectures": "100a",
+            "accelerated_precision": "float"}
+
+
+def _points(a, name):
+    out = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if out.ndim != 2 or out.shape[1] != 3:
+        raise ValueError(f"{name} must have shape (n, 3)")
+    return out
+
+
+def _faces(a, name):
+    out = np.asarray(a)
+    if out.ndim != 2 or out.shape[1] != 3:
+        raise ValueError(f"{name} must have shape (n, 3)")
+    return np.ascontiguousarray(out.astype(np.int64).astype(np.int32))
+
+
+def bounding_box_diagonal(points) -> float:
+    p = _points(points, "points")
+    return float(np.linalg.norm(p.max(0) - p.min(0))) if len(p) else 0.0
+
+
+def normalization(points) -> dict:
+    """Centering and scaling that puts the bounding-box diagonal at 1
+    (src/core/mesh.cpp:174-181)."""
+    p = _points(points, "points")
+    if len(p) == 0:
+        return {"center": np.zeros((1, 3)), "scale": 1.0}
+    lo, hi = p.min(0), p.max(0)
+    center = (lo + hi) * 0.5
+    d = hi - lo
+    diagonal = math.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+    return {"center": center[None, :], "scale": 1.0 / diagonal if diagonal > 0 else 1.0}
+
+
+def validate_mesh(points, faces) -> dict:
+    """Structural validation (src/core/mesh.cpp:90-116)."""
+    p, f = _points(points, "points"), np.asarray(faces)
+    problems = []
+    if len(p) == 0:
+        problems.append("mesh has no vertices")
+    if len(f) == 0:
+        problems.append("mesh has no faces; closest-point queries need a surface")
+    for i in np.nonzero(~np.isfinite(p).all(1))[0]:
+        problems.append(f"vertex {i} is not finite")
+    if len(f):
+        bad = (f < 0) | (f >= len(p))
+        for i, k in zip(*np.nonzero(bad)):
+            problems.append(f"face {i} corner {k} index {f[i, k]} is out of range")
+    return {"ok": not problems, "problems": problems}
+
+
+def build_template_graph(points, faces, levels: int = 4, nodes_initial: int = 100,
+                         growth: int = 2, max_nodes_per_vertex: int = 4,
+                         use_device: bool = False, edge_neighbours: int = 4) -> dict:
+    """The cached template side: nodes, bindings and edges per level
+    (bindings.cpp:886-925).  Built with the reference's FP64 rules, so it is
+    identical to the reference's graph whichever `use_device` says."""
+    p, f = _points(points, "points"), _faces(faces, "faces")
+    report = validate_mesh(p, f)
+    if not report["ok"]:
+        raise ValueError("invalid mesh: " + "; ".join(report["problems"]))
+    lib = load()
+    n = len(p)
+    level_count = max(1, int(levels))
+    out_levels = []
+    center = np.zeros(3)
+    scale = C.c_double()
+    for level in range(level_count):
+        g = float(max(1, growth)) ** level
+        nodes = min(max(1, int(math.floor(nodes_initial * g + 0.5))), n)
+        idx = np.zeros(nodes, dtype=np.int32)
+        pos = np.zeros((nodes, 3))
+        bn = np.zeros((n, _abi.MAX_SLOTS), dtype=np.int32)
+        bw = np.zeros((n, _abi.MAX_SLOTS))
+        bc = np.zeros(n, dtype=np.int32)
+        cap = max(1, nodes * max(1, edge_neighbours))
+        edges = np.zeros((cap, 2), dtype=np.int32)
+        count = C.c_int()
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+        check(lib.nricp_template_graph_level(
+            P(p, C.c_double), n, level_count, nodes_initial, growth, max_nodes_per_vertex,
+            edge_neighbours, level, P(center, C.c_double), C.byref(scale), P(idx, C.c_int32),
+            P(pos, C.c_double), P(bn, C.c_int32), P(bw, C.c_double), P(bc, C.c_int32),
+            P(edges, C.c_int32), cap, C.byref(count)))
+        support = max(4, int(max_nodes_per_vertex))
+        out_levels.append({
+            "node_positions": pos,
+            "node_template_indices": idx.astype(np.int64),
+            "bindings": {"nodes": bn[:, :support].astype(np.int64), "weights": bw[:, :support],
+                         "counts": bc.astype(np.int64)},
+            "edges": edges[:count.value].astype(np.int64),
+        })
+    return {"normalization": {"center": center[None, :].copy(), "scale": scale.value},
+            "levels": out_levels}
+
+
+def closest_points(target_points, target_faces, query_points) -> dict:
+    """Closest point and interpolated normal on the target surface, through
+    the device hierarchy."""
+    p, f, q = _points(target_points, "target_points"), _faces(target_faces, "target_faces"), \
+        _points(query_points, "query_points")
+    n = len(q)
+    out = {"points": np.zeros((n, 3)), "normals": np.zeros((n, 3)), "distances": np.zeros(n),
+           "triangles": np.zeros(n, dtype=np.int32)}
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    check(load().nricp_closest_points(P(p, C.c_double), len(p), P(f, C.c_int32), len(f),
+                                      P(q, C.c_double), n, P(out["points"], C.c_double),
+                                      P(out["normals"], C.c_double),
+                                      P(out["distances"], C.c_double),
+                                      P(out["triangles"], C.c_int32)))
+    out["triangles"] = out["triangles"].astype(np.int64)
+    return out
+
+
+def serialize_report(report: str) -> dict:
+    return json.loads(report)

@@ -1,0 +1,5 @@
+"""`import nricp_dp` for callers of the reference's extension module: the
+B200 implementation of its route B / route C surface (nricp_b200.nricp_dp)."""
+
+from nricp_b200.nricp_dp import *  # noqa: F401,F403
+from nricp_b200.nricp_dp import __version__  # noqa: F401

@@ -1,0 +1,272 @@
+"""Python access to the oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two interchangeable checkers with one interface:
+
+* ``Oracle("restatement")`` -- the plain-C restatement (oracle/nricp_oracle.c),
+  built on demand with gcc.  Always available.
+* ``Oracle("reference")`` -- the reference's own route A compiled from its
+  sources (oracle/_ref/libnricp_ref.so, see oracle/build.py); available where
+  that library was built.
+
+Only tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, and only as the checker.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+
+from nricp_b200 import _abi  # noqa: E402
+
+from . import build  # noqa: E402
+
+ROUTE_A = 0
+ROUTE_C = 1
+
+_LIBS: dict[str, C.CDLL] = {}
+
+
+def _load(kind: str) -> C.CDLL:
+    if kind in _LIBS:
+        return _LIBS[kind]
+    if kind == "restatement":
+        path = build.build_oracle()
+        prefix = "oracle_"
+    elif kind == "reference":
+        path = build.REF_LIB
+        if not path.exists():
+            built = build.build_reference()
+            if built is None:
+                raise FileNotFoundError("the reference's route A is not built here")
+        prefix = "ref_"
+    else:
+        raise ValueError(kind)
+    lib = C.CDLL(str(path))
+    lib._prefix = prefix  # type: ignore[attr-defined]
+    _LIBS[kind] = lib
+    return lib
+
+
+def reference_available() -> bool:
+    try:
+        _load("reference")
+        return True
+    except (FileNotFoundError, OSError):
+        return False
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a).astype(np.int32))
+
+
+def _p(a: np.ndarray, ctype=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Oracle:
+    def __init__(self, kind: str = "restatement"):
+        self.kind = kind
+        self.lib = _load(kind)
+        self._prefix = self.lib._prefix
+
+    def _fn(self, name: str):
+        return getattr(self.lib, self._prefix + name)
+
+    # ---- whole wrap ------------------------------------------------------
+    def solve(self, template_points, template_faces, target_points, target_faces,
+              level_settings, route: int = ROUTE_A, **kwargs) -> dict:
+        """route_a (or the FP64 route C restatement) with the route functions'
+        signature (src/python/bindings.cpp:1426-1481); returns the same dict."""
+        desc = _abi.Desc(template_points, template_faces, target_points, target_faces,
+                         level_settings, route=0, **kwargs)
+        out = _abi.ResultBuffers(desc.template_points.shape[0], desc.level_node_counts())
+        if self.kind == "reference":
+            if route != ROUTE_A:
+                raise ValueError("the reference has no CPU route C")
+            fn = self.lib.ref_solve_route_a
+            fn.argtypes = [C.POINTER(_abi.SolveDesc), C.POINTER(_abi.Result)]
+            status = fn(C.byref(desc.struct), C.byref(out.struct))
+            if status:
+                self.lib.ref_last_error.restype = C.c_char_p
+                raise (ValueError if status == _abi.ERR_INVALID else RuntimeError)(
+                    self.lib.ref_last_error().decode())
+        else:
+            fn = self.lib.oracle_solve
+            fn.argtypes = [C.POINTER(_abi.SolveDesc), C.c_int, C.POINTER(_abi.Result)]
+            status = fn(C.byref(desc.struct), route, C.byref(out.struct))
+            if status:
+                self.lib.oracle_last_error.restype = C.c_char_p
+                raise (ValueError if status == _abi.ERR_INVALID else RuntimeError)(
+                    self.lib.oracle_last_error().decode())
+        return out.to_dict()
+
+    # ---- graph pieces ----------------------------------------------------
+    def normalization(self, points):
+        pts = _f64(points)
+        center = np.zeros(3)
+        scale = C.c_double()
+        self._fn("normalization")(_p(pts), C.c_int(len(pts)), _p(center), C.byref(scale))
+        return center, scale.value
+
+    def farthest_point_seeds(self, points, count: int, first_index: int = 0) -> np.ndarray:
+        pts = _f64(points)
+        out = np.zeros(max(1, count), dtype=np.int32)
+        n = self._fn("farthest_point_seeds")(_p(pts), C.c_int(len(pts)), C.c_int(count),
+                                             C.c_int(first_index), _p(out, C.c_int32))
+        return out[:n].astype(np.int64)
+
+    def bind_vertices(self, points, nodes, max_nodes: int = 4):
+        pts, nds = _f64(points), _f64(nodes)
+        n = len(pts)
+        out_nodes = np.zeros((n, _abi.MAX_SLOTS), dtype=np.int32)
+        out_weights = np.zeros((n, _abi.MAX_SLOTS))
+        out_counts = np.zeros(n, dtype=np.int32)
+        self._fn("bind_vertices")(_p(pts), C.c_int(n), _p(nds), C.c_int(len(nds)),
+                                  C.c_int(max_nodes), _p(out_nodes, C.c_int32),
+                                  _p(out_weights), _p(out_counts, C.c_int32))
+        return out_nodes, out_weights, out_counts
+
+    def node_edges(self, nodes, neighbours: int = 4) -> np.ndarray:
+        nds = _f64(nodes)
+        cap = max(1, len(nds) * neighbours)
+        out = np.zeros((cap, 2), dtype=np.int32)
+        n = self._fn("node_edges")(_p(nds), C.c_int(len(nds)), C.c_int(neighbours),
+                                   _p(out, C.c_int32), C.c_int(cap))
+        return out[:max(n, 0)].astype(np.int64)
+
+    def vertex_normals(self, points, faces) -> np.ndarray:
+        pts, fcs = _f64(points), _i32(faces)
+        out = np.zeros_like(pts)
+        self._fn("vertex_normals")(_p(pts), C.c_int(len(pts)), _p(fcs, C.c_int32),
+                                   C.c_int(len(fcs)), _p(out))
+        return out
+
+    def closest_points(self, points, faces, queries, brute: bool = False) -> dict:
+        pts, fcs, q = _f64(points), _i32(faces), _f64(queries)
+        n = len(q)
+        out = dict(points=np.zeros((n, 3)), normals=np.zeros((n, 3)),
+                   distances=np.zeros(n), triangles=np.zeros(n, dtype=np.int32))
+        self._fn("closest_points")(_p(pts), C.c_int(len(pts)), _p(fcs, C.c_int32),
+                                   C.c_int(len(fcs)), _p(q), C.c_int(n), C.c_int(int(brute)),
+                                   _p(out["points"]), _p(out["normals"]),
+                                   _p(out["distances"]), _p(out["triangles"], C.c_int32))
+        return out
+
+    # ---- assembly and solve ----------------------------------------------
+    def fused_system(self, template_points, binding_nodes, binding_weights, binding_counts,
+                     node_positions, rotations, translations, corr_points, corr_normals,
+                     corr_robust, corr_accepted, edges, landmark_indices, landmark_targets,
+                     weights, mask=None) -> dict:
+        keep = []
+
+        def hold(a):
+            keep.append(a)
+            return a
+
+        class Inputs(C.Structure):
+            _fields_ = [
+                ("template_points", C.POINTER(C.c_double)), ("vertex_count", C.c_int),
+                ("binding_nodes", C.POINTER(C.c_int32)), ("binding_weights", C.POINTER(C.c_double)),
+                ("binding_counts", C.POINTER(C.c_int32)),
+                ("node_positions", C.POINTER(C.c_double)), ("node_count", C.c_int),
+                ("rotations", C.POINTER(C.c_double)), ("translations", C.POINTER(C.c_double)),
+                ("corr_points", C.POINTER(C.c_double)), ("corr_normals", C.POINTER(C.c_double)),
+                ("corr_robust", C.POINTER(C.c_double)), ("corr_accepted", C.POINTER(C.c_uint8)),
+                ("edges", C.POINTER(C.c_int32)), ("edge_count", C.c_int),
+                ("landmark_indices", C.POINTER(C.c_int32)),
+                ("landmark_targets", C.POINTER(C.c_double)), ("landmark_count", C.c_int),
+                ("mask", C.POINTER(C.c_uint8)), ("weights", C.c_double * 5),
+            ]
+
+        tp = hold(_f64(template_points))
+        bn = hold(_i32(binding_nodes))
+        bw = hold(_f64(binding_weights))
+        bc = hold(_i32(binding_counts))
+        npos = hold(_f64(node_positions))
+        rot = hold(_f64(rotations).reshape(-1, 9))
+        tr = hold(_f64(translations))
+        cp, cn, cr = hold(_f64(corr_points)), hold(_f64(corr_normals)), hold(_f64(corr_robust))
+        ca = hold(np.ascontiguousarray(np.asarray(corr_accepted).astype(np.uint8)))
+        ed = hold(_i32(edges).reshape(-1, 2))
+        li = hold(_i32(landmark_indices).reshape(-1))
+        lt = hold(_f64(landmark_targets).reshape(-1, 3))
+        mk = hold(np.ascontiguousarray(np.asarray(mask).astype(np.uint8))) if mask is not None else None
+        x = Inputs()
+        x.template_points, x.vertex_count = _p(tp), len(tp)
+        x.binding_nodes, x.binding_weights = _p(bn, C.c_int32), _p(bw)
+        x.binding_counts = _p(bc, C.c_int32)
+        x.node_positions, x.node_count = _p(npos), len(npos)
+        x.rotations, x.translations = _p(rot), _p(tr)
+        x.corr_points, x.corr_normals, x.corr_robust = _p(cp), _p(cn), _p(cr)
+        x.corr_accepted = _p(ca, C.c_uint8)
+        x.edges, x.edge_count = _p(ed, C.c_int32), len(ed)
+        x.landmark_indices, x.landmark_targets = _p(li, C.c_int32), _p(lt)
+        x.landmark_count = len(li)
+        x.mask = _p(mk, C.c_uint8) if mk is not None else C.POINTER(C.c_uint8)()
+        for i in range(5):
+            x.weights[i] = float(weights[i])
+        n = len(npos)
+        cap = max(16, len(tp) * 16 + len(ed) + 16)
+        diag = np.zeros((n, 6, 6))
+        rhs = np.zeros((n, 6))
+        oa = np.zeros(cap, dtype=np.int32)
+        ob = np.zeros(cap, dtype=np.int32)
+        ob_blocks = np.zeros((cap, 6, 6))
+        count = C.c_int()
+        energies = np.zeros(5)
+        status = self._fn("fused_system")(C.byref(x), _p(diag), _p(rhs), _p(oa, C.c_int32),
+                                          _p(ob, C.c_int32), _p(ob_blocks), C.c_int(cap),
+                                          C.byref(count), _p(energies))
+        if status:
+            raise RuntimeError("fused_system capacity")
+        k = count.value
+        return dict(diagonal=diag, rhs=rhs, edges=np.stack([oa[:k], ob[:k]], 1).astype(np.int64),
+                    edge_blocks=ob_blocks[:k].copy(), energies=energies)
+
+    def solve_direct(self, diagonal, edges, edge_blocks, rhs, damping=0.0,
+                     diagonal_scaling=True):
+        lib = _load("restatement")
+        d = _f64(diagonal).reshape(-1, 36)
+        e = _i32(edges).reshape(-1, 2)
+        a, b = np.ascontiguousarray(e[:, 0]), np.ascontiguousarray(e[:, 1])
+        blocks = _f64(edge_blocks).reshape(-1, 36)
+        r = _f64(rhs).reshape(-1)
+        delta = np.zeros_like(r)
+        ok = lib.oracle_solve_direct(C.c_int(len(d)), _p(d), C.c_int(len(a)), _p(a, C.c_int32),
+                                     _p(b, C.c_int32), _p(blocks), _p(r), C.c_double(damping),
+                                     C.c_int(int(diagonal_scaling)), _p(delta))
+        return bool(ok), delta.reshape(-1, 6)
+
+    def lbvh_build(self, points_f32, faces):
+        lib = _load("restatement")
+        pts = np.ascontiguousarray(np.asarray(points_f32, dtype=np.float32))
+        fcs = _i32(faces)
+        n = len(fcs)
+        codes = np.zeros(n, dtype=np.uint32)
+        order = np.zeros(n, dtype=np.uint32)
+        left = np.zeros(max(1, n - 1), dtype=np.int32)
+        right = np.zeros(max(1, n - 1), dtype=np.int32)
+        bounds = np.zeros(6, dtype=np.float32)
+        lib.oracle_lbvh_build(pts.ctypes.data_as(C.POINTER(C.c_float)), C.c_int(len(pts)),
+                              _p(fcs, C.c_int32), C.c_int(n), _p(codes, C.c_uint32),
+                              _p(order, C.c_uint32), _p(left, C.c_int32), _p(right, C.c_int32),
+                              bounds.ctypes.data_as(C.POINTER(C.c_float)))
+        return dict(codes=codes, order=order, left=left[: max(0, n - 1)],
+                    right=right[: max(0, n - 1)], bounds=bounds)
+
+    def horn_rotation(self, correlation) -> np.ndarray:
+        lib = _load("restatement")
+        c = _f64(correlation).reshape(9)
+        out = np.zeros(9)
+        lib.oracle_horn_rotation(_p(c), _p(out))
+        return out.reshape(3, 3)
