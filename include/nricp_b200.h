@@ -143,6 +143,10 @@ typedef struct NricpProgress {
  * raises as ValueError / RuntimeError). */
 const char* nricp_last_error(void);
 
+/* Bytes this thread has copied host->device and device->host through the
+ * library since the last reset (no reference counterpart; for accounting). */
+int nricp_transfer_counters(unsigned long long* h2d, unsigned long long* d2h, int reset);
+
 /* device_info(), src/python/bindings.cpp:1614-1622. */
 int nricp_device_info(int* available, char* description, size_t capacity);
 
@@ -199,6 +203,24 @@ int nricp_batch_counters(NricpBatch* batch, long* ticks, long* launches);
  * linear solve and the assembly of every tick; totals in milliseconds. */
 int nricp_batch_profile(NricpBatch* batch, double* query_ms, double* pcg_ms,
                         double* assemble_ms, long* ticks);
+/* Device time (CUDA events on the batch's stream) of one full pass: every
+ * wrap reset to the start of its schedule (hierarchies rebuilt) and run to
+ * completion.  Inputs stay resident in device memory. */
+int nricp_batch_step(NricpBatch* batch, double* device_ms);
+/* Per-tick records of wrap 0 from the last nricp_batch_profile. */
+typedef struct NricpTickRecord {
+    int phase;          /* 0 transfer, 1 refresh, 2 solve, 3 final */
+    int level;
+    int pcg_iterations; /* of this tick's solve */
+    int pad;
+    float query_ms, pcg_ms, assemble_ms, tick_ms;
+} NricpTickRecord;
+int nricp_batch_tick_records(NricpBatch* batch, NricpTickRecord* out, int capacity,
+                             int* count);
+/* Sizes of one level of one wrap: nodes, smoothness edges, node-pair groups,
+ * (vertex, slot) entries, pair entries, template vertices, target triangles,
+ * target vertices, template triangles, level count. */
+int nricp_batch_level_sizes(NricpBatch* batch, int index, int level, int32_t* sizes);
 void nricp_batch_destroy(NricpBatch* batch);
 /* One call: create, run, results, destroy. */
 int nricp_batch_solve(const NricpSolveDesc* descs, int count, NricpResult* results);

@@ -108,6 +108,14 @@ class Progress(C.Structure):
     ]
 
 
+class TickRecord(C.Structure):
+    _fields_ = [
+        ("phase", C.c_int), ("level", C.c_int), ("pcg_iterations", C.c_int), ("pad", C.c_int),
+        ("query_ms", C.c_float), ("pcg_ms", C.c_float), ("assemble_ms", C.c_float),
+        ("tick_ms", C.c_float),
+    ]
+
+
 # Defaults of the route functions, src/python/bindings.cpp:1470-1481.
 ROUTE_DEFAULTS: dict[str, Any] = dict(
     mask=None,

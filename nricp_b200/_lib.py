@@ -41,6 +41,7 @@ def _declare(lib: C.CDLL) -> None:
     desc_p, result_p = P(_abi.SolveDesc), P(_abi.Result)
     sig = {
         "nricp_last_error": (C.c_char_p, []),
+        "nricp_transfer_counters": (C.c_int, [P(C.c_ulonglong), P(C.c_ulonglong), C.c_int]),
         "nricp_device_info": (C.c_int, [P(C.c_int), C.c_char_p, C.c_size_t]),
         "nricp_plan": (C.c_int, [desc_p, i32p, C.c_int, P(C.c_int)]),
         "nricp_solve": (C.c_int, [desc_p, result_p]),
@@ -59,6 +60,9 @@ def _declare(lib: C.CDLL) -> None:
         "nricp_batch_counters": (C.c_int, [C.c_void_p, P(C.c_long), P(C.c_long)]),
         "nricp_batch_profile": (C.c_int, [C.c_void_p, dp, dp, dp, P(C.c_long)]),
         "nricp_batch_destroy": (None, [C.c_void_p]),
+        "nricp_batch_step": (C.c_int, [C.c_void_p, dp]),
+        "nricp_batch_tick_records": (C.c_int, [C.c_void_p, P(_abi.TickRecord), C.c_int, P(C.c_int)]),
+        "nricp_batch_level_sizes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, i32p]),
         "nricp_batch_solve": (C.c_int, [desc_p, C.c_int, result_p]),
         "nricp_template_graph_level": (C.c_int, [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                                  C.c_int, C.c_int, dp, dp, i32p, dp, i32p, dp, i32p,

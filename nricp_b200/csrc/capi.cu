@@ -109,6 +109,13 @@ void nricp_default_desc(NricpSolveDesc* d) {
 
 const char* nricp_last_error(void) { return g_last_error.c_str(); }
 
+int nricp_transfer_counters(unsigned long long* h2d, unsigned long long* d2h, int reset) {
+    *h2d = g_transfers.h2d;
+    *d2h = g_transfers.d2h;
+    if (reset) g_transfers = TransferCounters{};
+    return NRICP_OK;
+}
+
 int nricp_device_info(int* available, char* description, size_t capacity) {
     return guarded([&] {
         int count = 0;
@@ -269,6 +276,36 @@ int nricp_batch_profile(NricpBatch* b, double* query_ms, double* pcg_ms, double*
         cudaEventDestroy(t.query_begin); cudaEventDestroy(t.query_end);
         cudaEventDestroy(t.pcg_begin); cudaEventDestroy(t.pcg_end);
         cudaEventDestroy(t.assemble_begin); cudaEventDestroy(t.assemble_end);
+    });
+}
+
+int nricp_batch_step(NricpBatch* b, double* device_ms) {
+    return guarded([&] { *device_ms = b->batch.timed_step(); });
+}
+
+int nricp_batch_tick_records(NricpBatch* b, NricpTickRecord* out, int capacity, int* count) {
+    return guarded([&] {
+        const auto& records = b->batch.tick_records();
+        *count = static_cast<int>(records.size());
+        for (int i = 0; i < *count && i < capacity; ++i) {
+            out[i].phase = records[i].phase;
+            out[i].level = records[i].level;
+            out[i].pcg_iterations = records[i].pcg_iterations;
+            out[i].query_ms = records[i].query_ms;
+            out[i].pcg_ms = records[i].pcg_ms;
+            out[i].assemble_ms = records[i].assemble_ms;
+            out[i].tick_ms = records[i].tick_ms;
+        }
+    });
+}
+
+int nricp_batch_level_sizes(NricpBatch* b, int index, int level, int32_t* sizes) {
+    return guarded([&] {
+        if (index < 0 || index >= b->batch.size()) throw InvalidArgument("wrap index out of range");
+        if (level < 0 || level >= b->batch.levels(index)) throw InvalidArgument("level out of range");
+        int v[10];
+        b->batch.level_sizes(index, level, v);
+        for (int i = 0; i < 10; ++i) sizes[i] = v[i];
     });
 }
 

@@ -56,8 +56,10 @@ struct LevelDev {
     // off-diagonal row lists for the matvec: for each node, the blocks that
     // touch it; entry = block * 2 + (1 if the node is the block's b side)
     const int32_t* row_begin;      // N + 1
-    const int32_t* row_entry;
+    const int32_t* row_entry;      // pairs: (block * 2 + side, other node)
     const int32_t* offdiag_nodes;  // offdiag_count x 2 (edges first, then pairs)
+    const int32_t* offdiag_slots;  // offdiag_count x 2: row-entry slots of B (a) and B^T (b)
+    int row_entries;               // 2 x offdiag_count
     // warm start from the previous level (level > 0): 4 source nodes + weights
     const int32_t* transfer_nodes;   // N x 4
     const double* transfer_weights;  // N x 4
@@ -166,9 +168,12 @@ struct WrapDev {
     // systems: two buffers, `control.system` selects the current one
     float* diag[2];               // N x 36
     float* rhs[2];                // N x 6
-    float* offdiag[2];            // max_offdiag x 36
+    float* offdiag[2];            // 2 x max_offdiag x 36, in row-entry order:
+                                  // slot j holds the block of row list entry j
+                                  // (B for the a side, B^T for the b side)
     // solve scratch
-    float* factor;                // N x 36 (lower Cholesky)
+    float* factor;                // N x 36: inverse of the damped diagonal block
+    float* damped;                // N x 36: damped diagonal blocks
     double* delta;                // N x 6
     double* pcg_x;                // N x 6
     double* pcg_r;                // N x 6

@@ -414,12 +414,20 @@ LevelLayout build_layout(const TemplateGraph& graph, int level, int V) {
         L.row_begin[L.offdiag_nodes[k * 2 + 1] + 1]++;
     }
     for (int n = 0; n < N; ++n) L.row_begin[n + 1] += L.row_begin[n];
-    L.row_entry.assign(L.row_begin[N], 0);
+    // entry pairs: (block * 2 + side, the other node of the block)
+    L.row_entry.assign(static_cast<size_t>(L.row_begin[N]) * 2, 0);
+    L.offdiag_slots.assign(static_cast<size_t>(B) * 2, 0);
     {
         std::vector<int32_t> cursor(L.row_begin.begin(), L.row_begin.end() - 1);
         for (int k = 0; k < B; ++k) {
-            L.row_entry[cursor[L.offdiag_nodes[k * 2]]++] = k * 2;
-            L.row_entry[cursor[L.offdiag_nodes[k * 2 + 1]]++] = k * 2 + 1;
+            const int a = L.offdiag_nodes[k * 2], b = L.offdiag_nodes[k * 2 + 1];
+            const int ia = cursor[a]++, ib = cursor[b]++;
+            L.row_entry[ia * 2] = k * 2;
+            L.row_entry[ia * 2 + 1] = b;
+            L.row_entry[ib * 2] = k * 2 + 1;
+            L.row_entry[ib * 2 + 1] = a;
+            L.offdiag_slots[k * 2] = ia;       // block k, as seen from a: B
+            L.offdiag_slots[k * 2 + 1] = ib;   // and from b: B^T
         }
     }
     // warm start from the previous level (deformation.cpp:141-160): the new

@@ -47,7 +47,7 @@ struct LevelLayout {
     std::vector<int32_t> gather_begin, gather_entry;
     std::vector<int32_t> node_edge_begin, node_edge_list, edges;
     std::vector<int32_t> pair_nodes, pair_begin, pair_entry;
-    std::vector<int32_t> row_begin, row_entry, offdiag_nodes;
+    std::vector<int32_t> row_begin, row_entry, offdiag_nodes, offdiag_slots;
     std::vector<int32_t> transfer_nodes, transfer_counts;
     std::vector<double> transfer_weights;
 };

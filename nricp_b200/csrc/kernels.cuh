@@ -36,6 +36,8 @@ struct TickShape {
     int energy_blocks;   // vertex-pass blocks per wrap (partials written)
     int edge_blocks;
     int node_blocks;
+    int pcg_cluster;     // CTAs per wrap in the cluster solve
+    int pcg_shared_bytes;  // direction staged in shared memory
 };
 
 // Device timing hooks for the dominant kernels (CUDA events on the launching
@@ -50,6 +52,8 @@ struct KernelTimers {
 void launch_tick(const WrapDev* wraps, const TickShape& shape, cudaStream_t stream,
                  KernelTimers* timers);
 int tick_kernel_launches(const TickShape& shape);
+int pcg_cluster_size(int max_nodes);
+int pcg_shared_bytes(int max_nodes);
 void launch_evaluate_state(const WrapDev* wraps, const TickShape& shape, cudaStream_t stream);
 
 }  // namespace nricp_b200

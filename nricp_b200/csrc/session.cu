@@ -26,6 +26,7 @@
 namespace nricp_b200 {
 
 thread_local std::string g_last_error;
+thread_local TransferCounters g_transfers;
 
 void check(cudaError_t status, const char* what) {
     if (status != cudaSuccess)
@@ -80,9 +81,11 @@ double target_diagonal(const std::vector<double>& p) {
 
 template <typename T>
 void upload(T* dst, const std::vector<T>& src, cudaStream_t stream) {
-    if (!src.empty())
+    if (!src.empty()) {
         check(cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, stream),
               "upload");
+        g_transfers.h2d += sizeof(T) * src.size();
+    }
 }
 
 }  // namespace
@@ -174,12 +177,13 @@ void prepare_host(Wrap& w) {
 }
 
 size_t bytes_of_layout(const LevelLayout& L) {
-    return 256 * 24 + sizeof(double) * (L.rest.size() + L.bind_weights.size() + L.transfer_weights.size()) +
+    return 256 * 26 + sizeof(double) * (L.rest.size() + L.bind_weights.size() + L.transfer_weights.size()) +
            sizeof(int32_t) * (L.bind_nodes.size() + L.bind_counts.size() + L.gather_begin.size() +
                               L.gather_entry.size() + L.node_edge_begin.size() +
                               L.node_edge_list.size() + L.edges.size() + L.pair_nodes.size() +
                               L.pair_begin.size() + L.pair_entry.size() + L.row_begin.size() +
-                              L.row_entry.size() + L.offdiag_nodes.size() + L.transfer_nodes.size() +
+                              L.row_entry.size() + L.offdiag_nodes.size() + L.offdiag_slots.size() +
+                              L.transfer_nodes.size() +
                               L.transfer_counts.size());
 }
 
@@ -215,7 +219,7 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
         o_trans[i] = a.reserve(sizeof(double) * 3 * N);
         o_diag[i] = a.reserve(sizeof(float) * 36 * N);
         o_rhs[i] = a.reserve(sizeof(float) * 6 * N);
-        o_off[i] = a.reserve(sizeof(float) * 36 * B);
+        o_off[i] = a.reserve(sizeof(float) * 36 * 2 * B);
     }
     const size_t o_rot32 = a.reserve(sizeof(float) * 9 * N);
     const size_t o_deformed = a.reserve(sizeof(double) * 3 * V);
@@ -231,6 +235,7 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     const size_t o_r1 = a.reserve(sizeof(float4) * V);
     const size_t o_r2 = a.reserve(sizeof(float4) * V);
     const size_t o_factor = a.reserve(sizeof(float) * 36 * N);
+    const size_t o_damped = a.reserve(sizeof(float) * 36 * N);
     const size_t o_delta = a.reserve(sizeof(double) * 6 * N);
     const size_t o_x = a.reserve(sizeof(double) * 6 * N);
     const size_t o_r = a.reserve(sizeof(double) * 6 * N);
@@ -343,6 +348,8 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
         G.row_begin = put(L.row_begin);
         G.row_entry = put(L.row_entry);
         G.offdiag_nodes = put(L.offdiag_nodes);
+        G.offdiag_slots = put(L.offdiag_slots);
+        G.row_entries = static_cast<int>(L.row_entry.size() / 2);
         G.transfer_nodes = put(L.transfer_nodes);
         G.transfer_weights = put(L.transfer_weights);
         G.transfer_counts = put(L.transfer_counts);
@@ -368,6 +375,7 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     D.resid_aux32 = a.at<float4>(o_r1);
     D.lm_resid32 = a.at<float4>(o_r2);
     D.factor = a.at<float>(o_factor);
+    D.damped = a.at<float>(o_damped);
     D.delta = a.at<double>(o_delta);
     D.pcg_x = a.at<double>(o_x);
     D.pcg_r = a.at<double>(o_r);
@@ -436,6 +444,10 @@ void reset_device(Wrap& w, cudaStream_t stream, LbvhExport* lbvh_out) {
     D.bvh_root = static_cast<int>(root);
 }
 
+// Kernels one hierarchy build launches (lbvh_build): centroids, two bound
+// passes, Morton codes, 8 radix passes of 3 kernels, Karras, refit, 2 packs.
+int lbvh_build_launches(int n) { return 4 + 8 * 3 + (n > 1 ? 1 : 0) + 1 + (n > 1 ? 2 : 1); }
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -483,6 +495,8 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
         shape_.max_edges = std::max(shape_.max_edges, w.max_edges);
         shape_.max_pairs = std::max(shape_.max_pairs, w.max_pairs);
     }
+    shape_.pcg_cluster = pcg_cluster_size(shape_.max_nodes);
+    shape_.pcg_shared_bytes = pcg_shared_bytes(shape_.max_nodes);
     check(cudaMalloc(&dev_wraps_, sizeof(WrapDev) * W), "cudaMalloc(wraps)");
     std::vector<WrapDev> host(W);
     for (int i = 0; i < W; ++i) host[i] = wraps_[i]->dev;
@@ -550,20 +564,68 @@ void Batch::run(int max_ticks) {
 
 void Batch::run_timed(KernelTimers* timers, std::vector<float>* query_ms, std::vector<float>* pcg_ms,
                       std::vector<float>* assemble_ms, int max_ticks) {
+    records_.clear();
+    cudaEvent_t tick_begin, tick_end;
+    check(cudaEventCreate(&tick_begin), "event");
+    check(cudaEventCreate(&tick_end), "event");
     pull_controls();
     while (!all_done()) {
         if (ticks_ >= max_ticks) throw StateError("the schedule did not finish within the tick limit");
+        TickRecord r{};
+        r.phase = host_controls_[0].phase;
+        r.level = host_controls_[0].level;
+        check(cudaEventRecord(tick_begin, stream_), "event");
         tick(timers);
+        check(cudaEventRecord(tick_end, stream_), "event");
         pull_controls();
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, timers->query_begin, timers->query_end);
-        query_ms->push_back(ms);
-        cudaEventElapsedTime(&ms, timers->pcg_begin, timers->pcg_end);
-        pcg_ms->push_back(ms);
-        cudaEventElapsedTime(&ms, timers->assemble_begin, timers->assemble_end);
-        assemble_ms->push_back(ms);
+        r.pcg_iterations = r.phase == kPhaseSolve ? host_controls_[0].pcg_iterations : 0;
+        cudaEventElapsedTime(&r.query_ms, timers->query_begin, timers->query_end);
+        cudaEventElapsedTime(&r.pcg_ms, timers->pcg_begin, timers->pcg_end);
+        cudaEventElapsedTime(&r.assemble_ms, timers->assemble_begin, timers->assemble_end);
+        cudaEventElapsedTime(&r.tick_ms, tick_begin, tick_end);
+        query_ms->push_back(r.query_ms);
+        pcg_ms->push_back(r.pcg_ms);
+        assemble_ms->push_back(r.assemble_ms);
+        records_.push_back(r);
     }
+    cudaEventDestroy(tick_begin);
+    cudaEventDestroy(tick_end);
     finish();
+}
+
+double Batch::timed_step() {
+    cudaEvent_t begin, end;
+    check(cudaEventCreate(&begin), "event");
+    check(cudaEventCreate(&end), "event");
+    check(cudaStreamSynchronize(stream_), "step");
+    check(cudaEventRecord(begin, stream_), "event");
+    for (auto& w : wraps_) reset_device(*w, stream_, nullptr);
+    ticks_ = 0;
+    launches_ = 0;
+    for (auto& w : wraps_) launches_ += lbvh_build_launches(w->F);
+    run();
+    check(cudaEventRecord(end, stream_), "event");
+    check(cudaEventSynchronize(end), "step");
+    float ms = 0.0f;
+    check(cudaEventElapsedTime(&ms, begin, end), "event");
+    cudaEventDestroy(begin);
+    cudaEventDestroy(end);
+    return ms;
+}
+
+void Batch::level_sizes(int i, int level, int* sizes) const {
+    const Wrap& w = *wraps_[i];
+    const LevelLayout& L = w.layouts[level];
+    sizes[0] = L.node_count;
+    sizes[1] = L.edge_count;
+    sizes[2] = L.pair_count;
+    sizes[3] = static_cast<int>(L.gather_entry.size());
+    sizes[4] = static_cast<int>(L.pair_entry.size());
+    sizes[5] = w.V;
+    sizes[6] = w.F;
+    sizes[7] = w.Vt;
+    sizes[8] = w.T;
+    sizes[9] = w.levels;
 }
 
 void Batch::finish() {
@@ -599,6 +661,9 @@ void Batch::result(int i, NricpResult* out) {
     check(cudaMemcpyAsync(&fstats, w.dev.final_stats, sizeof(CorrStats), cudaMemcpyDeviceToHost,
                           stream_), "download stats");
     check(cudaStreamSynchronize(stream_), "download");
+    g_transfers.d2h += sizeof(double) * (rot.size() + trans.size()) +
+                       sizeof(LevelRecord) * records.size() + sizeof(CorrStats) * (lstats.size() + 1) +
+                       sizeof(WrapControl);
     const std::vector<double> vertices = evaluate_host(i, rot, trans, level);
     if (out->vertices) std::memcpy(out->vertices, vertices.data(), sizeof(double) * vertices.size());
     if (out->rotations) std::memcpy(out->rotations, rot.data(), sizeof(double) * rot.size());

@@ -46,6 +46,15 @@ public:
     // Eager ticks with per-tick kernel timing of the dominant kernels.
     void run_timed(KernelTimers* timers, std::vector<float>* query_ms, std::vector<float>* pcg_ms,
                    std::vector<float>* assemble_ms, int max_ticks = 1 << 20);
+    // Per-tick records of wrap 0 from the last run_timed.
+    struct TickRecord {
+        int phase, level, pcg_iterations, pad;
+        float query_ms, pcg_ms, assemble_ms, tick_ms;
+    };
+    const std::vector<TickRecord>& tick_records() const { return records_; }
+    // Device time of reset() + run() on the batch's stream (CUDA events).
+    double timed_step();
+    void level_sizes(int i, int level, int* sizes) const;
     void pull_controls();
     bool all_done() const;
     void finish();
@@ -74,10 +83,15 @@ private:
     WrapControl* host_controls_ = nullptr;
     TickShape shape_{};
     cudaGraphExec_t graph_exec_ = nullptr;
+    std::vector<TickRecord> records_;
     long ticks_ = 0;
     long launches_ = 0;
 };
 
 extern thread_local std::string g_last_error;
+struct TransferCounters {
+    unsigned long long h2d = 0, d2h = 0;
+};
+extern thread_local TransferCounters g_transfers;
 
 }  // namespace nricp_b200

@@ -16,7 +16,11 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
+#include <cooperative_groups.h>
+
 namespace nricp_b200 {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -598,29 +602,138 @@ __device__ inline void solve6(const float* l, const double* rhs, double* x) {
     for (int r = 0; r < 6; ++r) x[r] = z[r];
 }
 
+// One thread-block cluster per wrap (blockIdx.y): each CTA of the cluster owns
+// a contiguous slice of the nodes (rows), the search direction lives in global
+// memory (L2) where every CTA's matvec reads it, and the FP64 inner products
+// are per-CTA partials exchanged through distributed shared memory and summed
+// in rank order -- deterministic, and the same whatever else shares the
+// launch.  Hardware cluster barriers separate the four stages of an
+// iteration; nothing spins.
+// Sum of one FP64 partial per CTA of the cluster.  Warp 0 reads the ranks'
+// slots lane by lane (lanes past the cluster size read zero) and reduces them
+// with a fixed butterfly, so the total does not depend on how many CTAs the
+// launch gave the cluster beyond the ones that own rows; the rest of the CTA
+// picks it up from local shared memory.  The cluster barrier before the read
+// orders the writes (release/acquire at cluster scope, which covers global
+// memory too).
+__device__ inline double cluster_sum(cg::cluster_group& cluster, double* slot, double* out) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        double v = lane < (int)cluster.num_blocks() ? *cluster.map_shared_rank(slot, lane) : 0.0;
+        v = warp_sum(v);
+        if (lane == 0) *out = v;
+    }
+    __syncthreads();
+    return *out;
+}
+
+__device__ inline double cluster_total(cg::cluster_group& cluster, double* slot, double local,
+                                       double* scratch, double* out) {
+    const double mine = block_sum<kPcgThreads>(local, scratch);
+    if (threadIdx.x == 0) *slot = mine;
+    cluster.sync();
+    return cluster_sum(cluster, slot, out);
+}
+
+// CTAs of a wrap's cluster that own rows: a function of the wrap's own node
+// count only, so the partition -- and with it every partial sum -- is the
+// same alone and in any batch.
+__host__ __device__ inline int owner_ranks(int nodes) {
+    int ranks = 1;
+    while (ranks < 16 && ranks * 128 < nodes) ranks *= 2;
+    return ranks;
+}
+
+constexpr int kPcgSharedNodes = 4096;  // all-node direction copy in shared memory up to this N
+constexpr int kPcgSharedOwn = 256;     // and the owned rows' vectors up to this many nodes
+
+// Shared-memory layout of the solve for `nodes` nodes and `own` owned nodes.
+__host__ __device__ inline int pcg_smem_floats(int nodes, int own) {
+    return ((nodes * 6 + 3) & ~3)   // direction, every node (all CTAs' copies)
+           + own * 36 * 2           // inverse and damped diagonal blocks
+           + own * 6 * 2 * 2        // x and r (FP64)
+           + own * 6;               // Ap, then z
+}
+
+// Inverse of a 6x6 SPD block from its Cholesky factor L (lower): L^-T L^-1.
+__device__ inline void cholesky_inverse6(const float* l, float* inv) {
+    float li[36];
+    for (int i = 0; i < 36; ++i) li[i] = 0.0f;
+    for (int c = 0; c < 6; ++c) {
+        li[c * 6 + c] = 1.0f / l[c * 6 + c];
+        for (int r = c + 1; r < 6; ++r) {
+            float s = 0.0f;
+            for (int k = c; k < r; ++k) s -= l[r * 6 + k] * li[k * 6 + c];
+            li[r * 6 + c] = s / l[r * 6 + r];
+        }
+    }
+    for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < 6; ++q) {
+            float s = 0.0f;
+            for (int k = r > q ? r : q; k < 6; ++k) s += li[k * 6 + r] * li[k * 6 + q];
+            inv[r * 6 + q] = s;
+        }
+}
+
+// The damped solve (pcg_solver.cu:15-241) for one wrap per thread-block
+// cluster.  Each CTA owns a contiguous slice of the nodes and keeps that
+// slice's inverse preconditioner blocks, damped diagonal, x, r and Ap in
+// shared memory (global scratch past the size limits -- same arithmetic, same
+// order); the search direction is broadcast slice by slice into every CTA's
+// copy through distributed shared memory, so the matvec reads it locally and
+// its only L2 traffic is the off-diagonal blocks, stored in row order.
+// Three cluster barriers per iteration; FP64 dots, residual and solution.
 __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__ wraps) {
+    cg::cluster_group cluster = cg::this_cluster();
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
-    if (c.phase != kPhaseSolve) return;
+    if (c.phase != kPhaseSolve) return;  // uniform across the cluster
     const LevelDev& L = w.levels[c.level];
     const int N = L.node_count;
-    const int M = N * 6;
+    const int rank = (int)cluster.block_rank();
+    const int ranks = (int)cluster.num_blocks();
+    const int owners = min(owner_ranks(N), ranks);
+    const int per = (N + owners - 1) / owners;
+    const int n0 = rank < owners ? min(N, rank * per) : N;
+    const int n1 = rank < owners ? min(N, n0 + per) : N;
+    const int own = n1 - n0;
+    const bool in_shared = N <= kPcgSharedNodes && per <= kPcgSharedOwn;
+    extern __shared__ float4 dynamic_shared[];
+    float* base = reinterpret_cast<float*>(dynamic_shared);
+    const int pn = (N * 6 + 3) & ~3;
+    float* P = in_shared ? base : w.pcg_p;                       // all nodes
+    float* Minv = in_shared ? base + pn : w.factor + n0 * 36;     // owned
+    float* Dd = in_shared ? base + pn + per * 36 : w.damped + n0 * 36;
+    double* X = in_shared ? reinterpret_cast<double*>(base + pn + per * 72) : w.pcg_x + n0 * 6;
+    double* R = in_shared ? X + per * 6 : w.pcg_r + n0 * 6;
+    float* Aq = in_shared ? reinterpret_cast<float*>(R + per * 6) : w.pcg_ap + n0 * 6;
     const float* D = w.diag[c.system];
     const float* B = w.offdiag[c.system];
     const float* b = w.rhs[c.system];
     const float damping = (float)c.damping;
     const bool scaled = w.diagonal_damping != 0;
     __shared__ double scratch[33];
-    __shared__ int done_s;
+    __shared__ double slots[8];
+    __shared__ double totals[8];
+    const int rows = own * 6;
 
-    // damped block factors (route A's damped(): scale = max(D_rr, 1e-12))
-    for (int n = threadIdx.x; n < N; n += blockDim.x) {
+    // writes row i (global index) of the direction into every CTA's copy
+    auto broadcast = [&](int i, float value) {
+        if (in_shared) {
+            for (int q = 0; q < ranks; ++q) cluster.map_shared_rank(P, q)[i] = value;
+        } else {
+            P[i] = value;
+        }
+    };
+
+    // ---- damped diagonal blocks and their inverses (route A's damped():
+    //      scale = max(D_rr, 1e-12)); Cholesky with the reference's jitter ----
+    for (int m = threadIdx.x; m < own; m += blockDim.x) {
+        const int n = n0 + m;
         float blk[36];
         for (int i = 0; i < 36; ++i) blk[i] = D[n * 36 + i];
-        for (int r = 0; r < 6; ++r) {
-            const float s = scaled ? fmaxf(blk[r * 7], 1e-12f) : 1.0f;
-            blk[r * 7] += damping * s;
-        }
+        for (int r = 0; r < 6; ++r) blk[r * 7] += damping * (scaled ? fmaxf(blk[r * 7], 1e-12f) : 1.0f);
+        for (int i = 0; i < 36; ++i) Dd[m * 36 + i] = blk[i];
         float jitter = 0.0f;
         bool ok = false;
         for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
@@ -628,120 +741,145 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
             for (int i = 0; i < 36; ++i) cand[i] = blk[i];
             for (int r = 0; r < 6; ++r) cand[r * 7] += jitter;
             if (cholesky6(cand)) {
-                for (int i = 0; i < 36; ++i) w.factor[n * 36 + i] = cand[i];
+                cholesky_inverse6(cand, Minv + m * 36);
                 ok = true;
             }
             jitter = jitter == 0.0f ? 1e-6f : jitter * 10.0f;
         }
         if (!ok)
-            for (int i = 0; i < 36; ++i) w.factor[n * 36 + i] = (i % 7 == 0) ? 1.0f : 0.0f;
+            for (int i = 0; i < 36; ++i) Minv[m * 36 + i] = (i % 7 == 0) ? 1.0f : 0.0f;
     }
     double local_bb = 0.0;
-    for (int i = threadIdx.x; i < M; i += blockDim.x) {
-        const double bi = b[i];
-        w.pcg_x[i] = 0.0;
-        w.pcg_r[i] = bi;
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+        const double bi = b[n0 * 6 + i];
+        X[i] = 0.0;
+        R[i] = bi;
         local_bb += bi * bi;
     }
     __syncthreads();
+    // z = M^-1 r, p = z
     double local_rz = 0.0;
-    for (int n = threadIdx.x; n < N; n += blockDim.x) {
-        double z[6];
-        solve6(w.factor + n * 36, w.pcg_r + n * 6, z);
-        for (int k = 0; k < 6; ++k) {
-            w.pcg_p[n * 6 + k] = (float)z[k];
-            local_rz += w.pcg_r[n * 6 + k] * z[k];
-        }
+    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+        const int m = i / 6, r = i - m * 6;
+        const float* mi = Minv + m * 36 + r * 6;
+        float z = 0.0f;
+        for (int q = 0; q < 6; ++q) z += mi[q] * (float)R[m * 6 + q];
+        broadcast(n0 * 6 + i, z);
+        local_rz += R[i] * (double)z;
     }
-    const double bb = block_sum<kPcgThreads>(local_bb, scratch);
-    double rz = block_sum<kPcgThreads>(local_rz, scratch);
+    {
+        const double s0 = block_sum<kPcgThreads>(local_bb, scratch);
+        const double s1 = block_sum<kPcgThreads>(local_rz, scratch);
+        if (threadIdx.x == 0) { slots[0] = s0; slots[1] = s1; }
+        if (!in_shared) __threadfence();
+        cluster.sync();
+    }
+    const double bb = cluster_sum(cluster, &slots[0], &totals[0]);
+    double rz = cluster_sum(cluster, &slots[1], &totals[1]);
     const double bnorm = sqrt(bb);
     int iterations = 0;
-    bool converged = false;
+    bool converged = !(bnorm > 0.0);
     double residual = bnorm > 0.0 ? 1.0 : 0.0;
-    if (!(bnorm > 0.0)) converged = true;
+    const int2* entries = reinterpret_cast<const int2*>(L.row_entry);
     for (int it = 0; it < w.pcg_max_iterations && !converged; ++it) {
-        // Ap, and p.Ap in FP64
+        // ---- A: Ap for the owned rows, and p.Ap ----
         double local_pap = 0.0;
-        for (int i = threadIdx.x; i < M; i += blockDim.x) {
-            const int n = i / 6, r = i - n * 6;
-            const float* Dn = D + n * 36 + r * 6;
-            const float* pn = w.pcg_p + n * 6;
+        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+            const int m = i / 6, r = i - m * 6, n = n0 + m;
+            const float* dd = Dd + m * 36 + r * 6;
+            const float* pn = P + n * 6;
             float y = 0.0f;
-            for (int q = 0; q < 6; ++q) y += Dn[q] * pn[q];
-            y += damping * (scaled ? fmaxf(D[n * 36 + r * 7], 1e-12f) : 1.0f) * pn[r];
-            for (int e = L.row_begin[n]; e < L.row_begin[n + 1]; ++e) {
-                const int entry = L.row_entry[e];
-                const int blk = entry >> 1;
-                const float* Bb = B + (long)blk * 36;
-                if (entry & 1) {  // this node is the block's b side: B^T p_a
-                    const float* pa = w.pcg_p + L.offdiag_nodes[blk * 2] * 6;
-                    for (int q = 0; q < 6; ++q) y += Bb[q * 6 + r] * pa[q];
-                } else {
-                    const float* pb = w.pcg_p + L.offdiag_nodes[blk * 2 + 1] * 6;
-                    for (int q = 0; q < 6; ++q) y += Bb[r * 6 + q] * pb[q];
+            for (int q = 0; q < 6; ++q) y += dd[q] * pn[q];
+            const int e1 = L.row_begin[n + 1];
+            int e = L.row_begin[n];
+            for (; e + 4 <= e1; e += 4) {
+                float bv[4][6];
+                int nb[4];
+                for (int u = 0; u < 4; ++u) {
+                    const float* Bb = B + (long)(e + u) * 36 + r * 6;
+                    for (int q = 0; q < 6; ++q) bv[u][q] = Bb[q];
+                    nb[u] = entries[e + u].y;
+                }
+                for (int u = 0; u < 4; ++u) {
+                    const float* pm = P + nb[u] * 6;
+                    for (int q = 0; q < 6; ++q) y += bv[u][q] * pm[q];
                 }
             }
-            w.pcg_ap[i] = y;
+            for (; e < e1; ++e) {
+                const float* Bb = B + (long)e * 36 + r * 6;
+                const float* pm = P + entries[e].y * 6;
+                for (int q = 0; q < 6; ++q) y += Bb[q] * pm[q];
+            }
+            Aq[i] = y;
             local_pap += (double)pn[r] * (double)y;
         }
-        const double pap = block_sum<kPcgThreads>(local_pap, scratch);
+        const double pap = cluster_total(cluster, &slots[2], local_pap, scratch, &totals[2]);
         if (fabs(pap) < 1e-300) break;
         const double alpha = rz / pap;
+        // ---- B: x, r per owned row; z = M^-1 r; r.r and r.z together ----
         double local_rr = 0.0;
-        for (int i = threadIdx.x; i < M; i += blockDim.x) {
-            w.pcg_x[i] += alpha * (double)w.pcg_p[i];
-            const double ri = w.pcg_r[i] - alpha * (double)w.pcg_ap[i];
-            w.pcg_r[i] = ri;
+        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+            X[i] += alpha * (double)P[n0 * 6 + i];
+            const double ri = R[i] - alpha * (double)Aq[i];
+            R[i] = ri;
             local_rr += ri * ri;
         }
-        const double rr = block_sum<kPcgThreads>(local_rr, scratch);
-        iterations = it + 1;
-        residual = sqrt(rr) / bnorm;
-        if (residual <= w.pcg_tolerance) { converged = true; break; }
+        __syncthreads();
         double local_rz2 = 0.0;
-        for (int n = threadIdx.x; n < N; n += blockDim.x) {
-            double z[6];
-            solve6(w.factor + n * 36, w.pcg_r + n * 6, z);
-            for (int k = 0; k < 6; ++k) {
-                w.pcg_ap[n * 6 + k] = (float)z[k];  // reuse as z storage
-                local_rz2 += w.pcg_r[n * 6 + k] * z[k];
-            }
+        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+            const int m = i / 6, r = i - m * 6;
+            const float* mi = Minv + m * 36 + r * 6;
+            float z = 0.0f;
+            for (int q = 0; q < 6; ++q) z += mi[q] * (float)R[m * 6 + q];
+            Aq[i] = z;  // z, in the Ap storage
+            local_rz2 += R[i] * (double)z;
         }
-        const double rz_next = block_sum<kPcgThreads>(local_rz2, scratch);
+        const double s_rr = block_sum<kPcgThreads>(local_rr, scratch);
+        const double s_rz = block_sum<kPcgThreads>(local_rz2, scratch);
+        if (threadIdx.x == 0) { slots[3] = s_rr; slots[4] = s_rz; }
+        cluster.sync();
+        const double rr_total = cluster_sum(cluster, &slots[3], &totals[3]);
+        const double rz_next = cluster_sum(cluster, &slots[4], &totals[4]);
+        iterations = it + 1;
+        residual = sqrt(rr_total) / bnorm;
+        if (residual <= w.pcg_tolerance) { converged = true; break; }
+        // ---- C: the next direction, broadcast to every CTA's copy ----
         const double beta = fabs(rz) > 1e-300 ? rz_next / rz : 0.0;
         rz = rz_next;
-        for (int i = threadIdx.x; i < M; i += blockDim.x)
-            w.pcg_p[i] = (float)((double)w.pcg_ap[i] + beta * (double)w.pcg_p[i]);
-        __syncthreads();
+        for (int i = threadIdx.x; i < rows; i += blockDim.x)
+            broadcast(n0 * 6 + i, (float)((double)Aq[i] + beta * (double)P[n0 * 6 + i]));
+        if (!in_shared) __threadfence();  // the global copy: visible device-wide first
+        cluster.sync();
     }
-    if (threadIdx.x == 0) {
+    if (rank == 0 && threadIdx.x == 0) {
         w.control->pcg_ok = converged ? 1 : 0;
         w.control->pcg_iterations = iterations;
         w.control->pcg_residual = residual;
-        done_s = converged ? 1 : 0;
     }
-    __syncthreads();
-    if (!done_s) return;
-    // candidate = retract(accepted, delta): R <- exp([w]) R, t <- t + u
-    // (deformation.cpp:19-32).  Route C's rotation half is zero and its
-    // rotations were already fitted into the candidate buffer.
-    for (int n = threadIdx.x; n < N; n += blockDim.x) {
-        const double* x = w.pcg_x + n * 6;
-        const D3 tcur = load_d3(w.trans[c.state], n);
-        store_d3(w.trans[1 - c.state], n, {tcur.x + x[3], tcur.y + x[4], tcur.z + x[5]});
-        double out[9];
-        if (c.route == 0) {
-            double e[9];
-            exp_so3({x[0], x[1], x[2]}, e);
-            mat_mul(e, w.rot[c.state] + n * 9, out);
-            for (int i = 0; i < 9; ++i) w.rot[1 - c.state][n * 9 + i] = out[i];
-        } else {
-            for (int i = 0; i < 9; ++i) out[i] = w.rot[1 - c.state][n * 9 + i];
+    if (converged) {
+        // candidate = retract(accepted, delta): R <- exp([w]) R, t <- t + u
+        // (deformation.cpp:19-32).  Route C's rotation half is zero and its
+        // rotations were already fitted into the candidate buffer.
+        for (int m = threadIdx.x; m < own; m += blockDim.x) {
+            const int n = n0 + m;
+            const double* x = X + m * 6;
+            const D3 tcur = load_d3(w.trans[c.state], n);
+            store_d3(w.trans[1 - c.state], n, {tcur.x + x[3], tcur.y + x[4], tcur.z + x[5]});
+            double out[9];
+            if (c.route == 0) {
+                double e[9];
+                exp_so3({x[0], x[1], x[2]}, e);
+                mat_mul(e, w.rot[c.state] + n * 9, out);
+                for (int i = 0; i < 9; ++i) w.rot[1 - c.state][n * 9 + i] = out[i];
+            } else {
+                for (int i = 0; i < 9; ++i) out[i] = w.rot[1 - c.state][n * 9 + i];
+            }
+            for (int i = 0; i < 9; ++i) w.rot32[n * 9 + i] = (float)out[i];
+            for (int k = 0; k < 6; ++k) w.delta[n * 6 + k] = x[k];
         }
-        for (int i = 0; i < 9; ++i) w.rot32[n * 9 + i] = (float)out[i];
-        for (int k = 0; k < 6; ++k) w.delta[n * 6 + k] = x[k];
     }
+    // no CTA may exit while another can still read its shared memory
+    cluster.sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -988,17 +1126,32 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_assemble(const WrapDev* _
     if (threadIdx.x == 0) w.node_partials[blockIdx.x] = total;
 }
 
-__global__ void k_pair_assemble(const WrapDev* __restrict__ wraps) {
+// Writes block k of the system twice, in row-entry order: B where the row
+// list of node a references it, B^T where node b's does.
+__device__ inline void store_block_pair(float* out, const LevelDev& L, int k, const float* blk) {
+    float* A = out + (long)L.offdiag_slots[k * 2] * 36;
+    float* T = out + (long)L.offdiag_slots[k * 2 + 1] * 36;
+    for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < 6; ++q) {
+            A[r * 6 + q] = blk[r * 6 + q];
+            T[q * 6 + r] = blk[r * 6 + q];
+        }
+}
+
+// Warp per node pair: lanes stride over the vertices the two nodes share,
+// each lane keeps a 6x6 block in registers, one butterfly reduction.
+__global__ void __launch_bounds__(kNodeThreads) k_pair_assemble(const WrapDev* __restrict__ wraps) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
     if (!assembles(c)) return;
     const LevelDev& L = w.levels[c.level];
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (p >= L.pair_count) return;
     const int na = L.pair_nodes[p * 2], nb = L.pair_nodes[p * 2 + 1];
     float blk[36];
     for (int i = 0; i < 36; ++i) blk[i] = 0.0f;
-    for (int i = L.pair_begin[p]; i < L.pair_begin[p + 1]; ++i) {
+    for (int i = L.pair_begin[p] + lane; i < L.pair_begin[p + 1]; i += 32) {
         const int code = L.pair_entry[i];
         const int v = code >> 6, sa = (code >> 3) & 7, sb = code & 7;
         const float wa = (float)L.bind_weights[v * kMaxSlots + sa];
@@ -1033,12 +1186,12 @@ __global__ void k_pair_assemble(const WrapDev* __restrict__ wraps) {
                 for (int q = 0; q < 6; ++q) blk[r * 6 + q] += s * ua[r] * ub[q];
         }
     }
+    for (int i = 0; i < 36; ++i) blk[i] = warp_sum(blk[i]);
     if (c.route == 1)
         for (int r = 0; r < 6; ++r)
             for (int q = 0; q < 6; ++q)
                 if (r < 3 || q < 3) blk[r * 6 + q] = 0.0f;
-    float* out = w.offdiag[1 - c.system] + (long)(L.edge_count + p) * 36;
-    for (int i = 0; i < 36; ++i) out[i] = blk[i];
+    if (lane == 0) store_block_pair(w.offdiag[1 - c.system], L, L.edge_count + p, blk);
 }
 
 __global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps) {
@@ -1078,8 +1231,7 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* _
                 }
                 blk[3 * 6 + 3] = -ws; blk[4 * 6 + 4] = -ws; blk[5 * 6 + 5] = -ws;
             }
-            float* out = w.offdiag[1 - c.system] + (long)e * 36;
-            for (int i = 0; i < 36; ++i) out[i] = blk[i];
+            store_block_pair(w.offdiag[1 - c.system], L, e, blk);
         }
     }
     __shared__ double scratch[33];
@@ -1221,7 +1373,22 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     k_c_fit<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
     k_c_rhs<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
     if (timers && timers->active) cudaEventRecord(timers->pcg_begin, stream);
-    k_pcg<<<dim3(1, W), kPcgThreads, 0, stream>>>(wraps);
+    {
+        const int cluster = s.pcg_cluster;
+        cudaLaunchConfig_t config = {};
+        config.gridDim = dim3(cluster, W);
+        config.blockDim = dim3(kPcgThreads);
+        config.dynamicSmemBytes = s.pcg_shared_bytes;
+        config.stream = stream;
+        cudaLaunchAttribute attribute[1];
+        attribute[0].id = cudaLaunchAttributeClusterDimension;
+        attribute[0].val.clusterDim.x = cluster;
+        attribute[0].val.clusterDim.y = 1;
+        attribute[0].val.clusterDim.z = 1;
+        config.attrs = attribute;
+        config.numAttrs = 1;
+        cudaLaunchKernelEx(&config, k_pcg, wraps);
+    }
     if (timers && timers->active) cudaEventRecord(timers->pcg_end, stream);
     k_evaluate<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
     k_normals<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
@@ -1233,7 +1400,8 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     k_residual<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
     k_node_assemble<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
     if (s.max_pairs > 0)
-        k_pair_assemble<<<dim3(blocks_of(s.max_pairs, 128), W), 128, 0, stream>>>(wraps);
+        k_pair_assemble<<<dim3(blocks_of((long)s.max_pairs * 32, kNodeThreads), W), kNodeThreads, 0,
+                          stream>>>(wraps);
     k_edge_assemble<<<dim3(blocks_of(s.max_edges > 0 ? s.max_edges : 1, kEdgeThreads), W),
                       kEdgeThreads, 0, stream>>>(wraps);
     if (timers && timers->active) cudaEventRecord(timers->assemble_end, stream);
@@ -1241,5 +1409,30 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
 }
 
 int tick_kernel_launches(const TickShape& s) { return s.max_pairs > 0 ? 15 : 14; }
+
+// Cluster size of the solve: enough CTAs that each owns ~128 nodes, a power
+// of two, at most 16 (the non-portable maximum, enabled here).
+int pcg_cluster_size(int max_nodes) {
+    static bool enabled = false;
+    if (!enabled) {
+        cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pcg_smem_floats(kPcgSharedNodes, kPcgSharedOwn) * (int)sizeof(float));
+        enabled = true;
+    }
+    return owner_ranks(max_nodes);
+}
+
+int pcg_shared_bytes(int max_nodes) {
+    // the largest layout any wrap of this size range can need
+    int best = 0;
+    for (int n = 1; n <= max_nodes; n = n < 64 ? n + 1 : n + n / 16) {
+        const int per = (n + owner_ranks(n) - 1) / owner_ranks(n);
+        if (n <= kPcgSharedNodes && per <= kPcgSharedOwn) best = max(best, pcg_smem_floats(n, per));
+    }
+    const int n = max_nodes, per = (n + owner_ranks(n) - 1) / owner_ranks(n);
+    if (n <= kPcgSharedNodes && per <= kPcgSharedOwn) best = max(best, pcg_smem_floats(n, per));
+    return best * (int)sizeof(float);
+}
 
 }  // namespace nricp_b200

@@ -81,6 +81,78 @@ def solve_batch(cases, route: str = "route_b") -> list[dict]:
     return [o.to_dict() for o in outs]
 
 
+class WrapBatch:
+    """Many wraps resident on the device, advanced together by the same
+    launches (no reference counterpart: the reference solves one wrap per
+    call).  `cases` as for solve_batch."""
+
+    def __init__(self, cases, route: str = "route_b"):
+        self._descs = [_abi.Desc(*case[:5], route=_ROUTES[route],
+                                 **(case[5] if len(case) > 5 else {})) for case in cases]
+        self._plans = [_plan(d) for d in self._descs]
+        array = (_abi.SolveDesc * len(self._descs))(*[d.struct for d in self._descs])
+        self._handle = C.c_void_p()
+        check(load().nricp_batch_create(array, len(self._descs), C.byref(self._handle)))
+
+    def __del__(self):
+        handle = getattr(self, "_handle", None)
+        if handle:
+            load().nricp_batch_destroy(handle)
+            self._handle = None
+
+    def __len__(self):
+        return len(self._descs)
+
+    def run(self) -> None:
+        check(load().nricp_batch_run(self._handle))
+
+    def step(self) -> float:
+        """Reset every wrap and run all of them to completion; returns the
+        device time in milliseconds (CUDA events on the batch's stream)."""
+        ms = C.c_double()
+        check(load().nricp_batch_step(self._handle, C.byref(ms)))
+        return ms.value
+
+    def result(self, index: int) -> dict:
+        out = _abi.ResultBuffers(self._descs[index].template_points.shape[0], self._plans[index])
+        check(load().nricp_batch_result(self._handle, index, C.byref(out.struct)))
+        return out.to_dict()
+
+    def counters(self) -> tuple[int, int]:
+        t, l = C.c_long(), C.c_long()
+        check(load().nricp_batch_counters(self._handle, C.byref(t), C.byref(l)))
+        return t.value, l.value
+
+    def profile(self) -> list[dict]:
+        """Re-runs the batch with CUDA events around the closest-point query,
+        the linear solve and the assembly of every tick; per-tick records of
+        the first wrap."""
+        q, p, a = C.c_double(), C.c_double(), C.c_double()
+        ticks = C.c_long()
+        check(load().nricp_batch_profile(self._handle, C.byref(q), C.byref(p), C.byref(a),
+                                         C.byref(ticks)))
+        records = (_abi.TickRecord * max(1, ticks.value))()
+        count = C.c_int()
+        check(load().nricp_batch_tick_records(self._handle, records, ticks.value, C.byref(count)))
+        return [{"phase": r.phase, "level": r.level, "pcg_iterations": r.pcg_iterations,
+                 "query_ms": r.query_ms, "pcg_ms": r.pcg_ms, "assemble_ms": r.assemble_ms,
+                 "tick_ms": r.tick_ms} for r in records[:count.value]]
+
+    def level_sizes(self, index: int, level: int) -> dict:
+        sizes = (C.c_int32 * 10)()
+        check(load().nricp_batch_level_sizes(self._handle, index, level, sizes))
+        keys = ("nodes", "edges", "pairs", "entries", "pair_entries", "vertices",
+                "target_triangles", "target_vertices", "template_triangles", "levels")
+        return dict(zip(keys, list(sizes)))
+
+
+def transfer_counters(reset: bool = False) -> tuple[int, int]:
+    """Bytes copied host->device and device->host by this thread's calls."""
+    h2d, d2h = C.c_ulonglong(), C.c_ulonglong()
+    check(load().nricp_transfer_counters(C.byref(h2d), C.byref(d2h), int(reset)))
+    return h2d.value, d2h.value
+
+
 class RouteBSession:
     """The device schedule with the caller holding the loop: construct the
     session, then call step() until finished().  `route` selects 'route_b'
