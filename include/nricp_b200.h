@@ -253,6 +253,22 @@ int nricp_lbvh_export(const double* target_points, int vertex_count,
                       const int32_t* faces, int face_count, uint32_t* codes,
                       uint32_t* order, int32_t* left, int32_t* right, float* bounds);
 
+/* nricp_lbvh_export with DEVICE buffers and no device allocation; it has no
+ * counterpart in the reference.  For callers that cannot allocate GPU memory
+ * (inside another framework's pool or allocator hooks, with a fixed arena, or
+ * with allocations audited after start-up): every intermediate lives in one
+ * static 8 MiB device array, so at most 262,144 faces (more returns
+ * NRICP_ERR_CAPACITY).  `target_points` (V x 3), `faces` (F x 3), `codes`,
+ * `order` (F), `left`, `right` (F - 1) and `bounds` (6) are device pointers;
+ * the work runs on `stream` (a cudaStream_t, NULL for the default stream) and
+ * the call returns once it has finished.  The first call on a device looks up
+ * the array's address and should come before any stream capture.  All calls
+ * share the array: calls whose work overlaps on the GPU race. */
+int nricp_lbvh_export_static(const double* target_points, int vertex_count,
+                             const int32_t* faces, int face_count, uint32_t* codes,
+                             uint32_t* order, int32_t* left, int32_t* right,
+                             float* bounds, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,9 @@ def _declare(lib: C.CDLL) -> None:
                                                  i32p, C.c_int, P(C.c_int)]),
         "nricp_closest_points": (C.c_int, [dp, C.c_int, i32p, C.c_int, dp, C.c_int, dp, dp, dp, i32p]),
         "nricp_lbvh_export": (C.c_int, [dp, C.c_int, i32p, C.c_int, u32p, u32p, i32p, i32p, fp]),
+        "nricp_lbvh_export_static": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p]),
         "nricp_default_desc": (None, [desc_p]),
         "nricp_default_level": (None, [P(_abi.LevelSettings)]),
     }

@@ -15,7 +15,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libnricp_b200.so"
-SOURCES = ["host.cpp", "lbvh.cu", "wrap_kernels.cu", "session.cu", "capi.cu"]
+SOURCES = ["host.cpp", "lbvh.cu", "wrap_kernels.cu", "session.cu", "capi.cu", "static_scratch.cu"]
 HEADERS = ["common.cuh", "kernels.cuh", "host.hpp", "session.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

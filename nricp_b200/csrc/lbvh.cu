@@ -766,3 +766,88 @@ void launch_closest_points(const WrapDev* wrap, const double* queries, int count
 }
 
 }  // namespace nricp_b200
+
+namespace nricp_b200 {
+
+namespace {
+
+// Out-of-range face indices would make the centroid pass read outside the
+// caller's vertex buffer; this pass only records that they exist.
+__global__ void k_check_faces(const int32_t* __restrict__ faces, int count, int vertex_count,
+                              int* __restrict__ flag) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count * 3) return;
+    const int v = faces[i];
+    if (v < 0 || v >= vertex_count) atomicOr(flag, 1);
+}
+
+}  // namespace
+
+size_t lbvh_export_scratch_bytes(int n) {
+    const size_t tiles = (size_t)((n + kSortTile - 1) / kSortTile);
+    const size_t pieces[] = {
+        sizeof(float) * 3 * (size_t)n,            // centroids
+        sizeof(float) * 6 * 1024,                 // bound partials
+        sizeof(uint32_t) * (size_t)n,             // second key buffer
+        sizeof(uint32_t) * (size_t)n,             // second value buffer
+        sizeof(uint32_t) * kRadix * (tiles + 1),  // digit counts
+        sizeof(int32_t) * 2 * (size_t)n,          // parent links (written by the split pass)
+        256,                                      // validation flag
+    };
+    size_t total = 0;
+    for (size_t bytes : pieces) total += (bytes + 255) & ~size_t(255);
+    return total;
+}
+
+// The canonical arrays of the hierarchy (sorted codes, permutation, Karras
+// children, centroid bounds) straight into caller-owned device buffers, with
+// every intermediate in `scratch`.  The sort ping-pongs between the caller's
+// code/permutation buffers and a scratch pair; with an even number of passes
+// the result lands in the caller's.  Returns false when a face index is out of
+// range (nothing past the check reads the vertices then).
+bool lbvh_export_to_device(const double* points, int vertex_count, const int32_t* faces, int n,
+                           void* scratch, uint32_t* codes, uint32_t* order, int32_t* left,
+                           int32_t* right, float* bounds, cudaStream_t stream) {
+    char* base = static_cast<char*>(scratch);
+    auto carve = [&base](size_t bytes) {
+        char* p = base;
+        base += (bytes + 255) & ~size_t(255);
+        return p;
+    };
+    float* centroids = reinterpret_cast<float*>(carve(sizeof(float) * 3 * n));
+    float* bound_partial = reinterpret_cast<float*>(carve(sizeof(float) * 6 * 1024));
+    uint32_t* keys[2] = {codes, reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n))};
+    uint32_t* values[2] = {order, reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * n))};
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* counts = reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * kRadix * (tiles + 1)));
+    int32_t* parent = reinterpret_cast<int32_t*>(carve(sizeof(int32_t) * 2 * n));
+    int* flag = reinterpret_cast<int*>(carve(256));
+
+    // the array keeps the previous call's contents: clear what starts at zero
+    cudaMemsetAsync(flag, 0, sizeof(int), stream);
+    k_check_faces<<<blocks_for((long)n * 3), kThreads, 0, stream>>>(faces, n, vertex_count, flag);
+    int host_flag = 0;
+    cudaMemcpyAsync(&host_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    cudaStreamSynchronize(stream);
+    if (host_flag) return false;
+
+    k_centroids<<<blocks_for(n), kThreads, 0, stream>>>(points, faces, n, centroids);
+    const int bound_blocks = blocks_for(n) < 1024 ? blocks_for(n) : 1024;
+    k_bounds_partial<<<bound_blocks, kThreads, 0, stream>>>(centroids, n, bound_partial);
+    k_bounds_final<<<1, 32, 0, stream>>>(bound_partial, bound_blocks, bounds);
+    k_morton<<<blocks_for(n), kThreads, 0, stream>>>(centroids, n, bounds, keys[0], values[0]);
+    int cur = 0;
+    for (int shift = 0; shift < 32; shift += kRadixBits) {
+        k_radix_histogram<<<tiles, kThreads, 0, stream>>>(keys[cur], n, shift, counts, tiles);
+        k_radix_scan<<<1, 1024, 0, stream>>>(counts, kRadix * tiles);
+        k_radix_scatter<<<tiles, kThreads, 0, stream>>>(keys[cur], values[cur], n, shift, counts,
+                                                        tiles, keys[1 - cur], values[1 - cur]);
+        cur = 1 - cur;
+    }
+    // eight passes: the sorted arrays are back in the caller's buffers
+    cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream);
+    if (n > 1) k_karras<<<blocks_for(n - 1), kThreads, 0, stream>>>(keys[cur], n, left, right, parent);
+    return true;
+}
+
+}  // namespace nricp_b200
