@@ -60,44 +60,12 @@ def parse_args():
 # distributed plumbing (replicas)
 # ---------------------------------------------------------------------------
 
-class Ranks:
-    def __init__(self, gpus: int):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.dist = None
-        if self.world > 1:
-            import datetime
+def Ranks(gpus: int):
+    """One process per GPU under torchrun (NCCL for the host bookkeeping:
+    barrier, max of the times, sum of the work); a single process otherwise."""
+    from nricp_b200.replicas import ReplicaGroup
 
-            import torch
-            import torch.distributed as dist
-
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-            self.dist = dist
-            self.torch = torch
-
-    def barrier(self):
-        if self.dist:
-            self.dist.barrier()
-
-    def max(self, value: float) -> float:
-        if not self.dist:
-            return value
-        t = self.torch.tensor([value], dtype=self.torch.float64, device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum(self, value: float) -> float:
-        if not self.dist:
-            return value
-        t = self.torch.tensor([value], dtype=self.torch.float64, device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
-        return float(t.item())
-
-    def close(self):
-        if self.dist:
-            self.dist.destroy_process_group()
+    return ReplicaGroup(backend="nccl", timeout_s=600.0)
 
 
 # ---------------------------------------------------------------------------
@@ -209,7 +177,7 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def run_reference_arm(args, ranks: Ranks):
+def run_reference_arm(args, ranks):
     if ranks.rank != 0:
         return
     cores = min(host_cores(), 64)
@@ -330,7 +298,7 @@ def flush_l2():
 # our arm
 # ---------------------------------------------------------------------------
 
-def run_ours(args, ranks: Ranks):
+def run_ours(args, ranks):
     import torch
 
     from nricp_b200 import nricp_dp as dp

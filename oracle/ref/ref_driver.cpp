@@ -220,6 +220,52 @@ void ref_vertex_normals(const double* points, int point_count, const int32_t* fa
     }
 }
 
+// One level of the reference's own template graph (src/core/graph.cpp:43-76):
+// normalisation, FPS prefix, frozen bindings and 4-NN edges.
+int ref_template_graph_level(const double* points, int count, int levels, int nodes_initial,
+                             int growth, int max_nodes, int level, double center[3],
+                             double* scale, int32_t* node_indices, double* node_positions,
+                             int32_t* binding_nodes, double* binding_weights,
+                             int32_t* binding_counts, int32_t* edges, int edge_capacity,
+                             int* node_count, int* edge_count) {
+    nricp::Mesh mesh;
+    mesh.vertices = points_of(points, count);
+    nricp::GraphSettings settings;
+    settings.levels = levels;
+    settings.nodes_initial = nodes_initial;
+    settings.node_growth = growth;
+    settings.max_nodes_per_vertex = max_nodes;
+    const nricp::TemplateGraph graph = nricp::build_template_graph(mesh, settings);
+    if (level < 0 || level >= static_cast<int>(graph.levels.size())) return -1;
+    const nricp::GraphLevel& g = graph.levels[static_cast<std::size_t>(level)];
+    center[0] = graph.normalization.center.x;
+    center[1] = graph.normalization.center.y;
+    center[2] = graph.normalization.center.z;
+    *scale = graph.normalization.scale;
+    *node_count = g.node_count();
+    for (int i = 0; i < g.node_count(); ++i) {
+        node_indices[i] = g.node_template_indices[i];
+        node_positions[i * 3] = g.node_rest_positions[i].x;
+        node_positions[i * 3 + 1] = g.node_rest_positions[i].y;
+        node_positions[i * 3 + 2] = g.node_rest_positions[i].z;
+    }
+    for (int v = 0; v < count; ++v) {
+        for (int s = 0; s < NRICP_MAX_SLOTS; ++s) {
+            const bool real = s < nricp::VertexBinding::kMaxNodes;
+            binding_nodes[v * NRICP_MAX_SLOTS + s] = real ? g.bindings[v].nodes[s] : -1;
+            binding_weights[v * NRICP_MAX_SLOTS + s] = real ? g.bindings[v].weights[s] : 0.0;
+        }
+        binding_counts[v] = g.bindings[v].count;
+    }
+    if (static_cast<int>(g.edges.size()) > edge_capacity) return -2;
+    *edge_count = static_cast<int>(g.edges.size());
+    for (std::size_t i = 0; i < g.edges.size(); ++i) {
+        edges[i * 2] = g.edges[i].a;
+        edges[i * 2 + 1] = g.edges[i].b;
+    }
+    return 0;
+}
+
 void ref_normalization(const double* points, int count, double center[3], double* scale) {
     nricp::Mesh mesh;
     mesh.vertices = points_of(points, count);
