@@ -207,6 +207,15 @@ int nricp_batch_profile(NricpBatch* batch, double* query_ms, double* pcg_ms,
  * wrap reset to the start of its schedule (hierarchies rebuilt) and run to
  * completion.  Inputs stay resident in device memory. */
 int nricp_batch_step(NricpBatch* batch, double* device_ms);
+
+/* No reference counterpart.  Cluster size of the batch's linear solve: a
+ * power of two from 1 to 16 gives every wrap that many CTAs in one launch;
+ * 0 (the default) gives each wrap its own size (about 128 nodes per CTA), one
+ * launch per size class, the classes running side by side; -s (s = 1..4)
+ * halves those per-wrap sizes s times.  Every choice gives bit-identical
+ * results; it trades one wrap's latency against the batch's throughput.
+ * *cluster_out (may be NULL) receives the largest size in effect. */
+int nricp_batch_tune(NricpBatch* batch, int pcg_cluster, int* cluster_out);
 /* Per-tick records of wrap 0 from the last nricp_batch_profile. */
 typedef struct NricpTickRecord {
     int phase;          /* 0 transfer, 1 refresh, 2 solve, 3 final */

@@ -61,6 +61,7 @@ def _declare(lib: C.CDLL) -> None:
         "nricp_batch_profile": (C.c_int, [C.c_void_p, dp, dp, dp, P(C.c_long)]),
         "nricp_batch_destroy": (None, [C.c_void_p]),
         "nricp_batch_step": (C.c_int, [C.c_void_p, dp]),
+        "nricp_batch_tune": (C.c_int, [C.c_void_p, C.c_int, P(C.c_int)]),
         "nricp_batch_tick_records": (C.c_int, [C.c_void_p, P(_abi.TickRecord), C.c_int, P(C.c_int)]),
         "nricp_batch_level_sizes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, i32p]),
         "nricp_batch_solve": (C.c_int, [desc_p, C.c_int, result_p]),

@@ -36,6 +36,9 @@ int guarded(F&& body) {
     } catch (const InvalidArgument& e) {
         g_last_error = e.what();
         return NRICP_ERR_INVALID;
+    } catch (const CapacityError& e) {
+        g_last_error = e.what();
+        return NRICP_ERR_CAPACITY;
     } catch (const StateError& e) {
         g_last_error = e.what();
         return NRICP_ERR_STATE;
@@ -281,6 +284,13 @@ int nricp_batch_profile(NricpBatch* b, double* query_ms, double* pcg_ms, double*
 
 int nricp_batch_step(NricpBatch* b, double* device_ms) {
     return guarded([&] { *device_ms = b->batch.timed_step(); });
+}
+
+int nricp_batch_tune(NricpBatch* b, int pcg_cluster, int* cluster_out) {
+    return guarded([&] {
+        b->batch.set_pcg_cluster(pcg_cluster);
+        if (cluster_out) *cluster_out = b->batch.shape().pcg_cluster;
+    });
 }
 
 int nricp_batch_tick_records(NricpBatch* b, NricpTickRecord* out, int capacity, int* count) {

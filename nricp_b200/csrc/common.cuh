@@ -173,12 +173,13 @@ struct WrapDev {
                                   // (B for the a side, B^T for the b side)
     // solve scratch
     float* factor;                // N x 36: inverse of the damped diagonal block
-    float* damped;                // N x 36: damped diagonal blocks
     double* delta;                // N x 6
     double* pcg_x;                // N x 6
     double* pcg_r;                // N x 6
-    float* pcg_p;                 // N x 6
-    float* pcg_ap;                // N x 6
+    float* pcg_p;                 // N x 6: direction p
+    float* pcg_ap;                // N x 6: w = A u
+    float* pcg_s;                 // N x 6: s = A p (by recurrence)
+    float* pcg_u;                 // N x 6: u = M^-1 r, every node
     // reductions
     double* partials;             // energy_blocks x kPartialStride
     double* edge_partials;        // edge blocks x 1 (smoothness energy)

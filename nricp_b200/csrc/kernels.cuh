@@ -36,8 +36,17 @@ struct TickShape {
     int energy_blocks;   // vertex-pass blocks per wrap (partials written)
     int edge_blocks;
     int node_blocks;
-    int pcg_cluster;     // CTAs per wrap in the cluster solve
-    int pcg_shared_bytes;  // direction staged in shared memory
+    int pcg_cluster;       // CTAs per wrap in the cluster solve (any value gives the same result)
+    int pcg_shared_bytes;  // dynamic shared memory of the solve launch
+    // The solve may instead be split into launches by cluster class, each over
+    // a list of wraps (device array), run as parallel branches of the tick.
+    int pcg_groups;                      // 0: one launch over every wrap
+    int pcg_group_cluster[5];
+    int pcg_group_count[5];
+    int pcg_group_shared[5];
+    const int* pcg_group_index[5];       // device: wrap indices of the group
+    cudaStream_t pcg_streams[5];         // branch streams (index 0 unused)
+    cudaEvent_t pcg_fork, pcg_join[5];
 };
 
 // Device timing hooks for the dominant kernels (CUDA events on the launching
@@ -52,8 +61,10 @@ struct KernelTimers {
 void launch_tick(const WrapDev* wraps, const TickShape& shape, cudaStream_t stream,
                  KernelTimers* timers);
 int tick_kernel_launches(const TickShape& shape);
-int pcg_cluster_size(int max_nodes);
-int pcg_shared_bytes(int max_nodes);
+int pcg_latency_cluster(int nodes);
+int pcg_cluster_size(int max_nodes, int wraps, int sm_count);
+int pcg_shared_bytes(const int* max_nodes, int wraps, int cluster);
+int pcg_max_nodes();
 void launch_evaluate_state(const WrapDev* wraps, const TickShape& shape, cudaStream_t stream);
 
 }  // namespace nricp_b200

@@ -162,6 +162,11 @@ void prepare_host(Wrap& w) {
     const NricpSolveDesc& d = w.desc;
     const int k = d.max_nodes_per_vertex > 0 ? d.max_nodes_per_vertex : 4;
     const int edge_k = d.edge_neighbours > 0 ? d.edge_neighbours : 4;
+    const int finest = level_node_count(std::max(1, d.graph_levels) - 1, d.nodes_initial, d.growth, w.V);
+    if (finest > pcg_max_nodes())
+        throw CapacityError("the finest graph level has " + std::to_string(finest) +
+                            " nodes; the device solve supports at most " +
+                            std::to_string(pcg_max_nodes()));
     w.graph = build_template_graph(d.template_points, w.V, d.graph_levels, d.nodes_initial,
                                    d.growth, k, edge_k);
     w.levels = static_cast<int>(w.graph.levels.size());
@@ -235,12 +240,13 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     const size_t o_r1 = a.reserve(sizeof(float4) * V);
     const size_t o_r2 = a.reserve(sizeof(float4) * V);
     const size_t o_factor = a.reserve(sizeof(float) * 36 * N);
-    const size_t o_damped = a.reserve(sizeof(float) * 36 * N);
     const size_t o_delta = a.reserve(sizeof(double) * 6 * N);
     const size_t o_x = a.reserve(sizeof(double) * 6 * N);
     const size_t o_r = a.reserve(sizeof(double) * 6 * N);
     const size_t o_p = a.reserve(sizeof(float) * 6 * N);
     const size_t o_ap = a.reserve(sizeof(float) * 6 * N);
+    const size_t o_s = a.reserve(sizeof(float) * 6 * N);
+    const size_t o_u = a.reserve(sizeof(float) * 6 * N);
     const int vblocks = (V + 255) / 256;
     const size_t o_part = a.reserve(sizeof(double) * kPartialStride * std::max(1, vblocks));
     const size_t o_epart = a.reserve(sizeof(double) * std::max(1, (w.max_edges + 127) / 128));
@@ -375,12 +381,13 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     D.resid_aux32 = a.at<float4>(o_r1);
     D.lm_resid32 = a.at<float4>(o_r2);
     D.factor = a.at<float>(o_factor);
-    D.damped = a.at<float>(o_damped);
     D.delta = a.at<double>(o_delta);
     D.pcg_x = a.at<double>(o_x);
     D.pcg_r = a.at<double>(o_r);
     D.pcg_p = a.at<float>(o_p);
     D.pcg_ap = a.at<float>(o_ap);
+    D.pcg_s = a.at<float>(o_s);
+    D.pcg_u = a.at<float>(o_u);
     D.partials = a.at<double>(o_part);
     D.edge_partials = a.at<double>(o_epart);
     D.node_partials = a.at<double>(o_npart);
@@ -395,7 +402,7 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
 // Puts a wrap back at the start of its schedule: identity transforms, no
 // previous correspondences, and a freshly built hierarchy of its target.  Runs
 // on the device only (the inputs are already resident).
-void reset_device(Wrap& w, cudaStream_t stream, LbvhExport* lbvh_out) {
+void reset_device(Wrap& w, cudaStream_t stream, void* lbvh_scratch, LbvhExport* lbvh_out) {
     WrapDev& D = w.dev;
     const int V = w.V, N = std::max(1, w.max_nodes);
     if (w.identity_rot == nullptr) {
@@ -433,14 +440,12 @@ void reset_device(Wrap& w, cudaStream_t stream, LbvhExport* lbvh_out) {
     c.damping = w.desc.initial_damping;
     check(cudaMemcpyAsync(w.control, &c, sizeof c, cudaMemcpyHostToDevice, stream), "init control");
 
-    // the target's hierarchy, in a scratch that lives only for the build
-    void* scratch = nullptr;
-    check(cudaMallocAsync(&scratch, lbvh_scratch_bytes(w.F), stream), "cudaMallocAsync(lbvh scratch)");
-    const uint32_t root = lbvh_build(D.tgt_points, D.tgt_faces, w.F, scratch,
+    // the target's hierarchy; the batch's build scratch (sized for its
+    // largest target) is reused by every wrap's build in stream order
+    const uint32_t root = lbvh_build(D.tgt_points, D.tgt_faces, w.F, lbvh_scratch,
                                      const_cast<float4*>(D.bvh_nodes), const_cast<float4*>(D.bvh_leaves),
                                      stream, lbvh_out);
     check(cudaGetLastError(), "lbvh build");
-    check(cudaFreeAsync(scratch, stream), "cudaFreeAsync(lbvh scratch)");
     D.bvh_root = static_cast<int>(root);
 }
 
@@ -463,6 +468,13 @@ Batch::~Batch() {
     wraps_.clear();
     if (dev_wraps_) cudaFree(dev_wraps_);
     if (dev_controls_) cudaFree(dev_controls_);
+    if (lbvh_scratch_) cudaFree(lbvh_scratch_);
+    if (pcg_index_) cudaFree(pcg_index_);
+    for (int g = 0; g < 5; ++g) {
+        if (pcg_streams_[g]) cudaStreamDestroy(pcg_streams_[g]);
+        if (pcg_join_[g]) cudaEventDestroy(pcg_join_[g]);
+    }
+    if (pcg_fork_) cudaEventDestroy(pcg_fork_);
     if (host_controls_) cudaFreeHost(host_controls_);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -482,21 +494,23 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
     const int W = static_cast<int>(wraps_.size());
     check(cudaMalloc(&dev_controls_, sizeof(WrapControl) * W), "cudaMalloc(controls)");
     check(cudaMallocHost(&host_controls_, sizeof(WrapControl) * W), "cudaMallocHost(controls)");
+    size_t scratch_bytes = 0;
+    for (const auto& w : wraps_) scratch_bytes = std::max(scratch_bytes, lbvh_scratch_bytes(w->F));
+    check(cudaMalloc(&lbvh_scratch_, scratch_bytes), "cudaMalloc(lbvh scratch)");
     shape_ = TickShape{};
     shape_.wraps = W;
     for (int i = 0; i < W; ++i) {
         Wrap& w = *wraps_[i];
         const double t0 = now_seconds();
         prepare_device(w, dev_controls_ + i, stream_);
-        reset_device(w, stream_, i == 0 ? lbvh_out : nullptr);
+        reset_device(w, stream_, lbvh_scratch_, i == 0 ? lbvh_out : nullptr);
         w.setup_seconds += now_seconds() - t0;
         shape_.max_vertices = std::max(shape_.max_vertices, w.V);
         shape_.max_nodes = std::max(shape_.max_nodes, w.max_nodes);
         shape_.max_edges = std::max(shape_.max_edges, w.max_edges);
         shape_.max_pairs = std::max(shape_.max_pairs, w.max_pairs);
     }
-    shape_.pcg_cluster = pcg_cluster_size(shape_.max_nodes);
-    shape_.pcg_shared_bytes = pcg_shared_bytes(shape_.max_nodes);
+    set_pcg_cluster(0);
     check(cudaMalloc(&dev_wraps_, sizeof(WrapDev) * W), "cudaMalloc(wraps)");
     std::vector<WrapDev> host(W);
     for (int i = 0; i < W; ++i) host[i] = wraps_[i]->dev;
@@ -510,7 +524,7 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
 void Batch::reset() {
     check(cudaStreamSynchronize(stream_), "reset");
     for (auto& w : wraps_) {
-        reset_device(*w, stream_, nullptr);
+        reset_device(*w, stream_, lbvh_scratch_, nullptr);
         w->solve_seconds = 0.0;
     }
     ticks_ = 0;
@@ -536,6 +550,68 @@ bool Batch::all_done() const {
     for (size_t i = 0; i < wraps_.size(); ++i)
         if (host_controls_[i].phase != kPhaseDone) return false;
     return true;
+}
+
+void Batch::set_pcg_cluster(int cluster) {
+    int device = 0, sms = 148;
+    check(cudaGetDevice(&device), "device");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device");
+    const int W = static_cast<int>(wraps_.size());
+    std::vector<int> nodes(W);
+    for (int i = 0; i < W; ++i) nodes[i] = wraps_[i]->max_nodes;
+    pcg_cluster_size(shape_.max_nodes, W, sms);  // enables the launch attributes
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    shape_.pcg_groups = 0;
+    if (cluster > 0) {
+        if (cluster > 16 || (cluster & (cluster - 1)) != 0)
+            throw InvalidArgument("the solve's cluster size is a power of two from 1 to 16");
+        shape_.pcg_cluster = cluster;
+        shape_.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), W, cluster);
+        return;
+    }
+    if (cluster < -4) throw InvalidArgument("the solve's class shift is 0 to 4");
+    // one class per wrap: its own latency cluster, halved `shift` times
+    const int shift = -cluster;
+    std::vector<int> cls(W);
+    for (int i = 0; i < W; ++i) cls[i] = std::max(1, pcg_latency_cluster(nodes[i]) >> shift);
+    std::vector<int> sizes;
+    for (int c = 16; c >= 1; c /= 2)
+        if (std::count(cls.begin(), cls.end(), c) > 0) sizes.push_back(c);
+    if (sizes.size() == 1) {
+        shape_.pcg_cluster = sizes[0];
+        shape_.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), W, sizes[0]);
+        return;
+    }
+    if (!pcg_index_) check(cudaMalloc(&pcg_index_, sizeof(int) * W), "cudaMalloc(solve groups)");
+    std::vector<int> order;
+    for (size_t g = 0; g < sizes.size(); ++g) {
+        const int first = static_cast<int>(order.size());
+        std::vector<int> members;
+        for (int i = 0; i < W; ++i)
+            if (cls[i] == sizes[g]) members.push_back(i);
+        std::vector<int> member_nodes;
+        for (int i : members) member_nodes.push_back(nodes[i]);
+        order.insert(order.end(), members.begin(), members.end());
+        shape_.pcg_group_cluster[g] = sizes[g];
+        shape_.pcg_group_count[g] = static_cast<int>(members.size());
+        shape_.pcg_group_shared[g] = pcg_shared_bytes(member_nodes.data(), (int)members.size(), sizes[g]);
+        shape_.pcg_group_index[g] = pcg_index_ + first;
+        if (g > 0 && !pcg_streams_[g]) {
+            check(cudaStreamCreateWithFlags(&pcg_streams_[g], cudaStreamNonBlocking), "stream");
+            check(cudaEventCreateWithFlags(&pcg_join_[g], cudaEventDisableTiming), "event");
+        }
+        shape_.pcg_streams[g] = pcg_streams_[g];
+        shape_.pcg_join[g] = pcg_join_[g];
+    }
+    if (!pcg_fork_) check(cudaEventCreateWithFlags(&pcg_fork_, cudaEventDisableTiming), "event");
+    shape_.pcg_fork = pcg_fork_;
+    check(cudaMemcpy(pcg_index_, order.data(), sizeof(int) * W, cudaMemcpyHostToDevice), "solve groups");
+    shape_.pcg_groups = static_cast<int>(sizes.size());
+    shape_.pcg_cluster = sizes[0];
+    shape_.pcg_shared_bytes = shape_.pcg_group_shared[0];
 }
 
 void Batch::run(int max_ticks) {
@@ -599,7 +675,7 @@ double Batch::timed_step() {
     check(cudaEventCreate(&end), "event");
     check(cudaStreamSynchronize(stream_), "step");
     check(cudaEventRecord(begin, stream_), "event");
-    for (auto& w : wraps_) reset_device(*w, stream_, nullptr);
+    for (auto& w : wraps_) reset_device(*w, stream_, lbvh_scratch_, nullptr);
     ticks_ = 0;
     launches_ = 0;
     for (auto& w : wraps_) launches_ += lbvh_build_launches(w->F);

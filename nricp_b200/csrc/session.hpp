@@ -17,6 +17,9 @@ namespace nricp_b200 {
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+struct CapacityError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 struct StateError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
@@ -55,6 +58,11 @@ public:
     // Device time of reset() + run() on the batch's stream (CUDA events).
     double timed_step();
     void level_sizes(int i, int level, int* sizes) const;
+    // Cluster size of the solve launch.  > 0: that size for every wrap; 0:
+    // each wrap its own latency cluster (about 128 nodes per CTA), one launch
+    // per size class, the classes in parallel; -s: the same classes halved s
+    // times.  Every choice gives bit-identical results.
+    void set_pcg_cluster(int cluster);
     void pull_controls();
     bool all_done() const;
     void finish();
@@ -80,6 +88,11 @@ private:
     cudaStream_t stream_ = nullptr;
     WrapDev* dev_wraps_ = nullptr;
     WrapControl* dev_controls_ = nullptr;
+    void* lbvh_scratch_ = nullptr;  // hierarchy build scratch, shared by the wraps' builds
+    int* pcg_index_ = nullptr;      // wraps ordered by solve class (device)
+    cudaStream_t pcg_streams_[5] = {};
+    cudaEvent_t pcg_join_[5] = {};
+    cudaEvent_t pcg_fork_ = nullptr;
     WrapControl* host_controls_ = nullptr;
     TickShape shape_{};
     cudaGraphExec_t graph_exec_ = nullptr;

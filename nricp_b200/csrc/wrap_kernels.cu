@@ -602,57 +602,48 @@ __device__ inline void solve6(const float* l, const double* rhs, double* x) {
     for (int r = 0; r < 6; ++r) x[r] = z[r];
 }
 
-// One thread-block cluster per wrap (blockIdx.y): each CTA of the cluster owns
-// a contiguous slice of the nodes (rows), the search direction lives in global
-// memory (L2) where every CTA's matvec reads it, and the FP64 inner products
-// are per-CTA partials exchanged through distributed shared memory and summed
-// in rank order -- deterministic, and the same whatever else shares the
-// launch.  Hardware cluster barriers separate the four stages of an
-// iteration; nothing spins.
-// Sum of one FP64 partial per CTA of the cluster.  Warp 0 reads the ranks'
-// slots lane by lane (lanes past the cluster size read zero) and reduces them
-// with a fixed butterfly, so the total does not depend on how many CTAs the
-// launch gave the cluster beyond the ones that own rows; the rest of the CTA
-// picks it up from local shared memory.  The cluster barrier before the read
-// orders the writes (release/acquire at cluster scope, which covers global
-// memory too).
-__device__ inline double cluster_sum(cg::cluster_group& cluster, double* slot, double* out) {
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        double v = lane < (int)cluster.num_blocks() ? *cluster.map_shared_rank(slot, lane) : 0.0;
-        v = warp_sum(v);
-        if (lane == 0) *out = v;
-    }
-    __syncthreads();
-    return *out;
+// ---- the solve's partition and shared-memory layout ------------------------
+//
+// Rows are grouped into segments of kSegNodes nodes (48 rows).  A segment is
+// the unit of ownership and of reduction: one warp forms the segment's FP64
+// partial dot products in a fixed lane order, and the cluster sums the
+// segments' partials in a fixed order.  A CTA owns a contiguous run of
+// segments, so the cluster size only decides which CTA computes which
+// segment, never the order of any sum: a wrap's solve is bit-identical for
+// every cluster size, and with it alone and in any batch.
+constexpr int kSegNodes = 8;
+constexpr int kPcgWarps = kPcgThreads / 32;
+constexpr int kPcgOwnFloats = 78;  // per owned node: X, R (2 x 6 FP64) + Minv 36 + P, S, W 18
+constexpr int kPcgMaxSmemBytes = 225 * 1024;
+
+__host__ __device__ inline int pcg_segments(int nodes) { return (nodes + kSegNodes - 1) / kSegNodes; }
+// FP64 slots for the segments' three partials, padded to 16 bytes
+__host__ __device__ inline int pcg_slot_doubles(int nodes) { return (3 * pcg_segments(nodes) + 1) & ~1; }
+
+// Owned-node capacity of one CTA when `ranks` CTAs share the solve.
+__host__ __device__ inline int pcg_owned_capacity(int nodes, int ranks) {
+    return (pcg_segments(nodes) + ranks - 1) / ranks * kSegNodes;
 }
 
-__device__ inline double cluster_total(cg::cluster_group& cluster, double* slot, double local,
-                                       double* scratch, double* out) {
-    const double mine = block_sum<kPcgThreads>(local, scratch);
-    if (threadIdx.x == 0) *slot = mine;
-    cluster.sync();
-    return cluster_sum(cluster, slot, out);
-}
-
-// CTAs of a wrap's cluster that own rows: a function of the wrap's own node
-// count only, so the partition -- and with it every partial sum -- is the
-// same alone and in any batch.
-__host__ __device__ inline int owner_ranks(int nodes) {
-    int ranks = 1;
-    while (ranks < 16 && ranks * 128 < nodes) ranks *= 2;
-    return ranks;
-}
-
-constexpr int kPcgSharedNodes = 4096;  // all-node direction copy in shared memory up to this N
-constexpr int kPcgSharedOwn = 256;     // and the owned rows' vectors up to this many nodes
-
-// Shared-memory layout of the solve for `nodes` nodes and `own` owned nodes.
-__host__ __device__ inline int pcg_smem_floats(int nodes, int own) {
-    return ((nodes * 6 + 3) & ~3)   // direction, every node (all CTAs' copies)
-           + own * 36 * 2           // inverse and damped diagonal blocks
-           + own * 6 * 2 * 2        // x and r (FP64)
-           + own * 6;               // Ap, then z
+// Placement for one wrap within a shared-memory budget: the segment slots
+// always, then the all-node direction copy U if it fits (the matvec reads it
+// ~10 times per row), then the owned rows' arrays if they fit.  Whatever does
+// not fit lives in the wrap's global scratch; the arithmetic is the same.
+struct PcgPlacement {
+    bool u_shared, own_shared;
+    int floats;  // shared floats this wrap uses
+};
+__host__ __device__ inline PcgPlacement pcg_place(int nodes, int ranks, int budget_floats) {
+    PcgPlacement p;
+    int used = pcg_slot_doubles(nodes) * 2;  // 3 FP64 partials per segment
+    const int u = (nodes * 6 + 3) & ~3;
+    const int own = pcg_owned_capacity(nodes, ranks) * kPcgOwnFloats;
+    p.u_shared = used + u <= budget_floats;
+    if (p.u_shared) used += u;
+    p.own_shared = used + own <= budget_floats;
+    if (p.own_shared) used += own;
+    p.floats = used;
+    return p;
 }
 
 // Inverse of a 6x6 SPD block from its Cholesky factor L (lower): L^-T L^-1.
@@ -675,56 +666,102 @@ __device__ inline void cholesky_inverse6(const float* l, float* inv) {
         }
 }
 
-// The damped solve (pcg_solver.cu:15-241) for one wrap per thread-block
-// cluster.  Each CTA owns a contiguous slice of the nodes and keeps that
-// slice's inverse preconditioner blocks, damped diagonal, x, r and Ap in
-// shared memory (global scratch past the size limits -- same arithmetic, same
-// order); the search direction is broadcast slice by slice into every CTA's
-// copy through distributed shared memory, so the matvec reads it locally and
-// its only L2 traffic is the off-diagonal blocks, stored in row order.
-// Three cluster barriers per iteration; FP64 dots, residual and solution.
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__ wraps) {
+__device__ inline float dot6(const float* a, const float* b) {
+    const float2* a2 = reinterpret_cast<const float2*>(a);
+    const float2* b2 = reinterpret_cast<const float2*>(b);
+    const float2 a0 = a2[0], a1 = a2[1], a3 = a2[2];
+    const float2 b0 = b2[0], b1 = b2[1], b3 = b2[2];
+    float y = a0.x * b0.x;
+    y += a0.y * b0.y;
+    y += a1.x * b1.x;
+    y += a1.y * b1.y;
+    y += a3.x * b3.x;
+    y += a3.y * b3.y;
+    return y;
+}
+
+// The damped solve (pcg_solver.cu:15-241): (A + lambda diag-scale) x = b,
+// x0 = 0, block-Jacobi preconditioner from the Cholesky factor of each damped
+// 6x6 diagonal block (with the reference's jitter retry), stop at
+// |r| / |b| <= tolerance or after the iteration cap.  One thread-block
+// cluster per wrap (blockIdx.y), any cluster size.
+//
+// The recurrence is the single-reduction form of preconditioned CG
+// (Chronopoulos & Gear, 1989): with u = M^-1 r and w = A u, the three inner
+// products (r,u), (w,u), (r,r) of an iteration are formed together, so an
+// iteration needs one exchange of partial sums and one exchange of u:
+//
+//   gamma = (r,u), delta = (w,u); beta = gamma / gamma_prev;
+//   alpha = gamma / (delta - beta gamma / alpha_prev)   (beta = 0 first);
+//   p = u + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s.
+//
+// FP32 blocks, matvec, p, s, u and w; FP64 x, r, the inner products and the
+// scalars.  Each CTA writes its slice of u once into its own shared copy and
+// then copies the slice, 16 bytes at a time, into every other CTA's copy
+// through distributed shared memory, so the matvec reads u locally and its
+// only L2 traffic is the blocks (stored in row order).  Two hardware cluster
+// barriers per iteration; nothing spins.
+__global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__ wraps,
+                                                     const int* __restrict__ index,
+                                                     int budget_floats) {
     cg::cluster_group cluster = cg::this_cluster();
-    const WrapDev& w = wraps[blockIdx.y];
+    const WrapDev& w = wraps[index ? index[blockIdx.y] : blockIdx.y];
     const WrapControl c = *w.control;
     if (c.phase != kPhaseSolve) return;  // uniform across the cluster
     const LevelDev& L = w.levels[c.level];
     const int N = L.node_count;
     const int rank = (int)cluster.block_rank();
     const int ranks = (int)cluster.num_blocks();
-    const int owners = min(owner_ranks(N), ranks);
-    const int per = (N + owners - 1) / owners;
-    const int n0 = rank < owners ? min(N, rank * per) : N;
-    const int n1 = rank < owners ? min(N, n0 + per) : N;
-    const int own = n1 - n0;
-    const bool in_shared = N <= kPcgSharedNodes && per <= kPcgSharedOwn;
+    const int segs = pcg_segments(N);
+    const int cap = pcg_owned_capacity(N, ranks);
+    const int seg_per = cap / kSegNodes;
+    const int s0 = min(segs, rank * seg_per);
+    const int s1 = min(segs, s0 + seg_per);
+    const int n0 = s0 * kSegNodes;
+    const int n1 = min(N, s1 * kSegNodes);
+    const int own = n1 > n0 ? n1 - n0 : 0;
+    const int rows = own * 6;
+    const PcgPlacement place = pcg_place(N, ranks, budget_floats);
+
     extern __shared__ float4 dynamic_shared[];
-    float* base = reinterpret_cast<float*>(dynamic_shared);
-    const int pn = (N * 6 + 3) & ~3;
-    float* P = in_shared ? base : w.pcg_p;                       // all nodes
-    float* Minv = in_shared ? base + pn : w.factor + n0 * 36;     // owned
-    float* Dd = in_shared ? base + pn + per * 36 : w.damped + n0 * 36;
-    double* X = in_shared ? reinterpret_cast<double*>(base + pn + per * 72) : w.pcg_x + n0 * 6;
-    double* R = in_shared ? X + per * 6 : w.pcg_r + n0 * 6;
-    float* Aq = in_shared ? reinterpret_cast<float*>(R + per * 6) : w.pcg_ap + n0 * 6;
-    const float* D = w.diag[c.system];
-    const float* B = w.offdiag[c.system];
-    const float* b = w.rhs[c.system];
+    double* slots = reinterpret_cast<double*>(dynamic_shared);  // 3 per segment, every CTA
+    float* cursor = reinterpret_cast<float*>(slots + pcg_slot_doubles(N));
+    float* U;
+    if (place.u_shared) {
+        U = cursor;
+        cursor += (N * 6 + 3) & ~3;
+    } else {
+        U = w.pcg_u;
+    }
+    double *X, *R;
+    float *Minv, *P, *S, *Wv;
+    if (place.own_shared) {
+        X = reinterpret_cast<double*>(cursor);
+        R = X + cap * 6;
+        Minv = reinterpret_cast<float*>(R + cap * 6);
+        P = Minv + cap * 36;
+        S = P + cap * 6;
+        Wv = S + cap * 6;
+    } else {
+        X = w.pcg_x + n0 * 6;
+        R = w.pcg_r + n0 * 6;
+        Minv = w.factor + n0 * 36;
+        P = w.pcg_p + n0 * 6;
+        S = w.pcg_s + n0 * 6;
+        Wv = w.pcg_ap + n0 * 6;
+    }
+    const float* __restrict__ D = w.diag[c.system];
+    const float* __restrict__ B = w.offdiag[c.system];
+    const float* __restrict__ b = w.rhs[c.system];
+    const int* __restrict__ row_begin = L.row_begin;
+    const int2* __restrict__ entries = reinterpret_cast<const int2*>(L.row_entry);
     const float damping = (float)c.damping;
     const bool scaled = w.diagonal_damping != 0;
-    __shared__ double scratch[33];
-    __shared__ double slots[8];
-    __shared__ double totals[8];
-    const int rows = own * 6;
-
-    // writes row i (global index) of the direction into every CTA's copy
-    auto broadcast = [&](int i, float value) {
-        if (in_shared) {
-            for (int q = 0; q < ranks; ++q) cluster.map_shared_rank(P, q)[i] = value;
-        } else {
-            P[i] = value;
-        }
-    };
+    const int max_iterations = w.pcg_max_iterations;
+    const double tolerance = w.pcg_tolerance;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ double red[3][kPcgWarps];
+    __shared__ double tot[3];
 
     // ---- damped diagonal blocks and their inverses (route A's damped():
     //      scale = max(D_rr, 1e-12)); Cholesky with the reference's jitter ----
@@ -733,7 +770,6 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
         float blk[36];
         for (int i = 0; i < 36; ++i) blk[i] = D[n * 36 + i];
         for (int r = 0; r < 6; ++r) blk[r * 7] += damping * (scaled ? fmaxf(blk[r * 7], 1e-12f) : 1.0f);
-        for (int i = 0; i < 36; ++i) Dd[m * 36 + i] = blk[i];
         float jitter = 0.0f;
         bool ok = false;
         for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
@@ -749,107 +785,137 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
         if (!ok)
             for (int i = 0; i < 36; ++i) Minv[m * 36 + i] = (i % 7 == 0) ? 1.0f : 0.0f;
     }
-    double local_bb = 0.0;
     for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-        const double bi = b[n0 * 6 + i];
         X[i] = 0.0;
-        R[i] = bi;
-        local_bb += bi * bi;
+        R[i] = (double)b[n0 * 6 + i];
+        P[i] = 0.0f;
+        S[i] = 0.0f;
     }
     __syncthreads();
-    // z = M^-1 r, p = z
-    double local_rz = 0.0;
-    for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-        const int m = i / 6, r = i - m * 6;
-        const float* mi = Minv + m * 36 + r * 6;
-        float z = 0.0f;
-        for (int q = 0; q < 6; ++q) z += mi[q] * (float)R[m * 6 + q];
-        broadcast(n0 * 6 + i, z);
-        local_rz += R[i] * (double)z;
-    }
-    {
-        const double s0 = block_sum<kPcgThreads>(local_bb, scratch);
-        const double s1 = block_sum<kPcgThreads>(local_rz, scratch);
-        if (threadIdx.x == 0) { slots[0] = s0; slots[1] = s1; }
-        if (!in_shared) __threadfence();
-        cluster.sync();
-    }
-    const double bb = cluster_sum(cluster, &slots[0], &totals[0]);
-    double rz = cluster_sum(cluster, &slots[1], &totals[1]);
-    const double bnorm = sqrt(bb);
-    int iterations = 0;
-    bool converged = !(bnorm > 0.0);
-    double residual = bnorm > 0.0 ? 1.0 : 0.0;
-    const int2* entries = reinterpret_cast<const int2*>(L.row_entry);
-    for (int it = 0; it < w.pcg_max_iterations && !converged; ++it) {
-        // ---- A: Ap for the owned rows, and p.Ap ----
-        double local_pap = 0.0;
-        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-            const int m = i / 6, r = i - m * 6, n = n0 + m;
-            const float* dd = Dd + m * 36 + r * 6;
-            const float* pn = P + n * 6;
-            float y = 0.0f;
-            for (int q = 0; q < 6; ++q) y += dd[q] * pn[q];
-            const int e1 = L.row_begin[n + 1];
-            int e = L.row_begin[n];
-            for (; e + 4 <= e1; e += 4) {
-                float bv[4][6];
-                int nb[4];
-                for (int u = 0; u < 4; ++u) {
-                    const float* Bb = B + (long)(e + u) * 36 + r * 6;
-                    for (int q = 0; q < 6; ++q) bv[u][q] = Bb[q];
-                    nb[u] = entries[e + u].y;
-                }
-                for (int u = 0; u < 4; ++u) {
-                    const float* pm = P + nb[u] * 6;
-                    for (int q = 0; q < 6; ++q) y += bv[u][q] * pm[q];
-                }
-            }
-            for (; e < e1; ++e) {
-                const float* Bb = B + (long)e * 36 + r * 6;
-                const float* pm = P + entries[e].y * 6;
-                for (int q = 0; q < 6; ++q) y += Bb[q] * pm[q];
-            }
-            Aq[i] = y;
-            local_pap += (double)pn[r] * (double)y;
-        }
-        const double pap = cluster_total(cluster, &slots[2], local_pap, scratch, &totals[2]);
-        if (fabs(pap) < 1e-300) break;
-        const double alpha = rz / pap;
-        // ---- B: x, r per owned row; z = M^-1 r; r.r and r.z together ----
-        double local_rr = 0.0;
-        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-            X[i] += alpha * (double)P[n0 * 6 + i];
-            const double ri = R[i] - alpha * (double)Aq[i];
-            R[i] = ri;
-            local_rr += ri * ri;
-        }
-        __syncthreads();
-        double local_rz2 = 0.0;
+
+    // u = M^-1 r for the owned rows into this CTA's copy, then the slice into
+    // every other CTA's copy (16-byte stores; the slice starts on a segment,
+    // so at a multiple of 192 bytes)
+    auto precondition_and_share = [&]() {
         for (int i = threadIdx.x; i < rows; i += blockDim.x) {
             const int m = i / 6, r = i - m * 6;
             const float* mi = Minv + m * 36 + r * 6;
             float z = 0.0f;
             for (int q = 0; q < 6; ++q) z += mi[q] * (float)R[m * 6 + q];
-            Aq[i] = z;  // z, in the Ap storage
-            local_rz2 += R[i] * (double)z;
+            U[n0 * 6 + i] = z;
         }
-        const double s_rr = block_sum<kPcgThreads>(local_rr, scratch);
-        const double s_rz = block_sum<kPcgThreads>(local_rz2, scratch);
-        if (threadIdx.x == 0) { slots[3] = s_rr; slots[4] = s_rz; }
+        if (place.u_shared && ranks > 1) {
+            __syncthreads();
+            const float4* src = reinterpret_cast<const float4*>(U + n0 * 6);
+            const int vec = rows / 4;  // rows = 6 * own, own a multiple of 8 except at the end
+            for (int q = 1; q < ranks; ++q) {
+                const int dst_rank = (rank + q) % ranks;
+                float4* dst = reinterpret_cast<float4*>(cluster.map_shared_rank(U, dst_rank) + n0 * 6);
+                for (int k = threadIdx.x; k < vec; k += blockDim.x) dst[k] = src[k];
+                float* dst_tail = cluster.map_shared_rank(U, dst_rank) + n0 * 6;
+                for (int k = vec * 4 + threadIdx.x; k < rows; k += blockDim.x) dst_tail[k] = U[n0 * 6 + k];
+            }
+        }
+        if (!place.u_shared) __threadfence();  // the global copy: visible device-wide first
+    };
+    precondition_and_share();
+    cluster.sync();
+
+    double gamma_prev = 0.0, alpha_prev = 0.0, bnorm = 0.0, residual = 0.0;
+    int iterations = 0;
+    bool converged = false;
+    for (int it = 0;; ++it) {
+        // ---- w = A u for the owned rows; per-segment partials of (r,u), (w,u), (r,r) ----
+        for (int sl = warp; sl < s1 - s0; sl += kPcgWarps) {
+            const int seg = s0 + sl;
+            const int sn0 = seg * kSegNodes;
+            const int seg_rows = (min(N, sn0 + kSegNodes) - sn0) * 6;
+            double g = 0.0, d = 0.0, rr = 0.0;
+            for (int k = lane; k < seg_rows; k += 32) {
+                const int n = sn0 + k / 6, r = k % 6;
+                const int i = (sn0 - n0) * 6 + k;
+                const float* drow = D + n * 36 + r * 6;
+                const float* un = U + n * 6;
+                const float dd = drow[r] + damping * (scaled ? fmaxf(drow[r], 1e-12f) : 1.0f);
+                float y = 0.0f;
+                for (int q = 0; q < 6; ++q) y += (q == r ? dd : drow[q]) * un[q];
+                const int e1 = row_begin[n + 1];
+                int e = row_begin[n];
+                for (; e + 4 <= e1; e += 4) {
+                    int nb[4];
+                    for (int u = 0; u < 4; ++u) nb[u] = entries[e + u].y;
+                    float part[4];
+                    for (int u = 0; u < 4; ++u) part[u] = dot6(B + (long)(e + u) * 36 + r * 6, U + nb[u] * 6);
+                    for (int u = 0; u < 4; ++u) y += part[u];
+                }
+                for (; e < e1; ++e) y += dot6(B + (long)e * 36 + r * 6, U + entries[e].y * 6);
+                Wv[i] = y;
+                const double ui = (double)un[r];
+                const double ri = R[i];
+                g += ri * ui;
+                d += (double)y * ui;
+                rr += ri * ri;
+            }
+            g = warp_sum(g);
+            d = warp_sum(d);
+            rr = warp_sum(rr);
+            if (lane < ranks) {  // lane q stores the partials in CTA q's slots
+                double* dst = cluster.map_shared_rank(slots, lane) + 3 * seg;
+                dst[0] = g;
+                dst[1] = d;
+                dst[2] = rr;
+            }
+        }
         cluster.sync();
-        const double rr_total = cluster_sum(cluster, &slots[3], &totals[3]);
-        const double rz_next = cluster_sum(cluster, &slots[4], &totals[4]);
-        iterations = it + 1;
+        // ---- totals over every segment, in one fixed order in every CTA ----
+        {
+            double g = 0.0, d = 0.0, rr = 0.0;
+            for (int sg = threadIdx.x; sg < segs; sg += blockDim.x) {
+                g += slots[3 * sg];
+                d += slots[3 * sg + 1];
+                rr += slots[3 * sg + 2];
+            }
+            g = warp_sum(g);
+            d = warp_sum(d);
+            rr = warp_sum(rr);
+            if (lane == 0) { red[0][warp] = g; red[1][warp] = d; red[2][warp] = rr; }
+            __syncthreads();
+            if (warp == 0) {
+                for (int k = 0; k < 3; ++k) {
+                    double v = lane < kPcgWarps ? red[k][lane] : 0.0;
+                    v = warp_sum(v);
+                    if (lane == 0) tot[k] = v;
+                }
+            }
+            __syncthreads();
+        }
+        const double gamma = tot[0], delta = tot[1], rr_total = tot[2];
+        if (it == 0) {
+            bnorm = sqrt(rr_total);
+            if (!(bnorm > 0.0)) { converged = true; residual = 0.0; break; }
+        }
         residual = sqrt(rr_total) / bnorm;
-        if (residual <= w.pcg_tolerance) { converged = true; break; }
-        // ---- C: the next direction, broadcast to every CTA's copy ----
-        const double beta = fabs(rz) > 1e-300 ? rz_next / rz : 0.0;
-        rz = rz_next;
-        for (int i = threadIdx.x; i < rows; i += blockDim.x)
-            broadcast(n0 * 6 + i, (float)((double)Aq[i] + beta * (double)P[n0 * 6 + i]));
-        if (!in_shared) __threadfence();  // the global copy: visible device-wide first
+        if (residual <= tolerance) { converged = true; break; }
+        if (it >= max_iterations) break;
+        const double beta = it == 0 ? 0.0 : gamma / gamma_prev;
+        const double denominator = it == 0 ? delta : delta - beta * gamma / alpha_prev;
+        if (!(fabs(denominator) > 1e-300)) break;
+        const double alpha = gamma / denominator;
+        gamma_prev = gamma;
+        alpha_prev = alpha;
+        // ---- p, s, x, r for the owned rows; then u = M^-1 r, shared ----
+        for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+            const float pn = (float)((double)U[n0 * 6 + i] + beta * (double)P[i]);
+            const float sn = (float)((double)Wv[i] + beta * (double)S[i]);
+            P[i] = pn;
+            S[i] = sn;
+            X[i] += alpha * (double)pn;
+            R[i] -= alpha * (double)sn;
+        }
+        __syncthreads();
+        precondition_and_share();
         cluster.sync();
+        iterations = it + 1;
     }
     if (rank == 0 && threadIdx.x == 0) {
         w.control->pcg_ok = converged ? 1 : 0;
@@ -878,7 +944,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
             for (int k = 0; k < 6; ++k) w.delta[n * 6 + k] = x[k];
         }
     }
-    // no CTA may exit while another can still read its shared memory
+    // no CTA may exit while another can still write into its shared memory
     cluster.sync();
 }
 
@@ -1373,13 +1439,12 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     k_c_fit<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
     k_c_rhs<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
     if (timers && timers->active) cudaEventRecord(timers->pcg_begin, stream);
-    {
-        const int cluster = s.pcg_cluster;
+    auto launch_pcg = [&](int cluster, int count, int shared, const int* index, cudaStream_t on) {
         cudaLaunchConfig_t config = {};
-        config.gridDim = dim3(cluster, W);
+        config.gridDim = dim3(cluster, count);
         config.blockDim = dim3(kPcgThreads);
-        config.dynamicSmemBytes = s.pcg_shared_bytes;
-        config.stream = stream;
+        config.dynamicSmemBytes = shared;
+        config.stream = on;
         cudaLaunchAttribute attribute[1];
         attribute[0].id = cudaLaunchAttributeClusterDimension;
         attribute[0].val.clusterDim.x = cluster;
@@ -1387,7 +1452,22 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
         attribute[0].val.clusterDim.z = 1;
         config.attrs = attribute;
         config.numAttrs = 1;
-        cudaLaunchKernelEx(&config, k_pcg, wraps);
+        cudaLaunchKernelEx(&config, k_pcg, wraps, index, (int)(shared / sizeof(float)));
+    };
+    if (s.pcg_groups <= 0) {
+        launch_pcg(s.pcg_cluster, W, s.pcg_shared_bytes, nullptr, stream);
+    } else {
+        // fork: every class launch after everything before it on `stream`
+        cudaEventRecord(s.pcg_fork, stream);
+        for (int g = 1; g < s.pcg_groups; ++g) {
+            cudaStreamWaitEvent(s.pcg_streams[g], s.pcg_fork, 0);
+            launch_pcg(s.pcg_group_cluster[g], s.pcg_group_count[g], s.pcg_group_shared[g],
+                       s.pcg_group_index[g], s.pcg_streams[g]);
+            cudaEventRecord(s.pcg_join[g], s.pcg_streams[g]);
+        }
+        launch_pcg(s.pcg_group_cluster[0], s.pcg_group_count[0], s.pcg_group_shared[0],
+                   s.pcg_group_index[0], stream);
+        for (int g = 1; g < s.pcg_groups; ++g) cudaStreamWaitEvent(stream, s.pcg_join[g], 0);
     }
     if (timers && timers->active) cudaEventRecord(timers->pcg_end, stream);
     k_evaluate<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
@@ -1408,31 +1488,47 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     k_decide<<<W, 256, 0, stream>>>(wraps);
 }
 
-int tick_kernel_launches(const TickShape& s) { return s.max_pairs > 0 ? 15 : 14; }
+int tick_kernel_launches(const TickShape& s) {
+    return (s.max_pairs > 0 ? 14 : 13) + (s.pcg_groups > 0 ? s.pcg_groups : 1);
+}
 
-// Cluster size of the solve: enough CTAs that each owns ~128 nodes, a power
-// of two, at most 16 (the non-portable maximum, enabled here).
-int pcg_cluster_size(int max_nodes) {
+// Cluster size of the solve for one wrap of `nodes` nodes on its own: a
+// power of two with about 128 nodes (16 segments, one per warp) per CTA, at
+// most 16 CTAs (the non-portable maximum, enabled here).
+int pcg_latency_cluster(int nodes) {
+    int ranks = 1;
+    while (ranks < 16 && ranks * 128 < nodes) ranks *= 2;
+    return ranks;
+}
+
+void pcg_enable() {
     static bool enabled = false;
     if (!enabled) {
         cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             pcg_smem_floats(kPcgSharedNodes, kPcgSharedOwn) * (int)sizeof(float));
+        cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, kPcgMaxSmemBytes);
         enabled = true;
     }
-    return owner_ranks(max_nodes);
 }
 
-int pcg_shared_bytes(int max_nodes) {
-    // the largest layout any wrap of this size range can need
-    int best = 0;
-    for (int n = 1; n <= max_nodes; n = n < 64 ? n + 1 : n + n / 16) {
-        const int per = (n + owner_ranks(n) - 1) / owner_ranks(n);
-        if (n <= kPcgSharedNodes && per <= kPcgSharedOwn) best = max(best, pcg_smem_floats(n, per));
-    }
-    const int n = max_nodes, per = (n + owner_ranks(n) - 1) / owner_ranks(n);
-    if (n <= kPcgSharedNodes && per <= kPcgSharedOwn) best = max(best, pcg_smem_floats(n, per));
-    return best * (int)sizeof(float);
+// Default cluster size for a batch: one wrap takes its latency cluster; many
+// wraps share the SMs, so the cluster shrinks until one CTA per SM holds the
+// whole batch (the result does not depend on the choice).
+int pcg_cluster_size(int max_nodes, int wraps, int sm_count) {
+    pcg_enable();
+    int ranks = pcg_latency_cluster(max_nodes);
+    while (ranks > 1 && (long)ranks * wraps > sm_count) ranks /= 2;
+    return ranks;
 }
+
+// Dynamic shared memory of the solve launch: what the largest wrap would use
+// at this cluster size, at most the per-CTA maximum.
+int pcg_shared_bytes(const int* max_nodes, int wraps, int cluster) {
+    int floats = 0;
+    for (int i = 0; i < wraps; ++i)
+        floats = max(floats, pcg_place(max_nodes[i], cluster, 1 << 30).floats);
+    return min(floats * (int)sizeof(float), kPcgMaxSmemBytes);
+}
+
+int pcg_max_nodes() { return 32768; }
 
 }  // namespace nricp_b200

@@ -113,6 +113,15 @@ class WrapBatch:
         check(load().nricp_batch_step(self._handle, C.byref(ms)))
         return ms.value
 
+    def tune(self, pcg_cluster: int = 0) -> int:
+        """Cluster size of the linear solve: a power of two up to 16 for every
+        wrap, 0 (default) for each wrap's own size in per-class launches, -s
+        for those sizes halved s times.  Returns the largest size in effect;
+        results are bit-identical for every choice."""
+        out = C.c_int()
+        check(load().nricp_batch_tune(self._handle, int(pcg_cluster), C.byref(out)))
+        return out.value
+
     def result(self, index: int) -> dict:
         out = _abi.ResultBuffers(self._descs[index].template_points.shape[0], self._plans[index])
         check(load().nricp_batch_result(self._handle, index, C.byref(out.struct)))

@@ -293,19 +293,35 @@ def config2(seed: int = 0, vertex_count: int = 25_000, triangle_count: int = 400
                               nodes=[nodes_initial * 2 ** l for l in range(levels)]))
 
 
-def config3(seed: int = 0, instances: int = 64):
-    """64 uneven wraps: template vertices log-uniform in [5k, 50k], nodes =
-    verts/15, target triangles log-uniform in [50k, 500k], generated as in
-    config 2."""
+def _config3_sizes(seed: int, instances: int):
     rng = np.random.default_rng(seed)
-    cases = []
+    sizes = []
     for i in range(instances):
         v = int(round(math.exp(rng.uniform(math.log(5_000), math.log(50_000)))))
         f = int(round(math.exp(rng.uniform(math.log(50_000), math.log(500_000)))))
-        nodes = max(8, v // 15)
-        cases.append(config2(seed=seed * 1000 + i + 1, vertex_count=v, triangle_count=f,
-                             nodes_finest=nodes, k=6, levels=4))
-    return cases
+        sizes.append((seed * 1000 + i + 1, v, f, max(8, v // 15)))
+    return sizes
+
+
+def _config3_case(spec):
+    case_seed, v, f, nodes = spec
+    return config2(seed=case_seed, vertex_count=v, triangle_count=f, nodes_finest=nodes,
+                   k=6, levels=4)
+
+
+def config3(seed: int = 0, instances: int = 64, workers: int = 1):
+    """64 uneven wraps: template vertices log-uniform in [5k, 50k], nodes =
+    verts/15, target triangles log-uniform in [50k, 500k], generated as in
+    config 2.  `workers` > 1 generates the instances in that many spawned
+    processes (the same cases, in the same order)."""
+    specs = _config3_sizes(seed, instances)
+    if workers <= 1:
+        return [_config3_case(s) for s in specs]
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as pool:
+        return list(pool.map(_config3_case, specs))
 
 
 def config5(seed: int = 0, vertex_count: int = 100_000, triangle_count: int = 2_000_000,

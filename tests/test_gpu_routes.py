@@ -136,6 +136,40 @@ def test_a_batch_gives_each_wrap_the_result_it_gets_alone(dp, device):
         assert ja["energy"] == jm["energy"] and ja["levels"] == jm["levels"]
 
 
+@pytest.mark.parametrize("route", ["route_b", "route_c"])
+def test_every_solve_cluster_size_gives_the_same_bits(dp, device, route):
+    """The linear solve's cluster size (1 to 16 CTAs per wrap) only decides
+    which CTA computes which 8-node segment, never the order of a sum: the
+    wraps' results must be bit-identical for every size, alone and batched."""
+    cases = [S.small_case(seed=4, nodes_initial=40),           # 40 / 80 nodes: idle CTAs at 16
+             S.config1(5),                                     # 50 / 100 / 200 nodes
+             S.small_case(seed=7, rings=40, segments=60, nodes_initial=300)]  # 300 / 600 nodes
+    tuples = [(*c.args(), c.options) for c in cases]
+    reference = None
+    for cluster in (1, 2, 4, 8, 16, 0, -1):
+        batch = dp.WrapBatch(tuples, route=route)
+        effective = batch.tune(cluster)
+        assert effective == cluster if cluster > 0 else effective >= 1
+        batch.run()
+        got = [batch.result(i) for i in range(len(cases))]
+        if reference is None:
+            reference = got
+            continue
+        for a, b in zip(reference, got):
+            assert np.array_equal(a["vertices"], b["vertices"]), cluster
+            assert np.array_equal(a["rotations"], b["rotations"]), cluster
+            ja, jb = json.loads(a["report"]), json.loads(b["report"])
+            assert ja["energy"] == jb["energy"] and ja["levels"] == jb["levels"], cluster
+
+
+def test_solve_cluster_size_is_validated(dp, device):
+    case = S.small_case(seed=6)
+    batch = dp.WrapBatch([(*case.args(), case.options)])
+    with pytest.raises(ValueError, match="power of two"):
+        batch.tune(3)
+    assert batch.tune(0) >= 1
+
+
 def test_masks_and_landmarks_reach_the_device(dp, device, oracle):
     case = S.small_case(seed=3)
     mask = np.ones(len(case.template_points), dtype=np.int64)
