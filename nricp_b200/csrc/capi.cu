@@ -230,7 +230,7 @@ int nricp_batch_create(const NricpSolveDesc* descs, int count, NricpBatch** out)
         if (count <= 0) throw InvalidArgument("a batch needs at least one wrap");
         require_device();
         auto b = std::make_unique<NricpBatch>();
-        for (int i = 0; i < count; ++i) b->batch.add(descs[i]);
+        b->batch.add_all(descs, count);
         b->batch.upload_all();
         *out = b.release();
     });
@@ -313,9 +313,9 @@ int nricp_batch_level_sizes(NricpBatch* b, int index, int level, int32_t* sizes)
     return guarded([&] {
         if (index < 0 || index >= b->batch.size()) throw InvalidArgument("wrap index out of range");
         if (level < 0 || level >= b->batch.levels(index)) throw InvalidArgument("level out of range");
-        int v[10];
+        int v[Batch::kLevelSizeEntries];
         b->batch.level_sizes(index, level, v);
-        for (int i = 0; i < 10; ++i) sizes[i] = v[i];
+        for (int i = 0; i < Batch::kLevelSizeEntries; ++i) sizes[i] = v[i];
     });
 }
 
@@ -326,7 +326,7 @@ int nricp_batch_solve(const NricpSolveDesc* descs, int count, NricpResult* resul
         if (count <= 0) throw InvalidArgument("a batch needs at least one wrap");
         require_device();
         Batch batch;
-        for (int i = 0; i < count; ++i) batch.add(descs[i]);
+        batch.add_all(descs, count);
         batch.upload_all();
         batch.run();
         for (int i = 0; i < count; ++i) batch.result(i, &results[i]);

@@ -70,6 +70,8 @@ struct LevelDev {
 struct LevelRecord {
     int level, nodes, outer_iterations, inner_iterations, converged, pad;
     double energy_start, energy_end, correspondence_mean;
+    // work done in the level (measurement, not part of the report)
+    int solves, pcg_iterations, queries, assemblies;
 };
 
 // Correspondence statistics, CorrespondenceCounts (correspondence.h:52-67).

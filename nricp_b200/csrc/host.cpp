@@ -184,37 +184,45 @@ std::vector<int> farthest_point_seeds(const std::vector<double>& pts, int count,
         nearest[i] = sqdist(&pts[i * 3], chosen);
         if (nearest[i] > best_sq) { best_sq = nearest[i]; best = i; }
     }
+    // The points are split into `chunks` fixed ranges; each range keeps its
+    // first maximum and the ranges are merged in order, so the seeds are the
+    // sequential scan's (first maximum) for any number of chunks or threads.
+    // The ranges are strided over whatever team runs the region: inside an
+    // enclosing parallel region (a batch preparing wraps side by side) that
+    // team is a single thread.
 #ifdef _OPENMP
-    const int threads = n >= 20000 ? std::min(omp_get_max_threads(), 16) : 1;
+    const int chunks = n >= 20000 ? std::min(omp_get_max_threads(), 16) : 1;
 #else
-    const int threads = 1;
+    const int chunks = 1;
 #endif
-    std::vector<double> t_best(threads);
-    std::vector<int> t_idx(threads);
+    std::vector<double> t_best(chunks);
+    std::vector<int> t_idx(chunks);
     while (static_cast<int>(seeds.size()) < count) {
         seeds.push_back(best);
         chosen = &pts[best * 3];
-#pragma omp parallel num_threads(threads)
+#pragma omp parallel num_threads(chunks)
         {
 #ifdef _OPENMP
-            const int t = omp_get_thread_num();
+            const int first_chunk = omp_get_thread_num(), team = omp_get_num_threads();
 #else
-            const int t = 0;
+            const int first_chunk = 0, team = 1;
 #endif
-            const int begin = static_cast<int>((long)n * t / threads);
-            const int end = static_cast<int>((long)n * (t + 1) / threads);
-            double bs = -1.0;
-            int bi = begin;
-            for (int i = begin; i < end; ++i) {
-                const double d = sqdist(&pts[i * 3], chosen);
-                nearest[i] = nearest[i] < d ? nearest[i] : d;
-                if (nearest[i] > bs) { bs = nearest[i]; bi = i; }
+            for (int t = first_chunk; t < chunks; t += team) {
+                const int begin = static_cast<int>((long)n * t / chunks);
+                const int end = static_cast<int>((long)n * (t + 1) / chunks);
+                double bs = -1.0;
+                int bi = begin;
+                for (int i = begin; i < end; ++i) {
+                    const double d = sqdist(&pts[i * 3], chosen);
+                    nearest[i] = nearest[i] < d ? nearest[i] : d;
+                    if (nearest[i] > bs) { bs = nearest[i]; bi = i; }
+                }
+                t_best[t] = bs;
+                t_idx[t] = bi;
             }
-            t_best[t] = bs;
-            t_idx[t] = bi;
         }
         best_sq = -1.0;
-        for (int t = 0; t < threads; ++t)
+        for (int t = 0; t < chunks; ++t)
             if (t_best[t] > best_sq) { best_sq = t_best[t]; best = t_idx[t]; }
     }
     return seeds;

@@ -479,7 +479,8 @@ Batch::~Batch() {
     if (stream_) cudaStreamDestroy(stream_);
 }
 
-void Batch::add(const NricpSolveDesc& desc) {
+namespace {
+std::unique_ptr<Wrap> make_wrap(const NricpSolveDesc& desc) {
     NricpSolveDesc d = desc;
     validate_settings(d);
     auto w = std::make_unique<Wrap>();
@@ -487,7 +488,42 @@ void Batch::add(const NricpSolveDesc& desc) {
     copy_inputs(*w, d);
     prepare_host(*w);
     w->setup_seconds = now_seconds() - t0;
-    wraps_.push_back(std::move(w));
+    return w;
+}
+}  // namespace
+
+void Batch::add(const NricpSolveDesc& desc) { wraps_.push_back(make_wrap(desc)); }
+
+void Batch::add_all(const NricpSolveDesc* descs, int count) {
+    // the wraps' host preparation is independent: one wrap per host thread
+    // (a single wrap keeps the threads for its own graph build)
+    std::vector<std::unique_ptr<Wrap>> prepared(count);
+    std::vector<int> kind(count, 0);
+    std::vector<std::string> message(count);
+#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
+    for (int i = 0; i < count; ++i) {
+        try {
+            prepared[i] = make_wrap(descs[i]);
+        } catch (const InvalidArgument& e) {
+            kind[i] = 1;
+            message[i] = e.what();
+        } catch (const CapacityError& e) {
+            kind[i] = 2;
+            message[i] = e.what();
+        } catch (const std::bad_alloc&) {
+            kind[i] = 3;
+        } catch (const std::exception& e) {
+            kind[i] = 4;
+            message[i] = e.what();
+        }
+    }
+    for (int i = 0; i < count; ++i) {
+        if (kind[i] == 1) throw InvalidArgument(message[i]);
+        if (kind[i] == 2) throw CapacityError(message[i]);
+        if (kind[i] == 3) throw std::bad_alloc();
+        if (kind[i] == 4) throw std::runtime_error(message[i]);
+    }
+    for (auto& w : prepared) wraps_.push_back(std::move(w));
 }
 
 void Batch::upload_all(LbvhExport* lbvh_out) {
@@ -702,6 +738,13 @@ void Batch::level_sizes(int i, int level, int* sizes) const {
     sizes[7] = w.Vt;
     sizes[8] = w.T;
     sizes[9] = w.levels;
+    // the work the last run did in this level
+    LevelRecord r{};
+    check(cudaMemcpy(&r, w.dev.records + level, sizeof r, cudaMemcpyDeviceToHost), "level record");
+    sizes[10] = r.solves;
+    sizes[11] = r.pcg_iterations;
+    sizes[12] = r.queries;
+    sizes[13] = r.assemblies;
 }
 
 void Batch::finish() {

@@ -37,6 +37,9 @@ public:
 
     // Host preparation of one more wrap (validation, graph, layouts).
     void add(const NricpSolveDesc& desc);
+    // The same for many wraps, prepared in parallel on the host's cores;
+    // the first invalid wrap (in order) raises.
+    void add_all(const NricpSolveDesc* descs, int count);
     // Device arenas, uploads, hierarchies; after this the batch can tick.
     void upload_all(LbvhExport* lbvh_out = nullptr);
     // Back to the start of every wrap's schedule, inputs kept resident
@@ -57,6 +60,8 @@ public:
     const std::vector<TickRecord>& tick_records() const { return records_; }
     // Device time of reset() + run() on the batch's stream (CUDA events).
     double timed_step();
+    // Sizes and work counters of one level (kLevelSizeEntries ints).
+    static constexpr int kLevelSizeEntries = 14;
     void level_sizes(int i, int level, int* sizes) const;
     // Cluster size of the solve launch.  > 0: that size for every wrap; 0:
     // each wrap its own latency cluster (about 128 nodes per CTA), one launch

@@ -1349,6 +1349,12 @@ __global__ void k_decide(const WrapDev* __restrict__ wraps) {
     c.steps += 1;
     const double total = parts_s[0] + parts_s[1] + parts_s[2] + parts_s[3] + parts_s[4];
     LevelRecord& rec = w.records[c.level];
+    if (c.phase == kPhaseSolve) {
+        rec.solves += 1;
+        rec.pcg_iterations += c.pcg_iterations;
+    }
+    if (refresh_like(c.phase)) rec.queries += 1;
+    if (assembles(c)) rec.assemblies += 1;
     bool close_outer = false;
     if (c.phase == kPhaseTransfer || c.phase == kPhaseRefresh) {
         if (c.phase == kPhaseTransfer) c.state = 1 - c.state;

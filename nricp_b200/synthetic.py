@@ -293,7 +293,9 @@ def config2(seed: int = 0, vertex_count: int = 25_000, triangle_count: int = 400
                               nodes=[nodes_initial * 2 ** l for l in range(levels)]))
 
 
-def _config3_sizes(seed: int, instances: int):
+def config3_specs(seed: int, instances: int = 64):
+    """(case seed, template vertices, target triangles, finest nodes) of each
+    of config 3's instances, in order."""
     rng = np.random.default_rng(seed)
     sizes = []
     for i in range(instances):
@@ -303,7 +305,8 @@ def _config3_sizes(seed: int, instances: int):
     return sizes
 
 
-def _config3_case(spec):
+def config3_case(spec):
+    """One config-3 instance from its spec (see config3_specs)."""
     case_seed, v, f, nodes = spec
     return config2(seed=case_seed, vertex_count=v, triangle_count=f, nodes_finest=nodes,
                    k=6, levels=4)
@@ -314,14 +317,14 @@ def config3(seed: int = 0, instances: int = 64, workers: int = 1):
     verts/15, target triangles log-uniform in [50k, 500k], generated as in
     config 2.  `workers` > 1 generates the instances in that many spawned
     processes (the same cases, in the same order)."""
-    specs = _config3_sizes(seed, instances)
+    specs = config3_specs(seed, instances)
     if workers <= 1:
-        return [_config3_case(s) for s in specs]
+        return [config3_case(s) for s in specs]
     import concurrent.futures as cf
     import multiprocessing as mp
 
     with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as pool:
-        return list(pool.map(_config3_case, specs))
+        return list(pool.map(config3_case, specs))
 
 
 def config5(seed: int = 0, vertex_count: int = 100_000, triangle_count: int = 2_000_000,
