@@ -1,24 +1,38 @@
 #!/usr/bin/env python
-"""Throughput of the nricp wrapping path on B200: wraps per second.
+"""Throughput of the nricp wrapping path on B200: wraps per second, batched
+against one wrap at a time, at equal fit error.
 
-Workload (N = 1): the large single wrap -- a 25,000-vertex ellipsoid template
-with 20 bumps onto a 400,000-triangle deformed, holed, outlier-laden target;
-graph 250/500/1000/2000 nodes, k = 6, 4 levels (nricp_b200.synthetic.config2,
-seeded synthetic data).  One step is one whole wrap: the target's hierarchy
-rebuilt, then the coarse-to-fine schedule run to completion.
+Workload (N = 1): 64 uneven wraps solved as one batch -- template vertices
+log-uniform in [5k, 50k] (ellipsoid grids with 20 bumps), graph nodes = V/15
+over 4 levels, k = 6, targets log-uniform in [50k, 500k] triangles (deformed,
+holed, 1 % outliers); seeded synthetic data (nricp_b200.synthetic.config3).
+One step is the whole batch: every target's hierarchy rebuilt, then every
+wrap's coarse-to-fine schedule run to completion, all wraps advancing
+together (one launch sequence per tick, replayed as a CUDA graph).
 
-Lines printed (one JSON line on rank 0):
-* ``value``      wraps/s with every input resident in HBM (CUDA events on the
-                 solver's stream, max over ranks),
-* ``e2e``        wraps/s through the public API (nricp_dp.solve_route_b) from
-                 host arrays, host<->device copies inside the timed region,
-* ``roofline``   the dominant kernel's algorithmic bytes / its event time,
-* ``cpu_baseline`` the reference's own FP64 route A (compiled from its
-                 sources, oracle/_ref) on the host's cores.
+Printed (one JSON line on rank 0):
+* ``value``        batched wraps/s, inputs resident in HBM (CUDA events on
+                   the batch's stream; the 64 wraps' data, ~3 GB, exceeds L2
+                   and a 256 MB write flushes it between steps as well),
+* ``plain``        the same 64 wraps one at a time through the same engine,
+                   and ``batched_vs_plain``,
+* ``latency_ms``   per-wrap latency one at a time (p50/p99 over the wraps)
+                   and the batch's step time (p50/p99 over the steps),
+* ``e2e``          wraps/s through the public API (nricp_dp.solve_batch) from
+                   host arrays: host graph builds, uploads, hierarchy builds,
+                   the solve and the result download all inside the clock,
+* ``roofline``     the dominant kernel's algorithmic bytes over the batch
+                   run / its CUDA-event time, against the measured HBM peak,
+* ``fit``          max vertex error and final-energy error of the GPU route
+                   against the reference's FP64 route A on a sample,
+* ``cpu_baseline`` the reference's own route A (compiled from its sources,
+                   oracle/_ref) on the host cores, on a bounded sample,
+* ``single_wrap``  the large single wrap of config 2 (25k vertices onto a
+                   393k-triangle target, 2,000 nodes) one at a time.
 
-``--impl reference`` times that reference CPU route instead (the reference has
-no other implementation of this path that runs here).  With torchrun (N > 1)
-every rank wraps its own target: replicas, no collective on the data path.
+``--impl reference`` times that reference CPU route instead.  With torchrun
+(N > 1) every rank solves its own 64-wrap batch: replicas, no collective on
+the data path.
 """
 
 from __future__ import annotations
@@ -40,8 +54,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "wraps/sec"
-WORKLOAD = ("config 2: 25k-vertex template -> 400k-triangle target, "
-            "2,000 nodes (250/500/1000/2000), k=6, 4 levels, route B")
+WORKLOAD = ("config 3: 64 uneven wraps batched (template 5k-50k vertices log-uniform, "
+            "nodes = V/15 over 4 levels, k=6, target 50k-500k triangles log-uniform), route B")
+INSTANCES = 64
+REFERENCE_SAMPLE = 16   # wraps per CPU-reference sample
 
 
 def parse_args():
@@ -56,16 +72,34 @@ def parse_args():
     return p.parse_args()
 
 
-# ---------------------------------------------------------------------------
-# distributed plumbing (replicas)
-# ---------------------------------------------------------------------------
-
 def Ranks(gpus: int):
     """One process per GPU under torchrun (NCCL for the host bookkeeping:
     barrier, max of the times, sum of the work); a single process otherwise."""
     from nricp_b200.replicas import ReplicaGroup
 
     return ReplicaGroup(backend="nccl", timeout_s=600.0)
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def make_cases(seed: int):
+    from nricp_b200 import synthetic as S
+
+    return S.config3(seed, instances=INSTANCES, workers=min(16, host_cores()))
+
+
+def reference_options(options: dict) -> dict:
+    """The reference's data model caps the binding at four nodes and its graph
+    at 4-NN edges (src/core/sampling.h:17, graph.h:52-53)."""
+    out = dict(options)
+    out["max_nodes_per_vertex"] = 4
+    out["edge_neighbours"] = 4
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -127,82 +161,75 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# the reference CPU route (oracle/_ref) on all host cores
+# the reference CPU route (oracle/_ref) on the host's cores
 # ---------------------------------------------------------------------------
 
 def _reference_wrap(args):
-    """One wrap through the reference's own route A, in a worker process."""
-    seed, kind = args
+    """One config-3 wrap through the reference's own route A, in a worker."""
+    spec, kind = args
     sys.path.insert(0, str(ROOT))
     from nricp_b200 import synthetic as S
     from oracle.oracle import Oracle
 
-    case = S.config2(seed)
-    options = dict(case.options)
-    if kind == "reference":
-        # the reference's data model caps the binding at four nodes and its
-        # graph at 4-NN edges (src/core/sampling.h:17, graph.h:52-53)
-        options["max_nodes_per_vertex"] = 4
-        options["edge_neighbours"] = 4
+    case = S.config3_case(spec)
     t0 = time.perf_counter()
-    Oracle(kind).solve(*case.args(), **options)
-    return time.perf_counter() - t0
+    result = Oracle(kind).solve(*case.args(), **reference_options(case.options))
+    seconds = time.perf_counter() - t0
+    return seconds, result["vertices"], json.loads(result["report"])["energy"]["total"]
 
 
-def cpu_reference_sample(cores: int, seed: int) -> dict:
-    """`cores` independent wraps, one per process (route A is single-threaded
-    by construction), all at once: wraps/s of the host."""
+def cpu_reference_sample(seed: int, cores: int) -> dict:
+    """The sample's wraps, one per process (route A is single-threaded by
+    construction), all at once: wraps/s of the host on that sample."""
     import multiprocessing as mp
 
+    from nricp_b200 import synthetic as S
     from oracle.oracle import reference_available
 
     kind = "reference" if reference_available() else "restatement"
+    specs = S.config3_specs(seed, INSTANCES)
+    order = sorted(range(INSTANCES), key=lambda i: (specs[i][1], i))
+    picked = sorted(order[:REFERENCE_SAMPLE])
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        times = pool.map(_reference_wrap, [(seed + i, kind) for i in range(cores)])
+    with ctx.Pool(min(cores, len(picked))) as pool:
+        out = pool.map(_reference_wrap, [(specs[i], kind) for i in picked])
     elapsed = time.perf_counter() - t0
-    return {"value": cores / elapsed, "unit": METRIC, "cores": cores,
+    times = [o[0] for o in out]
+    sizes = [specs[i][1] for i in picked]
+    return {"value": len(picked) / elapsed, "unit": METRIC, "cores": min(cores, len(picked)),
             "kind": "reference" if kind == "reference" else "port",
-            "sample": (f"{cores} config-2 wraps (k=4, 4-NN: the reference's caps), one per "
-                       f"process on {cores} host cores, run to completion; "
-                       f"per-wrap {min(times):.1f}-{max(times):.1f} s"),
-            "seconds": elapsed}
-
-
-def host_cores() -> int:
-    try:
-        return len(os.sched_getaffinity(0))
-    except AttributeError:
-        return os.cpu_count() or 1
+            "sample": (f"the {len(picked)} smallest of the 64 config-3 wraps ({min(sizes)}-"
+                       f"{max(sizes)} template vertices; k=4, 4-NN: the reference's caps), one "
+                       f"per process, run to completion; per wrap {min(times):.1f}-"
+                       f"{max(times):.1f} s"),
+            "seconds": elapsed, "indices": picked,
+            "vertices": [o[1] for o in out], "energies": [o[2] for o in out]}
 
 
 def run_reference_arm(args, ranks):
     if ranks.rank != 0:
         return
-    cores = min(host_cores(), 64)
+    cores = host_cores()
     for _ in range(args.warmup):
         cpu_reference_warmup()
-    samples = []
-    for _ in range(args.steps):
-        samples.append(cpu_reference_sample(cores, args.seed))
+    samples = [cpu_reference_sample(args.seed, cores) for _ in range(args.steps)]
     value = statistics.median(s["value"] for s in samples)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * statistics.median(s["seconds"] for s in samples),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded numpy generator, nricp_b200.synthetic.config2)",
-        "config": {"workload": WORKLOAD, "model": None, "inputs": "host memory"},
-        "cpu_baseline": {k: samples[-1][k] for k in ("kind", "cores", "sample")} | {"value": value,
-                                                                                    "unit": METRIC},
+        "data": "synthetic (seeded numpy generator, nricp_b200.synthetic.config3)",
+        "config": {"workload": WORKLOAD, "inputs": "host memory"},
+        "cpu_baseline": {k: samples[-1][k] for k in ("kind", "cores", "sample")} | {
+            "value": value, "unit": METRIC},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 def cpu_reference_warmup():
-    sys.path.insert(0, str(ROOT))
     from nricp_b200 import synthetic as S
     from oracle.oracle import Oracle, reference_available
 
@@ -211,68 +238,58 @@ def cpu_reference_warmup():
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes per launch (the formulas of the design's roofline table)
+# algorithmic bytes (the formulas of the design's roofline table)
 # ---------------------------------------------------------------------------
 
 def query_bytes(s: dict) -> float:
-    # V (24 in + 33 out) + one read of the tree (2F x 32) + mesh (F x 12 + Vt x 24)
+    # per pass: V (24 in + 33 out) + one read of the tree (2F x 32) + mesh (F x 12 + Vt x 24)
     return s["vertices"] * 57 + s["target_triangles"] * 76 + s["target_vertices"] * 24
 
 
-def pcg_bytes(s: dict, iterations: int) -> float:
-    # per iteration N x 504 + (E + G) x 248
-    return iterations * (s["nodes"] * 504 + (s["edges"] + s["pairs"]) * 248)
+def pcg_bytes(s: dict) -> float:
+    # per iteration: N x 504 + (E + G) x 248
+    return s["nodes"] * 504 + (s["edges"] + s["pairs"]) * 248
 
 
 def assembly_bytes(s: dict) -> float:
-    # S x 98 + P x 106 + V x 98 + N x 168 + (E + G) x 144
+    # per pass: S x 98 + P x 106 + V x 98 + N x 168 + (E + G) x 144
     return (s["entries"] * 98 + s["pair_entries"] * 106 + s["vertices"] * 98 +
             s["nodes"] * 168 + (s["edges"] + s["pairs"]) * 144)
 
 
 def roofline(batch, peak_gbs: float) -> tuple[dict, dict]:
+    """Re-runs the batch with CUDA events around the query, the solve and the
+    assembly of every tick, then divides each kernel group's algorithmic bytes
+    over every wrap (per-level work counters of that run) by its event time."""
     records = batch.profile()
-    levels = batch.level_sizes(0, 0)["levels"]
-    sizes = [batch.level_sizes(0, l) for l in range(levels)]
-    kernels = {"query": [0.0, 0.0, 0], "pcg": [0.0, 0.0, 0], "assembly": [0.0, 0.0, 0]}
-    for r in records:
-        s = sizes[min(r["level"], levels - 1)]
-        if r["phase"] in (0, 1, 3):  # transfer / refresh / final: the query works
-            kernels["query"][0] += r["query_ms"]
-            kernels["query"][1] += query_bytes(s)
-            kernels["query"][2] += 1
-        if r["phase"] == 2 and r["pcg_iterations"] > 0:
-            kernels["pcg"][0] += r["pcg_ms"]
-            kernels["pcg"][1] += pcg_bytes(s, r["pcg_iterations"])
-            kernels["pcg"][2] += 1
-        if r["phase"] in (0, 1, 2):
-            kernels["assembly"][0] += r["assemble_ms"]
-            kernels["assembly"][1] += assembly_bytes(s)
-            kernels["assembly"][2] += 1
+    ms = {"query": sum(r["query_ms"] for r in records), "pcg": sum(r["pcg_ms"] for r in records),
+          "assembly": sum(r["assemble_ms"] for r in records)}
+    nbytes = {"query": 0.0, "pcg": 0.0, "assembly": 0.0}
+    launches = len(records)
+    work = {"pcg_iterations": 0, "solves": 0, "queries": 0, "assemblies": 0}
+    for i in range(len(batch)):
+        levels = batch.level_sizes(i, 0)["levels"]
+        for level in range(levels):
+            s = batch.level_sizes(i, level)
+            nbytes["query"] += s["queries"] * query_bytes(s)
+            nbytes["pcg"] += s["pcg_iterations"] * pcg_bytes(s)
+            nbytes["assembly"] += s["assemblies"] * assembly_bytes(s)
+            for k in work:
+                work[k] += s[k]
     total_tick = sum(r["tick_ms"] for r in records)
-    dominant = max(kernels, key=lambda k: kernels[k][0])
-    ms, nbytes, launches = kernels[dominant]
-    achieved = (nbytes / launches) / (ms / launches * 1e-3) / 1e9 if ms > 0 else 0.0
-    detail = {k: {"ms": v[0], "launches": v[2], "share_of_ticks": v[0] / total_tick if total_tick else 0,
-                  "gbs": (v[1] / (v[0] * 1e-3) / 1e9) if v[0] > 0 else 0.0}
-              for k, v in kernels.items()}
-    by_level = {}
-    for r in records:
-        if r["phase"] == 2:
-            entry = by_level.setdefault(r["level"], {"solves": 0, "iterations": 0, "pcg_ms": 0.0,
-                                                     "max_iterations": 0})
-            entry["solves"] += 1
-            entry["iterations"] += r["pcg_iterations"]
-            entry["pcg_ms"] += r["pcg_ms"]
-            entry["max_iterations"] = max(entry["max_iterations"], r["pcg_iterations"])
-    detail["pcg_by_level"] = by_level
-    detail["ticks"] = len(records)
+    dominant = max(ms, key=lambda k: ms[k])
+    achieved = nbytes[dominant] / (ms[dominant] * 1e-3) / 1e9 if ms[dominant] > 0 else 0.0
+    detail = {k: {"ms": ms[k], "share_of_ticks": ms[k] / total_tick if total_tick else 0.0,
+                  "algorithmic_gb": nbytes[k] / 1e9,
+                  "gbs": nbytes[k] / (ms[k] * 1e-3) / 1e9 if ms[k] > 0 else 0.0} for k in ms}
+    detail["ticks"] = launches
     detail["tick_ms_total"] = total_tick
+    detail["work"] = work
     line = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak_gbs,
             "unit": "GB/s", "frac": achieved / peak_gbs if peak_gbs else None,
-            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": None, "algorithmic_bytes_per_launch": nbytes / max(1, launches),
-            "avg_launch_us": 1000.0 * ms / max(1, launches)}
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": None,
+            "algorithmic_bytes_per_launch": nbytes[dominant] / max(1, launches),
+            "avg_launch_us": 1000.0 * ms[dominant] / max(1, launches)}
     return line, detail
 
 
@@ -294,6 +311,14 @@ def flush_l2():
     del buf
 
 
+def percentiles(values) -> dict:
+    v = sorted(values)
+    if not v:
+        return {}
+    pick = lambda q: v[min(len(v) - 1, int(math.ceil(q * len(v))) - 1)]  # noqa: E731
+    return {"p50": pick(0.50), "p99": pick(0.99), "n": len(v)}
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -305,10 +330,12 @@ def run_ours(args, ranks):
     from nricp_b200 import synthetic as S
 
     torch.cuda.set_device(ranks.local)
-    case = S.config2(args.seed + ranks.rank)
-    batch = dp.WrapBatch([(*case.args(), case.options)])
+    cases = make_cases(args.seed + ranks.rank)
+    tuples = [(*c.args(), c.options) for c in cases]
 
-    # ---- value: device-resident steps ----
+    # ---- value: the batch, device-resident ----
+    batch = dp.WrapBatch(tuples)
+    cluster = batch.tune(-1)
     for _ in range(max(3, args.warmup)):
         batch.step()
     step_ms = []
@@ -323,61 +350,106 @@ def run_ours(args, ranks):
     torch.cuda.synchronize()
     ranks.barrier()
     total_ms = ranks.max(sum(step_ms))
-    wraps = ranks.sum(float(args.steps))
+    wraps = ranks.sum(float(args.steps * len(cases)))
     value = wraps / (total_ms * 1e-3)
 
+    # ---- plain: the same wraps one at a time through the same engine ----
+    plain_ms = []
+    plain_results = []
+    for t in tuples:
+        one = dp.WrapBatch([t])
+        one.step()
+        plain_ms.append(one.step())
+        plain_results.append(one.result(0)["vertices"])
+        del one
+    plain_total = ranks.max(sum(plain_ms))
+    plain = ranks.sum(float(len(cases))) / (plain_total * 1e-3)
+    identical = sum(int(np.array_equal(plain_results[i], batch.result(i)["vertices"]))
+                    for i in range(len(cases)))
+
     # ---- e2e: the public API from host arrays ----
-    dp.solve_route_b(*case.args(), **case.options)  # warm
     dp.transfer_counters(reset=True)
     ranks.barrier()
-    e2e_steps = max(2, min(args.steps, 3))
+    e2e_steps = 2
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        dp.solve_route_b(*case.args(), **case.options)
+        dp.solve_batch(tuples)
     torch.cuda.synchronize()
     e2e_s = ranks.max(time.perf_counter() - t0)
     h2d, d2h = dp.transfer_counters(reset=True)
-    result_bytes = case.template_points.nbytes + 8 * 12 * batch.level_sizes(0, 3)["nodes"]
-    e2e = {"value": ranks.sum(float(e2e_steps)) / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": int(h2d / e2e_steps),
-           "d2h_bytes_per_step": int(d2h / e2e_steps + result_bytes)}
+    e2e = {"value": ranks.sum(float(e2e_steps * len(cases))) / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": int(h2d / e2e_steps), "d2h_bytes_per_step": int(d2h / e2e_steps)}
 
-    # ---- roofline of the dominant kernel ----
+    # ---- roofline of the dominant kernel over the batch ----
     roof, detail = (None, None)
     if not args.no_profile:
         roof, detail = roofline(batch, measured_peak())
 
-    result = batch.result(0)
-    report = json.loads(result["report"])
-
-    cpu = None
+    # ---- CPU reference sample and the fit against it ----
+    cpu, fit = None, None
     if ranks.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_sample(min(host_cores(), 64), args.seed)
+        cpu = cpu_reference_sample(args.seed, host_cores())
+        idx = cpu.pop("indices")
+        ref_vertices, ref_energies = cpu.pop("vertices"), cpu.pop("energies")
         cpu.pop("seconds", None)
+        same = [(*cases[i].args(), reference_options(cases[i].options)) for i in idx]
+        ours = dp.solve_batch(same)
+        errors, energy_errors = [], []
+        for i, mine, rv, re in zip(idx, ours, ref_vertices, ref_energies):
+            p = cases[i].target_points
+            diag = float(np.linalg.norm(p.max(0) - p.min(0)))
+            errors.append(float(np.abs(mine["vertices"] - rv).max()) / diag)
+            e = json.loads(mine["report"])["energy"]["total"]
+            energy_errors.append(abs(e - re) / abs(re) if re else abs(e))
+        order = sorted(range(len(errors)), key=lambda k: errors[k])
+        fit = {"against": "the reference's FP64 route A (oracle/_ref) on the CPU sample, "
+                          "same settings (k=4, 4-NN)",
+               "wraps": len(idx), "max_vertex_error_over_diag": max(errors),
+               "median_vertex_error_over_diag": errors[order[len(order) // 2]],
+               "max_final_energy_rel_error": max(energy_errors),
+               "wraps_within_1e-4": sum(1 for e in errors if e <= 1e-4)}
 
-    lat = sorted(step_ms)
+    # ---- the large single wrap (config 2), one at a time ----
+    single = None
+    if ranks.rank == 0:
+        c2 = S.config2(args.seed)
+        one = dp.WrapBatch([(*c2.args(), c2.options)])
+        one.step()
+        ms2 = [one.step() for _ in range(3)]
+        single = {"workload": "config 2: 25k-vertex template -> 393k-triangle target, 2,000 nodes, "
+                              "k=6, 4 levels, route B",
+                  "value": 1000.0 / statistics.median(ms2), "unit": METRIC,
+                  "ms": [round(x, 2) for x in ms2]}
+        del one
+
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ranks.world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-        "data": "synthetic (seeded numpy generator, nricp_b200.synthetic.config2)",
-        "config": {"workload": WORKLOAD, "model": None, "global_batch": ranks.world,
-                   "template_vertices": int(len(case.template_points)),
-                   "target_triangles": int(len(case.target_faces)),
+        "data": "synthetic (seeded numpy generator, nricp_b200.synthetic.config3)",
+        "config": {"workload": WORKLOAD, "wraps_per_gpu": len(cases),
+                   "template_vertices": [int(min(len(c.template_points) for c in cases)),
+                                         int(max(len(c.template_points) for c in cases))],
+                   "target_triangles": [int(min(len(c.target_faces) for c in cases)),
+                                        int(max(len(c.target_faces) for c in cases))],
                    "parallelism": f"replicas x{ranks.world}",
-                   "l2": "flushed (256 MB write) between timed steps",
+                   "solve_cluster": f"per-wrap classes (largest {cluster})",
+                   "l2": "inputs larger than L2 (~3 GB per batch), plus a 256 MB write between steps",
                    "precision": "FP32 assembly/matvec/traversal, FP64 state/energies/dots/Horn"},
-        "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-                       "steps": [round(x, 3) for x in step_ms]},
+        "plain": {"value": plain, "unit": METRIC,
+                  "how": "the same 64 wraps one at a time (a batch of one each), device-resident"},
+        "batched_vs_plain": value / plain if plain else None,
+        "bit_identical_alone_and_batched": f"{identical}/{len(cases)}",
+        "latency_ms": {"plain_wrap": percentiles(plain_ms), "batch_step": percentiles(step_ms)},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "e2e": e2e,
         "roofline": roof,
         "kernels": detail,
+        "fit": fit,
         "cpu_baseline": cpu,
-        "fit": {"energy": report["energy"]["total"],
-                "levels": [(l["outer_iterations"], l["inner_iterations"]) for l in report["levels"]]},
+        "single_wrap": single,
     }
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)

@@ -184,6 +184,40 @@ int nricp_session_vertices(NricpSession* session, double* out);
 int nricp_session_result(NricpSession* session, NricpResult* out);
 /* Schedule ticks run and kernels launched so far. */
 int nricp_session_ticks(NricpSession* session, long* ticks, long* launches);
+/* No reference counterpart.  A session's current linear system and the state
+ * it was assembled at, for checking the assembly against an FP64 restatement
+ * of the reference's fused_system (bindings.cpp:1328-1360, the same system
+ * as (J^T J, -J^T r)).  Call it when the session's phase is a solve
+ * attempt right after a refresh: the system is then the one assembled at
+ * the accepted state with the correspondences of that state.  All arrays are
+ * caller-allocated: rotations (nodes x 9), translations (nodes x 3),
+ * correspondence points and normals (template vertices x 3, normalised
+ * frame), robust weights (V), rejection codes (V), diagonal blocks
+ * (nodes x 36), right-hand side (nodes x 6), and for every off-diagonal block
+ * its node pair (a < b) and its (a, b) block (capacity x 2 and capacity x 36).
+ * Blocks appear once per smoothness edge and once per node pair that shares
+ * a vertex, so one pair may appear twice; their sum is the system's block.
+ * Also the damping of the next attempt and the last converged solve's
+ * increment (nodes x 6). */
+typedef struct NricpInspect {
+    int level, node_count, phase, off_count;     /* out */
+    int off_capacity;                            /* in */
+    double energies[5];                          /* out: accepted energy parts */
+    double* rotations;
+    double* translations;
+    double* corr_points;
+    double* corr_normals;
+    double* corr_robust;
+    uint8_t* corr_codes;
+    float* diag;
+    float* rhs;
+    int32_t* off_nodes;
+    float* off_blocks;
+    double damping;                              /* out: the next attempt's damping */
+    double* delta;                               /* nodes x 6: the last converged solve's increment */
+} NricpInspect;
+int nricp_session_inspect(NricpSession* session, NricpInspect* out);
+
 void nricp_session_destroy(NricpSession* session);
 
 /* ---- batches: many uneven wraps advanced by the same launches ----------- */

@@ -116,6 +116,20 @@ class TickRecord(C.Structure):
     ]
 
 
+class Inspect(C.Structure):
+    P = C.POINTER
+    _fields_ = [
+        ("level", C.c_int), ("node_count", C.c_int), ("phase", C.c_int), ("off_count", C.c_int),
+        ("off_capacity", C.c_int), ("energies", C.c_double * 5),
+        ("rotations", P(C.c_double)), ("translations", P(C.c_double)),
+        ("corr_points", P(C.c_double)), ("corr_normals", P(C.c_double)),
+        ("corr_robust", P(C.c_double)), ("corr_codes", P(C.c_uint8)),
+        ("diag", P(C.c_float)), ("rhs", P(C.c_float)),
+        ("off_nodes", P(C.c_int32)), ("off_blocks", P(C.c_float)),
+        ("damping", C.c_double), ("delta", P(C.c_double)),
+    ]
+
+
 # Defaults of the route functions, src/python/bindings.cpp:1470-1481.
 ROUTE_DEFAULTS: dict[str, Any] = dict(
     mask=None,

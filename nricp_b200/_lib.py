@@ -53,6 +53,7 @@ def _declare(lib: C.CDLL) -> None:
         "nricp_session_result": (C.c_int, [C.c_void_p, result_p]),
         "nricp_session_ticks": (C.c_int, [C.c_void_p, P(C.c_long), P(C.c_long)]),
         "nricp_session_destroy": (None, [C.c_void_p]),
+        "nricp_session_inspect": (C.c_int, [C.c_void_p, P(_abi.Inspect)]),
         "nricp_batch_create": (C.c_int, [desc_p, C.c_int, P(C.c_void_p)]),
         "nricp_batch_reset": (C.c_int, [C.c_void_p]),
         "nricp_batch_run": (C.c_int, [C.c_void_p]),

@@ -206,6 +206,10 @@ int nricp_session_ticks(NricpSession* s, long* ticks, long* launches) {
     });
 }
 
+int nricp_session_inspect(NricpSession* s, NricpInspect* out) {
+    return guarded([&] { s->batch.inspect(0, out); });
+}
+
 void nricp_session_destroy(NricpSession* s) { delete s; }
 
 // ---- one-call solves -------------------------------------------------------
@@ -385,7 +389,7 @@ int nricp_closest_points(const double* target_points, int vertex_count, const in
         const size_t o_n = reserve(sizeof(double) * normals.size());
         const size_t o_f = reserve(sizeof(int32_t) * 3 * face_count);
         const size_t o_nodes = reserve(sizeof(float4) * 4 * std::max(1, face_count - 1));
-        const size_t o_leaves = reserve(sizeof(float4) * 3 * face_count);
+        const size_t o_leaves = reserve(sizeof(float4) * kLeafFloat4s * face_count);
         const size_t o_q = reserve(sizeof(double) * 3 * std::max(1, query_count));
         const size_t o_op = reserve(sizeof(double) * 3 * std::max(1, query_count));
         const size_t o_on = reserve(sizeof(double) * 3 * std::max(1, query_count));
@@ -464,7 +468,7 @@ int nricp_lbvh_export(const double* target_points, int vertex_count, const int32
         const size_t o_p = reserve(sizeof(double) * 3 * vertex_count);
         const size_t o_f = reserve(sizeof(int32_t) * 3 * face_count);
         const size_t o_nodes = reserve(sizeof(float4) * 4 * std::max(1, face_count - 1));
-        const size_t o_leaves = reserve(sizeof(float4) * 3 * face_count);
+        const size_t o_leaves = reserve(sizeof(float4) * kLeafFloat4s * face_count);
         const size_t o_scratch = reserve(lbvh_scratch_bytes(face_count));
         check(cudaMalloc(&base, bytes), "cudaMalloc(lbvh)");
         std::unique_ptr<char, void (*)(char*)> guard(base, [](char* p) { cudaFree(p); });

@@ -145,9 +145,9 @@ struct WrapDev {
     const double* tgt_normals;    // Vt x 3 area-weighted, normalised
     const int32_t* tgt_faces;     // F x 3
     const float4* bvh_nodes;      // (F - 1) x 4 : child boxes + children
-    const float4* bvh_leaves;     // F x 3 : corners + triangle id, sorted
+    const float4* bvh_leaves;     // F x kLeafFloat4s: FP64 corners + triangle id, sorted
     int bvh_root;                 // encoded child (leaf flag in bit 31)
-    float rank_window;            // FP32 ranking error bound (distance, target units)
+    float rank_window;            // FP32 box-pruning slack (distance, normalised units)
     // levels
     LevelDev levels[kMaxLevels];
     // state: two buffers, `control.state` selects the accepted one
@@ -232,5 +232,7 @@ __device__ inline F3 mul3f(const float* m, F3 v) {
 
 // Leaf / internal child encoding of the traversal hierarchy.
 constexpr uint32_t kLeafBit = 0x80000000u;
+// A hierarchy leaf: the triangle's three FP64 corners and its index, 80 bytes.
+constexpr int kLeafFloat4s = 5;
 
 }  // namespace nricp_b200

@@ -11,11 +11,11 @@
 // visit costs one 64-byte load instead of three dependent ones.
 //
 // Query (thread per template vertex): the previous correspondence's triangle
-// seeds the search radius, the traversal walks FP32 boxes and triangles with
-// a fixed-depth stack whose overflow is reported (never silently pruned), and
-// the winning triangle is re-evaluated in FP64 so that the correspondence
-// point, normal and distance are those of the reference's FP64 closest-point
-// routine (src/geometry/closest_point.cpp:24-121).
+// seeds the search radius, the traversal prunes FP32 boxes with a fixed-depth
+// stack whose overflow is reported (never silently pruned), and every
+// triangle it reaches is measured with the reference's FP64 closest-point
+// routine (src/geometry/closest_point.cpp:24-121), so the winner, its point,
+// normal and distance are those of an FP64 brute-force scan.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -320,12 +320,15 @@ __global__ void k_pack_leaves(const double* __restrict__ points, const int32_t* 
     if (i >= n) return;
     const int tri = (int)order[i];
     const int32_t* f = faces + (long)tri * 3;
-    float c[9];
+    double c[9];
     for (int k = 0; k < 3; ++k)
-        for (int a = 0; a < 3; ++a) c[k * 3 + a] = __double2float_rn(points[(long)f[k] * 3 + a]);
-    leaves[(long)i * 3 + 0] = make_float4(c[0], c[1], c[2], c[3]);
-    leaves[(long)i * 3 + 1] = make_float4(c[4], c[5], c[6], c[7]);
-    leaves[(long)i * 3 + 2] = make_float4(c[8], __int_as_float(tri), 0.0f, 0.0f);
+        for (int a = 0; a < 3; ++a) c[k * 3 + a] = points[(long)f[k] * 3 + a];
+    double2* l = reinterpret_cast<double2*>(leaves) + (long)i * kLeafFloat4s;
+    l[0] = make_double2(c[0], c[1]);
+    l[1] = make_double2(c[2], c[3]);
+    l[2] = make_double2(c[4], c[5]);
+    l[3] = make_double2(c[6], c[7]);
+    l[4] = make_double2(c[8], __longlong_as_double((long long)tri));
 }
 
 int blocks_for(long n, int threads = kThreads) { return (int)((n + threads - 1) / threads); }
@@ -353,7 +356,7 @@ size_t lbvh_scratch_bytes(int n) {
 }
 
 // Builds the hierarchy over `n` target triangles into `nodes` ((n-1) x 4
-// float4) and `leaves` (n x 3 float4) using `scratch`; optionally exports the
+// float4) and `leaves` (n x kLeafFloat4s float4) using `scratch`; optionally exports the
 // canonical arrays (sorted codes, permutation, Karras children) for parity
 // tests.  Returns the encoded root.
 uint32_t lbvh_build(const double* points, const int32_t* faces, int n, void* scratch,
@@ -425,57 +428,6 @@ __device__ inline float box_distance(F3 p, float lx, float ly, float lz, float h
     const float dy = fmaxf(fmaxf(ly - p.y, p.y - hy), 0.0f);
     const float dz = fmaxf(fmaxf(lz - p.z, p.z - hz), 0.0f);
     return dx * dx + dy * dy + dz * dz;
-}
-
-// Squared distance from p to a triangle (Voronoi-region closest point,
-// closest_point.cpp:24-121), FP32, for ranking candidates.
-__device__ inline float triangle_distance(F3 p, F3 a, F3 b, F3 c) {
-    const F3 ab = b - a, ac = c - a, ap = p - a;
-    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
-    F3 q;
-    if (d1 <= 0.0f && d2 <= 0.0f) {
-        q = a;
-    } else {
-        const F3 bp = p - b;
-        const float d3 = dot(ab, bp), d4 = dot(ac, bp);
-        if (d3 >= 0.0f && d4 <= d3) {
-            q = b;
-        } else {
-            const float vc = d1 * d4 - d3 * d2;
-            if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
-                const float den = d1 - d3;
-                q = a + ab * (den != 0.0f ? d1 / den : 0.0f);
-            } else {
-                const F3 cp = p - c;
-                const float d5 = dot(ab, cp), d6 = dot(ac, cp);
-                if (d6 >= 0.0f && d5 <= d6) {
-                    q = c;
-                } else {
-                    const float vb = d5 * d2 - d1 * d6;
-                    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
-                        const float den = d2 - d6;
-                        q = a + ac * (den != 0.0f ? d2 / den : 0.0f);
-                    } else {
-                        const float va = d3 * d6 - d5 * d4;
-                        if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
-                            const float den = (d4 - d3) + (d5 - d6);
-                            q = b + (c - b) * (den != 0.0f ? (d4 - d3) / den : 0.0f);
-                        } else {
-                            const float den = va + vb + vc;
-                            if (fabsf(den) < 1e-30f) {
-                                q = a;
-                            } else {
-                                const float v = vb / den, w = vc / den;
-                                q = a + ab * v + ac * w;
-                            }
-                        }
-                    }
-                }
-            }
-        }
-    }
-    const F3 d = q - p;
-    return dot(d, d);
 }
 
 // FP64 closest point with barycentrics, the reference routine's exact steps
@@ -560,51 +512,42 @@ __device__ inline double triangle_distance_fp64(const WrapDev& w, D3 q, int tri)
     return vdot(d, d);
 }
 
-// Nearest target triangle for `q`.  The walk ranks boxes and triangles in
-// FP32; whenever a triangle lands within the FP32 error window of the best so
-// far (`w.rank_window`, a distance in the target's units) the two are
-// re-ranked in FP64, and exact FP64 ties go to the lower triangle index -- the
-// rule of an FP64 brute-force scan.  `seed` is a triangle whose distance
-// bounds the search from the start.  Returns the winner, or -1.
+// FP64 squared distance from q to the triangle of leaf `leaf` (its corners
+// are stored in FP64), and the triangle's index.
+__device__ inline double leaf_distance(const WrapDev& w, int leaf, D3 q, int* tri) {
+    const double2* l = reinterpret_cast<const double2*>(w.bvh_leaves) + (long)leaf * (kLeafFloat4s);
+    const double2 l0 = __ldg(l), l1 = __ldg(l + 1), l2 = __ldg(l + 2), l3 = __ldg(l + 3),
+                  l4 = __ldg(l + 4);
+    *tri = (int)__double_as_longlong(l4.y);
+    double bary[3];
+    const D3 c = closest_point_fp64(q, {l0.x, l0.y, l1.x}, {l1.y, l2.x, l2.y}, {l3.x, l3.y, l4.x}, bary);
+    const D3 d = vsub(c, q);
+    return vdot(d, d);
+}
+
+// Nearest target triangle for `q`: the FP64 brute-force answer (smallest
+// FP64 distance from the reference's closest-point routine, exact ties to the
+// lowest triangle index), found by walking the hierarchy.  Boxes are pruned
+// in FP32, which is well conditioned (a box distance is a clamp and three
+// squares), with `w.rank_window` of slack, far above the rounding of the FP32
+// boxes and query; every triangle reached is measured in FP64 -- an FP32
+// closest-point routine can misplace its point on thin sliver triangles by
+// far more than any fixed window.  `seed` is a triangle whose distance bounds
+// the search from the start.  Returns the winner, or -1.
 __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* overflow) {
-    const float window = w.rank_window;
-    float best = 3.4e38f;    // smallest FP32 squared distance seen
-    float bound = 3.4e38f;   // (sqrt(best) + window)^2: prune at or beyond
+    const double slack = (double)w.rank_window;
+    double best = 1e300;     // FP64 squared distance of the best triangle so far
+    float bound = 3.4e38f;   // FP32 pruning radius^2: (sqrt(best) + slack)^2, rounded up
     int best_tri = -1;
-    double best64 = 0.0;
-    bool best64_valid = false;
-    auto consider = [&](int tri, float d) {
-        if (!(d < bound)) return;
-        if (best_tri < 0 || sqrtf(d) + window < sqrtf(best)) {
-            best_tri = tri;
-            best64_valid = false;
-        } else {
-            // within the window of the current best: decide in FP64
-            if (!best64_valid) {
-                best64 = triangle_distance_fp64(w, q64, best_tri);
-                best64_valid = true;
-            }
-            const double d64 = triangle_distance_fp64(w, q64, tri);
-            if (d64 < best64 || (d64 == best64 && tri < best_tri)) {
-                best_tri = tri;
-                best64 = d64;
-            }
-        }
-        if (d < best) {
+    auto consider = [&](int tri, double d) {
+        if (d < best || (d == best && tri < best_tri)) {
             best = d;
-            const float r = sqrtf(best) + window;
-            bound = r * r;
+            best_tri = tri;
+            const double r = sqrt(best) + slack;
+            bound = __double2float_ru(r * r);
         }
     };
-    if (seed >= 0 && seed < w.F) {
-        const int32_t* f = w.tgt_faces + (long)seed * 3;
-        F3 c[3];
-        for (int k = 0; k < 3; ++k)
-            c[k] = {__double2float_rn(w.tgt_points[(long)f[k] * 3]),
-                    __double2float_rn(w.tgt_points[(long)f[k] * 3 + 1]),
-                    __double2float_rn(w.tgt_points[(long)f[k] * 3 + 2])};
-        consider(seed, triangle_distance(q, c[0], c[1], c[2]));
-    }
+    if (seed >= 0 && seed < w.F) consider(seed, triangle_distance_fp64(w, q64, seed));
     uint32_t stack[kStackDepth];
     float stack_d[kStackDepth];
     int sp = 0;
@@ -619,14 +562,9 @@ __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* o
             break;
         }
         if (node & kLeafBit) {
-            const int leaf = (int)(node & ~kLeafBit);
-            const float4 l0 = __ldg(&w.bvh_leaves[(long)leaf * 3 + 0]);
-            const float4 l1 = __ldg(&w.bvh_leaves[(long)leaf * 3 + 1]);
-            const float4 l2 = __ldg(&w.bvh_leaves[(long)leaf * 3 + 2]);
-            const int tri = __float_as_int(l2.y);
-            if (tri != seed)
-                consider(tri, triangle_distance(q, {l0.x, l0.y, l0.z}, {l0.w, l1.x, l1.y},
-                                                {l1.z, l1.w, l2.x}));
+            int tri;
+            const double d = leaf_distance(w, (int)(node & ~kLeafBit), q64, &tri);
+            if (tri != seed) consider(tri, d);
         } else {
             const float4* nd = w.bvh_nodes + (long)node * 4;
             const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);

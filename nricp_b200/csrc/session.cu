@@ -213,7 +213,7 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     const size_t o_tgt_normals = a.reserve(sizeof(double) * 3 * w.Vt);
     const size_t o_tgt_faces = a.reserve(sizeof(int32_t) * 3 * w.F);
     const size_t o_bvh_nodes = a.reserve(sizeof(float4) * 4 * std::max(1, w.F - 1));
-    const size_t o_bvh_leaves = a.reserve(sizeof(float4) * 3 * w.F);
+    const size_t o_bvh_leaves = a.reserve(sizeof(float4) * kLeafFloat4s * w.F);
     // levels
     std::vector<size_t> level_base(w.levels);
     for (int l = 0; l < w.levels; ++l) level_base[l] = a.reserve(bytes_of_layout(w.layouts[l]));
@@ -757,6 +757,45 @@ void Batch::finish() {
 }
 
 const WrapControl& Batch::control(int i) const { return host_controls_[i]; }
+
+void Batch::inspect(int i, NricpInspect* out) {
+    pull_controls();
+    const Wrap& w = *wraps_[i];
+    const WrapControl& c = host_controls_[i];
+    const int level = std::min(c.level, w.levels - 1);
+    const LevelLayout& L = w.layouts[level];
+    const int N = L.node_count, V = w.V;
+    const int K = L.edge_count + L.pair_count;
+    out->level = level;
+    out->node_count = N;
+    out->phase = c.phase;
+    out->off_count = K;
+    for (int k = 0; k < kEnergyKinds; ++k) out->energies[k] = c.energy_parts[k];
+    if (out->off_capacity < K) throw InvalidArgument("off-diagonal capacity too small");
+    const WrapDev& D = w.dev;
+    auto get = [this](void* dst, const void* src, size_t bytes) {
+        check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_), "inspect");
+    };
+    get(out->rotations, D.rot[c.state], sizeof(double) * 9 * N);
+    get(out->translations, D.trans[c.state], sizeof(double) * 3 * N);
+    get(out->corr_points, D.corr_point, sizeof(double) * 3 * V);
+    get(out->corr_normals, D.corr_normal, sizeof(double) * 3 * V);
+    get(out->corr_robust, D.robust, sizeof(double) * V);
+    get(out->corr_codes, D.corr_code, V);
+    get(out->diag, D.diag[c.system], sizeof(float) * 36 * N);
+    get(out->rhs, D.rhs[c.system], sizeof(float) * 6 * N);
+    get(out->delta, D.delta, sizeof(double) * 6 * N);
+    out->damping = c.damping;
+    std::vector<float> rows(L.row_entry.size() / 2 * 36);
+    if (!rows.empty()) get(rows.data(), D.offdiag[c.system], sizeof(float) * rows.size());
+    check(cudaStreamSynchronize(stream_), "inspect");
+    for (int k = 0; k < K; ++k) {
+        out->off_nodes[k * 2] = L.offdiag_nodes[k * 2];
+        out->off_nodes[k * 2 + 1] = L.offdiag_nodes[k * 2 + 1];
+        const float* block = rows.data() + static_cast<size_t>(L.offdiag_slots[k * 2]) * 36;
+        std::copy(block, block + 36, out->off_blocks + static_cast<size_t>(k) * 36);
+    }
+}
 
 // Result of wrap `i` in the caller's units (route_result_to_dict,
 // src/python/bindings.cpp:674-710).

@@ -74,6 +74,8 @@ public:
 
     int size() const { return static_cast<int>(wraps_.size()); }
     const WrapControl& control(int i) const;
+    // The current system of wrap `i` and the state it was assembled at.
+    void inspect(int i, NricpInspect* out);
     void result(int i, NricpResult* out);
     void current_vertices(int i, double* out);
     int finest_nodes(int i) const;

@@ -220,6 +220,39 @@ class RouteBSession:
         check(load().nricp_session_ticks(self._handle, C.byref(t), C.byref(l)))
         return t.value, l.value
 
+    def inspect(self) -> dict:
+        """The current linear system and the state it was assembled at (no
+        reference counterpart; for checking the assembly): phase, level,
+        accepted rotations / translations, correspondences in the solver's
+        normalised frame, the FP32 diagonal blocks, right-hand side and
+        off-diagonal (a, b) blocks, and the accepted energy parts."""
+        n_max = max(self._levels)
+        v = self._desc.template_points.shape[0]
+        cap = max(1, n_max * 64)
+        out = {"rotations": np.zeros((n_max, 3, 3)), "translations": np.zeros((n_max, 3)),
+               "corr_points": np.zeros((v, 3)), "corr_normals": np.zeros((v, 3)),
+               "corr_robust": np.zeros(v), "corr_codes": np.zeros(v, np.uint8),
+               "diag": np.zeros((n_max, 6, 6), np.float32), "rhs": np.zeros((n_max, 6), np.float32),
+               "off_nodes": np.zeros((cap, 2), np.int32), "off_blocks": np.zeros((cap, 6, 6), np.float32),
+               "delta": np.zeros((n_max, 6))}
+        s = _abi.Inspect()
+        s.off_capacity = cap
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+        s.rotations, s.translations = P(out["rotations"], C.c_double), P(out["translations"], C.c_double)
+        s.corr_points, s.corr_normals = P(out["corr_points"], C.c_double), P(out["corr_normals"], C.c_double)
+        s.corr_robust, s.corr_codes = P(out["corr_robust"], C.c_double), P(out["corr_codes"], C.c_uint8)
+        s.diag, s.rhs = P(out["diag"], C.c_float), P(out["rhs"], C.c_float)
+        s.off_nodes, s.off_blocks = P(out["off_nodes"], C.c_int32), P(out["off_blocks"], C.c_float)
+        s.delta = P(out["delta"], C.c_double)
+        check(load().nricp_session_inspect(self._handle, C.byref(s)))
+        n, k = s.node_count, s.off_count
+        for key in ("rotations", "translations", "diag", "rhs", "delta"):
+            out[key] = out[key][:n]
+        out["off_nodes"], out["off_blocks"] = out["off_nodes"][:k], out["off_blocks"][:k]
+        out.update(level=s.level, node_count=n, phase=s.phase, energies=list(s.energies),
+                   damping=s.damping)
+        return out
+
 
 def device_info() -> dict:
     """Report whether the accelerated path can run here, and on what."""

@@ -49,6 +49,7 @@ STRUCTS = {
     "NricpResult": _abi.Result,
     "NricpProgress": _abi.Progress,
     "NricpTickRecord": _abi.TickRecord,
+    "NricpInspect": _abi.Inspect,
 }
 
 
