@@ -272,6 +272,53 @@ int nricp_batch_solve(const NricpSolveDesc* descs, int count, NricpResult* resul
 
 /* ---- components ---------------------------------------------------------- */
 
+/* ---- serving: continuous batching (no reference counterpart) ----------
+ * The reference solves one wrap per call.  A server keeps a set of resident
+ * wrap slots on one device and advances every running wrap by the same
+ * launches, tick by tick; requests that arrive while others run are
+ * prepared on host threads (graph and level layouts, cached per template),
+ * admitted into a free slot as soon as one is free and the device-memory
+ * budget allows, and retired -- result downloaded -- when their schedule
+ * ends.  A wrap's result does not depend on what else shares its launches:
+ * it is bit-identical to the same wrap solved alone. */
+typedef struct NricpServer NricpServer;
+typedef struct NricpServerConfig {
+    size_t memory_budget_bytes;  /* device bytes resident wraps may hold; 0: 90 % of free memory */
+    int max_slots;               /* wraps resident at once (1..1024) */
+    int prep_threads;            /* host threads preparing requests; 0: half the cores */
+    int pcg_cluster;             /* solve cluster size, a power of two up to 16; 0: by load */
+    int ticks_per_poll;          /* ticks launched between looks at the wraps' progress */
+} NricpServerConfig;
+typedef struct NricpServerStats {
+    long submitted, completed, failed, waiting, running;
+    double latency_p50_ms, latency_p99_ms, latency_mean_ms;  /* submit -> result ready */
+    double queue_p50_ms;                                     /* submit -> admitted */
+    double wraps_per_second;     /* completed / (last completion - first submission) */
+    long ticks, launches, captures;
+    size_t resident_bytes, peak_resident_bytes;
+    int slots_used;
+} NricpServerStats;
+/* Request status from nricp_server_poll. */
+enum { NRICP_REQUEST_WAITING = 0, NRICP_REQUEST_RUNNING = 1, NRICP_REQUEST_DONE = 2,
+       NRICP_REQUEST_FAILED = 3 };
+
+void nricp_server_default_config(NricpServerConfig* config);
+int nricp_server_create(const NricpServerConfig* config, NricpServer** out);
+/* Copies the inputs and validates them (NRICP_ERR_INVALID with the
+ * reference's messages); the request then runs in the background. */
+int nricp_server_submit(NricpServer* server, const NricpSolveDesc* desc, long* id);
+/* Status of a request and, once done, its latency (submit to result ready). */
+int nricp_server_poll(NricpServer* server, long id, int* status, double* latency_seconds);
+/* Blocks until the request is done or failed, or `timeout_seconds` pass
+ * (NRICP_ERR_TIMEOUT). */
+int nricp_server_wait(NricpServer* server, long id, double timeout_seconds);
+/* Copies a done request's result (sizes as nricp_solve's) and forgets it; a
+ * failed request returns its error. */
+int nricp_server_result(NricpServer* server, long id, NricpResult* out);
+int nricp_server_stats(NricpServer* server, NricpServerStats* out);
+/* Stops the server; requests still running are abandoned. */
+void nricp_server_destroy(NricpServer* server);
+
 /* build_template_graph(...) (bindings.cpp:886-925), one level: the
  * normalisation, the sampled nodes, the bindings (stride NRICP_MAX_SLOTS) and
  * the k-NN edges of `level`. */

@@ -130,6 +130,29 @@ class Inspect(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("memory_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("prep_threads", C.c_int),
+        ("pcg_cluster", C.c_int), ("ticks_per_poll", C.c_int),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_long), ("completed", C.c_long), ("failed", C.c_long),
+        ("waiting", C.c_long), ("running", C.c_long),
+        ("latency_p50_ms", C.c_double), ("latency_p99_ms", C.c_double),
+        ("latency_mean_ms", C.c_double), ("queue_p50_ms", C.c_double),
+        ("wraps_per_second", C.c_double),
+        ("ticks", C.c_long), ("launches", C.c_long), ("captures", C.c_long),
+        ("resident_bytes", C.c_size_t), ("peak_resident_bytes", C.c_size_t),
+        ("slots_used", C.c_int),
+    ]
+
+
+REQUEST_STATES = {0: "waiting", 1: "running", 2: "done", 3: "failed"}
+
+
 # Defaults of the route functions, src/python/bindings.cpp:1470-1481.
 ROUTE_DEFAULTS: dict[str, Any] = dict(
     mask=None,

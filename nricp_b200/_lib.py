@@ -74,6 +74,14 @@ def _declare(lib: C.CDLL) -> None:
         "nricp_lbvh_export_static": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_void_p, C.c_void_p]),
+        "nricp_server_default_config": (None, [P(_abi.ServerConfig)]),
+        "nricp_server_create": (C.c_int, [P(_abi.ServerConfig), P(C.c_void_p)]),
+        "nricp_server_submit": (C.c_int, [C.c_void_p, desc_p, P(C.c_long)]),
+        "nricp_server_poll": (C.c_int, [C.c_void_p, C.c_long, P(C.c_int), P(C.c_double)]),
+        "nricp_server_wait": (C.c_int, [C.c_void_p, C.c_long, C.c_double]),
+        "nricp_server_result": (C.c_int, [C.c_void_p, C.c_long, result_p]),
+        "nricp_server_stats": (C.c_int, [C.c_void_p, P(_abi.ServerStats)]),
+        "nricp_server_destroy": (None, [C.c_void_p]),
         "nricp_default_desc": (None, [desc_p]),
         "nricp_default_level": (None, [P(_abi.LevelSettings)]),
     }

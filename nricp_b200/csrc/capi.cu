@@ -36,6 +36,9 @@ int guarded(F&& body) {
     } catch (const InvalidArgument& e) {
         g_last_error = e.what();
         return NRICP_ERR_INVALID;
+    } catch (const TimeoutError& e) {
+        g_last_error = e.what();
+        return NRICP_ERR_TIMEOUT;
     } catch (const CapacityError& e) {
         g_last_error = e.what();
         return NRICP_ERR_CAPACITY;
@@ -483,5 +486,57 @@ int nricp_lbvh_export(const double* target_points, int vertex_count, const int32
         cudaStreamDestroy(stream);
     });
 }
+
+
+// ---- serving -------------------------------------------------------------
+
+struct NricpServer {
+    explicit NricpServer(const NricpServerConfig& c) : server(c) {}
+    Server server;
+};
+
+void nricp_server_default_config(NricpServerConfig* c) {
+    c->memory_budget_bytes = 0;
+    c->max_slots = 64;
+    c->prep_threads = 0;
+    c->pcg_cluster = 0;
+    c->ticks_per_poll = 8;
+}
+
+int nricp_server_create(const NricpServerConfig* config, NricpServer** out) {
+    *out = nullptr;
+    return guarded([&] {
+        require_device();
+        NricpServerConfig c;
+        nricp_server_default_config(&c);
+        if (config) c = *config;
+        *out = new NricpServer(c);
+    });
+}
+
+int nricp_server_submit(NricpServer* s, const NricpSolveDesc* desc, long* id) {
+    return guarded([&] { *id = s->server.submit(*desc); });
+}
+
+int nricp_server_poll(NricpServer* s, long id, int* status, double* latency_seconds) {
+    return guarded([&] { *status = s->server.poll(id, latency_seconds); });
+}
+
+int nricp_server_wait(NricpServer* s, long id, double timeout_seconds) {
+    return guarded([&] {
+        if (!s->server.wait(id, timeout_seconds))
+            throw TimeoutError("request " + std::to_string(id) + " did not finish in time");
+    });
+}
+
+int nricp_server_result(NricpServer* s, long id, NricpResult* out) {
+    return guarded([&] { s->server.result(id, out); });
+}
+
+int nricp_server_stats(NricpServer* s, NricpServerStats* out) {
+    return guarded([&] { *out = s->server.stats(); });
+}
+
+void nricp_server_destroy(NricpServer* s) { delete s; }
 
 }  // extern "C"

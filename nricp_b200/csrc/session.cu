@@ -8,6 +8,10 @@
 // the caller advances one tick at a time.
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -64,8 +68,8 @@ private:
     size_t size_ = 0;
 };
 
-// Candidates whose FP32 distances are this close (relative to the target's
-// diagonal) are re-ranked in FP64.
+// Slack of the FP32 box pruning in the closest-point walk, relative to the
+// target's diagonal: far above the rounding of FP32 boxes and queries.
 constexpr double kRankWindow = 4e-6;
 
 double target_diagonal(const std::vector<double>& p) {
@@ -194,7 +198,7 @@ size_t bytes_of_layout(const LevelLayout& L) {
 
 // Lays out, allocates and fills the wrap's device arena; builds the target's
 // hierarchy.  `control` is this wrap's slot in the batch's control array.
-void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
+size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool plan_only = false) {
     const NricpSolveDesc& d = w.desc;
     const int V = w.V, N = std::max(1, w.max_nodes), B = std::max(1, w.max_offdiag);
     Arena& a = w.arena;
@@ -254,6 +258,11 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     const size_t o_records = a.reserve(sizeof(LevelRecord) * w.levels);
     const size_t o_lstats = a.reserve(sizeof(CorrStats) * w.levels);
     const size_t o_fstats = a.reserve(sizeof(CorrStats));
+    if (plan_only) {  // the arena's size only, nothing allocated
+        const size_t bytes = a.size() + sizeof(double) * 9 * N + sizeof(LevelRecord) * w.levels;
+        a = Arena();
+        return bytes;
+    }
     a.allocate();
 
     // ---- fill the descriptor ----
@@ -396,7 +405,7 @@ void prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream) {
     D.final_stats = a.at<CorrStats>(o_fstats);
     D.control = control;
     w.control = control;
-
+    return a.size();
 }
 
 // Puts a wrap back at the start of its schedule: identity transforms, no
@@ -797,32 +806,57 @@ void Batch::inspect(int i, NricpInspect* out) {
     }
 }
 
-// Result of wrap `i` in the caller's units (route_result_to_dict,
-// src/python/bindings.cpp:674-710).
-void Batch::result(int i, NricpResult* out) {
-    Wrap& w = *wraps_[i];
-    const WrapControl& c = host_controls_[i];
+namespace {
+
+// v' = sum w (R (v - g) + g + t), then back to the caller's units
+// (mesh.cpp:189-193).
+std::vector<double> evaluate_host(const Wrap& w, const std::vector<double>& rot,
+                                  const std::vector<double>& trans, int level) {
+    const LevelLayout& L = w.layouts[level];
+    const std::vector<double> tpl = normalized(w.template_in.data(), w.V, w.graph.center, w.graph.scale);
+    std::vector<double> out(static_cast<size_t>(w.V) * 3);
+    for (int v = 0; v < w.V; ++v) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < L.bind_counts[v]; ++k) {
+            const int j = L.bind_nodes[v * NRICP_MAX_SLOTS + k];
+            const double wt = L.bind_weights[v * NRICP_MAX_SLOTS + k];
+            const double* g = &L.rest[j * 3];
+            const double* R = &rot[j * 9];
+            const double p[3] = {tpl[v * 3] - g[0], tpl[v * 3 + 1] - g[1], tpl[v * 3 + 2] - g[2]};
+            for (int r = 0; r < 3; ++r) {
+                const double a = R[r * 3] * p[0] + R[r * 3 + 1] * p[1] + R[r * 3 + 2] * p[2];
+                s[r] = s[r] + ((a + g[r]) + trans[j * 3 + r]) * wt;
+            }
+        }
+        for (int r = 0; r < 3; ++r) out[v * 3 + r] = s[r] / w.graph.scale + w.graph.center[r];
+    }
+    return out;
+}
+
+// Result of one wrap in the caller's units (route_result_to_dict,
+// src/python/bindings.cpp:674-710), from its control `c` as last pulled.
+void write_result(const Wrap& w, const WrapControl& c, cudaStream_t stream, NricpResult* out) {
     const int level = std::min(c.level, w.levels - 1);
     const int N = w.layouts[level].node_count;
     std::vector<double> rot(static_cast<size_t>(N) * 9), trans(static_cast<size_t>(N) * 3);
     check(cudaMemcpyAsync(rot.data(), w.dev.rot[c.state], sizeof(double) * rot.size(),
-                          cudaMemcpyDeviceToHost, stream_), "download rot");
+                          cudaMemcpyDeviceToHost, stream), "download rot");
     check(cudaMemcpyAsync(trans.data(), w.dev.trans[c.state], sizeof(double) * trans.size(),
-                          cudaMemcpyDeviceToHost, stream_), "download trans");
+                          cudaMemcpyDeviceToHost, stream), "download trans");
     std::vector<LevelRecord> records(w.levels);
     std::vector<CorrStats> lstats(w.levels);
     CorrStats fstats;
     check(cudaMemcpyAsync(records.data(), w.dev.records, sizeof(LevelRecord) * w.levels,
-                          cudaMemcpyDeviceToHost, stream_), "download records");
+                          cudaMemcpyDeviceToHost, stream), "download records");
     check(cudaMemcpyAsync(lstats.data(), w.dev.level_stats, sizeof(CorrStats) * w.levels,
-                          cudaMemcpyDeviceToHost, stream_), "download stats");
+                          cudaMemcpyDeviceToHost, stream), "download stats");
     check(cudaMemcpyAsync(&fstats, w.dev.final_stats, sizeof(CorrStats), cudaMemcpyDeviceToHost,
-                          stream_), "download stats");
-    check(cudaStreamSynchronize(stream_), "download");
+                          stream), "download stats");
+    check(cudaStreamSynchronize(stream), "download");
     g_transfers.d2h += sizeof(double) * (rot.size() + trans.size()) +
                        sizeof(LevelRecord) * records.size() + sizeof(CorrStats) * (lstats.size() + 1) +
                        sizeof(WrapControl);
-    const std::vector<double> vertices = evaluate_host(i, rot, trans, level);
+    const std::vector<double> vertices = evaluate_host(w, rot, trans, level);
     if (out->vertices) std::memcpy(out->vertices, vertices.data(), sizeof(double) * vertices.size());
     if (out->rotations) std::memcpy(out->rotations, rot.data(), sizeof(double) * rot.size());
     if (out->translations) std::memcpy(out->translations, trans.data(), sizeof(double) * trans.size());
@@ -853,30 +887,13 @@ void Batch::result(int i, NricpResult* out) {
     }
 }
 
-// v' = sum w (R (v - g) + g + t), then back to the caller's units
-// (mesh.cpp:189-193).
+}  // namespace
+
+void Batch::result(int i, NricpResult* out) { write_result(*wraps_[i], host_controls_[i], stream_, out); }
+
 std::vector<double> Batch::evaluate_host(int i, const std::vector<double>& rot,
                                          const std::vector<double>& trans, int level) const {
-    const Wrap& w = *wraps_[i];
-    const LevelLayout& L = w.layouts[level];
-    const std::vector<double> tpl = normalized(w.template_in.data(), w.V, w.graph.center, w.graph.scale);
-    std::vector<double> out(static_cast<size_t>(w.V) * 3);
-    for (int v = 0; v < w.V; ++v) {
-        double s[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < L.bind_counts[v]; ++k) {
-            const int j = L.bind_nodes[v * NRICP_MAX_SLOTS + k];
-            const double wt = L.bind_weights[v * NRICP_MAX_SLOTS + k];
-            const double* g = &L.rest[j * 3];
-            const double* R = &rot[j * 9];
-            const double p[3] = {tpl[v * 3] - g[0], tpl[v * 3 + 1] - g[1], tpl[v * 3 + 2] - g[2]};
-            for (int r = 0; r < 3; ++r) {
-                const double a = R[r * 3] * p[0] + R[r * 3 + 1] * p[1] + R[r * 3 + 2] * p[2];
-                s[r] = s[r] + ((a + g[r]) + trans[j * 3 + r]) * wt;
-            }
-        }
-        for (int r = 0; r < 3; ++r) out[v * 3 + r] = s[r] / w.graph.scale + w.graph.center[r];
-    }
-    return out;
+    return nricp_b200::evaluate_host(*wraps_[i], rot, trans, level);
 }
 
 int Batch::finest_nodes(int i) const { return wraps_[i]->layouts.back().node_count; }
@@ -902,5 +919,493 @@ void Batch::current_vertices(int i, double* out) {
 }
 
 const WrapDev* Batch::device_wrap(int i) const { return dev_wraps_ + i; }
+
+
+// ---------------------------------------------------------------------------
+// Server: continuous batching
+// ---------------------------------------------------------------------------
+namespace {
+
+// A template's graph and level layouts, shared by every request that wraps
+// the same template with the same graph settings.
+struct TemplateEntry {
+    TemplateGraph graph;
+    std::vector<LevelLayout> layouts;
+    int levels = 0, max_nodes = 0, max_edges = 0, max_pairs = 0, max_offdiag = 0;
+};
+
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < bytes; ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return h;
+}
+
+uint64_t template_key(const Wrap& w) {
+    const NricpSolveDesc& d = w.desc;
+    const int settings[5] = {d.graph_levels, d.nodes_initial, d.growth, d.max_nodes_per_vertex,
+                             d.edge_neighbours};
+    uint64_t h = 14695981039346656037ull;
+    h = fnv1a(w.template_in.data(), sizeof(double) * w.template_in.size(), h);
+    h = fnv1a(w.template_faces.data(), sizeof(int32_t) * w.template_faces.size(), h);
+    return fnv1a(settings, sizeof settings, h);
+}
+
+double percentile(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const size_t k = static_cast<size_t>(std::ceil(q * v.size()));
+    return v[std::min(v.size() - 1, k > 0 ? k - 1 : 0)];
+}
+
+}  // namespace
+
+struct Server::Impl {
+    struct Request {
+        long id = 0;
+        std::unique_ptr<Wrap> wrap;
+        int state = NRICP_REQUEST_WAITING;
+        bool invalid = false;
+        std::string error;
+        double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;
+        size_t bytes = 0;
+        std::vector<double> vertices, rotations, translations, nodes;
+        std::vector<int32_t> level_nodes;
+        std::string report;
+    };
+    using RequestPtr = std::shared_ptr<Request>;
+
+    NricpServerConfig cfg{};
+    int device = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    WrapDev* dev_wraps = nullptr;
+    WrapControl* dev_controls = nullptr;
+    WrapControl* host_controls = nullptr;
+    std::vector<WrapDev> host_wraps;
+    std::vector<RequestPtr> slot_req;  // the request resident in each slot, running or finished
+    std::vector<int> slot_nodes;
+    int slots_used = 0;
+    size_t resident = 0, peak = 0;
+    void* lbvh_scratch = nullptr;
+    size_t lbvh_bytes = 0;
+    TickShape shape{};
+    bool shape_dirty = true;
+    cudaGraphExec_t graph = nullptr;
+
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::map<long, RequestPtr> requests;
+    std::deque<RequestPtr> prep_queue, ready;
+    long next_id = 1;
+    int running = 0;
+    bool stop = false;
+    std::vector<std::thread> preppers;
+    std::thread pump_thread;
+    std::mutex cache_mu;
+    std::map<uint64_t, std::shared_ptr<const TemplateEntry>> cache;
+
+    long submitted = 0, completed = 0, failed = 0, ticks = 0, launches = 0, captures = 0;
+    std::vector<double> latencies, queue_waits;
+    double first_submit = -1.0, last_done = 0.0;
+
+    void prepare_cached(Wrap& w) {
+        const uint64_t key = template_key(w);
+        std::shared_ptr<const TemplateEntry> entry;
+        {
+            std::lock_guard<std::mutex> lk(cache_mu);
+            auto it = cache.find(key);
+            if (it != cache.end()) entry = it->second;
+        }
+        if (!entry) {
+            prepare_host(w);
+            auto fresh = std::make_shared<TemplateEntry>();
+            fresh->graph = w.graph;
+            fresh->layouts = w.layouts;
+            fresh->levels = w.levels;
+            fresh->max_nodes = w.max_nodes;
+            fresh->max_edges = w.max_edges;
+            fresh->max_pairs = w.max_pairs;
+            fresh->max_offdiag = w.max_offdiag;
+            std::lock_guard<std::mutex> lk(cache_mu);
+            cache.emplace(key, std::move(fresh));
+            return;
+        }
+        w.graph = entry->graph;
+        w.layouts = entry->layouts;
+        w.levels = entry->levels;
+        w.max_nodes = entry->max_nodes;
+        w.max_edges = entry->max_edges;
+        w.max_pairs = entry->max_pairs;
+        w.max_offdiag = entry->max_offdiag;
+    }
+
+    void fail(const RequestPtr& r, const std::string& why, bool invalid) {
+        // caller holds `mu`
+        r->state = NRICP_REQUEST_FAILED;
+        r->error = why;
+        r->invalid = invalid;
+        failed += 1;
+        cv_done.notify_all();
+    }
+
+    void prep_loop() {
+        while (true) {
+            RequestPtr r;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stop || !prep_queue.empty(); });
+                if (stop) return;
+                r = prep_queue.front();
+                prep_queue.pop_front();
+            }
+            std::string why;
+            bool invalid = false;
+            try {
+                prepare_cached(*r->wrap);
+                r->bytes = prepare_device(*r->wrap, nullptr, nullptr, true);
+            } catch (const InvalidArgument& e) {
+                why = e.what();
+                invalid = true;
+            } catch (const std::exception& e) {
+                why = e.what();
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            if (why.empty()) {
+                ready.push_back(r);
+            } else {
+                fail(r, why, invalid);
+            }
+            cv_work.notify_all();
+        }
+    }
+
+    void grow_shape(const Wrap& w) {
+        const TickShape before = shape;
+        shape.max_vertices = std::max(shape.max_vertices, w.V);
+        shape.max_nodes = std::max(shape.max_nodes, w.max_nodes);
+        shape.max_edges = std::max(shape.max_edges, w.max_edges);
+        shape.max_pairs = std::max(shape.max_pairs, w.max_pairs);
+        shape.wraps = slots_used;
+        if (std::memcmp(&before, &shape, sizeof shape) != 0) shape_dirty = true;
+    }
+
+    void capture() {
+        shape.pcg_groups = 0;
+        const int cluster = cfg.pcg_cluster > 0 ? cfg.pcg_cluster
+                                                : pcg_cluster_size(shape.max_nodes, slots_used, sms);
+        pcg_cluster_size(shape.max_nodes, slots_used, sms);  // enables the launch attributes
+        shape.pcg_cluster = cluster;
+        shape.pcg_shared_bytes = pcg_shared_bytes(slot_nodes.data(), slots_used, cluster);
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        cudaGraph_t g = nullptr;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
+        launch_tick(dev_wraps, shape, stream, nullptr);
+        check(cudaStreamEndCapture(stream, &g), "capture end");
+        check(cudaGraphInstantiate(&graph, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        captures += 1;
+        shape_dirty = false;
+    }
+
+    // Brings an admitted request onto the device in `slot` (pump thread).
+    void place(int slot, const RequestPtr& r, RequestPtr old) {
+        if (old) old->wrap.reset();  // the slot's previous wrap; its results are already copied out
+        old.reset();
+        Wrap& w = *r->wrap;
+        prepare_device(w, dev_controls + slot, stream);
+        const size_t need = lbvh_scratch_bytes(w.F);
+        if (need > lbvh_bytes) {
+            check(cudaStreamSynchronize(stream), "scratch");
+            if (lbvh_scratch) cudaFree(lbvh_scratch);
+            lbvh_scratch = nullptr;
+            check(cudaMalloc(&lbvh_scratch, need), "cudaMalloc(lbvh scratch)");
+            lbvh_bytes = need;
+        }
+        reset_device(w, stream, lbvh_scratch, nullptr);
+        host_wraps[slot] = w.dev;
+        check(cudaMemcpyAsync(dev_wraps + slot, &host_wraps[slot], sizeof(WrapDev),
+                              cudaMemcpyHostToDevice, stream), "slot descriptor");
+        slot_nodes[slot] = w.max_nodes;
+        grow_shape(w);
+    }
+
+    void retire(int slot, const RequestPtr& r) {
+        Wrap& w = *r->wrap;
+        const WrapControl& c = host_controls[slot];
+        const int N = w.layouts.back().node_count;
+        r->vertices.assign(static_cast<size_t>(w.V) * 3, 0.0);
+        r->rotations.assign(static_cast<size_t>(N) * 9, 0.0);
+        r->translations.assign(static_cast<size_t>(N) * 3, 0.0);
+        r->nodes.assign(static_cast<size_t>(N) * 3, 0.0);
+        r->level_nodes.assign(w.levels, 0);
+        std::vector<char> report(1 << 20);
+        NricpResult out{r->vertices.data(), r->rotations.data(), r->translations.data(),
+                        r->nodes.data(), r->level_nodes.data(), report.data(), report.size(), 0};
+        w.solve_seconds = now_seconds() - r->t_admit;
+        write_result(w, c, stream, &out);
+        r->report.assign(report.data(), std::min(out.report_length, report.size() - 1));
+    }
+
+    void pump_loop() {
+        cudaSetDevice(device);
+        const int per_poll = cfg.ticks_per_poll > 0 ? cfg.ticks_per_poll : 8;
+        while (true) {
+            std::vector<std::pair<int, RequestPtr>> admits;
+            std::vector<RequestPtr> evicted;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stop || running > 0 || !ready.empty(); });
+                if (stop) return;
+                std::vector<bool> taken(cfg.max_slots, false);
+                while (!ready.empty()) {
+                    RequestPtr r = ready.front();
+                    if (r->bytes > cfg.memory_budget_bytes) {
+                        ready.pop_front();
+                        fail(r, "the wrap needs " + std::to_string(r->bytes) +
+                                    " device bytes, more than the server's budget of " +
+                                    std::to_string(cfg.memory_budget_bytes), false);
+                        continue;
+                    }
+                    int slot = -1;
+                    for (int i = 0; i < slots_used && slot < 0; ++i)
+                        if (!taken[i] && (!slot_req[i] || slot_req[i]->state != NRICP_REQUEST_RUNNING))
+                            slot = i;
+                    if (slot < 0 && slots_used < cfg.max_slots) slot = slots_used;
+                    if (slot < 0) break;
+                    const size_t freed = slot_req[slot] ? slot_req[slot]->bytes : 0;
+                    if (resident - freed + r->bytes > cfg.memory_budget_bytes) break;
+                    ready.pop_front();
+                    resident = resident - freed + r->bytes;
+                    peak = std::max(peak, resident);
+                    taken[slot] = true;
+                    r->state = NRICP_REQUEST_RUNNING;
+                    r->t_admit = now_seconds();
+                    queue_waits.push_back(r->t_admit - r->t_submit);
+                    running += 1;
+                    evicted.push_back(slot_req[slot]);
+                    slot_req[slot] = r;
+                    if (slot == slots_used) slots_used += 1;
+                    admits.emplace_back(slot, r);
+                }
+            }
+            for (size_t k = 0; k < admits.size(); ++k) {
+                try {
+                    place(admits[k].first, admits[k].second, std::move(evicted[k]));
+                } catch (const std::exception& e) {
+                    // keep the slot harmless: a finished control, no work
+                    WrapControl done{};
+                    done.phase = kPhaseDone;
+                    host_wraps[admits[k].first].control = dev_controls + admits[k].first;
+                    cudaMemcpyAsync(dev_controls + admits[k].first, &done, sizeof done,
+                                    cudaMemcpyHostToDevice, stream);
+                    cudaMemcpyAsync(dev_wraps + admits[k].first, &host_wraps[admits[k].first],
+                                    sizeof(WrapDev), cudaMemcpyHostToDevice, stream);
+                    cudaStreamSynchronize(stream);
+                    std::lock_guard<std::mutex> lk(mu);
+                    running -= 1;
+                    fail(admits[k].second, e.what(), false);
+                }
+            }
+            try {
+                if (shape_dirty) capture();
+                for (int i = 0; i < per_poll; ++i) check(cudaGraphLaunch(graph, stream), "graph launch");
+                check(cudaMemcpyAsync(host_controls, dev_controls, sizeof(WrapControl) * slots_used,
+                                      cudaMemcpyDeviceToHost, stream), "pull controls");
+                check(cudaStreamSynchronize(stream), "tick");
+            } catch (const std::exception& e) {
+                // the device failed under every running request
+                std::lock_guard<std::mutex> lk(mu);
+                for (int i = 0; i < slots_used; ++i)
+                    if (slot_req[i] && slot_req[i]->state == NRICP_REQUEST_RUNNING) {
+                        running -= 1;
+                        fail(slot_req[i], e.what(), false);
+                    }
+                stop = true;
+                cv_work.notify_all();
+                return;
+            }
+            ticks += per_poll;
+            launches += (long)per_poll * tick_kernel_launches(shape);
+            for (int i = 0; i < slots_used; ++i) {
+                RequestPtr r = slot_req[i];
+                if (!r || r->state != NRICP_REQUEST_RUNNING || host_controls[i].phase != kPhaseDone) continue;
+                std::string why;
+                if (host_controls[i].error) {
+                    why = "a closest-point traversal exceeded its stack; the hierarchy is too deep";
+                } else {
+                    try {
+                        retire(i, r);
+                    } catch (const std::exception& e) {
+                        why = e.what();
+                    }
+                }
+                std::lock_guard<std::mutex> lk(mu);
+                running -= 1;
+                if (!why.empty()) {
+                    fail(r, why, false);
+                    continue;
+                }
+                r->state = NRICP_REQUEST_DONE;
+                r->t_done = now_seconds();
+                latencies.push_back(r->t_done - r->t_submit);
+                last_done = std::max(last_done, r->t_done);
+                completed += 1;
+                cv_done.notify_all();
+            }
+        }
+    }
+};
+
+Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()) {
+    Impl& m = *impl_;
+    m.cfg = config;
+    if (m.cfg.max_slots <= 0 || m.cfg.max_slots > 1024)
+        throw InvalidArgument("max_slots is " + std::to_string(m.cfg.max_slots) + "; it must be 1 to 1024");
+    if (m.cfg.pcg_cluster != 0 && (m.cfg.pcg_cluster < 0 || m.cfg.pcg_cluster > 16 ||
+                                  (m.cfg.pcg_cluster & (m.cfg.pcg_cluster - 1)) != 0))
+        throw InvalidArgument("the solve's cluster size is a power of two from 1 to 16");
+    check(cudaGetDevice(&m.device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&m.sms, cudaDevAttrMultiProcessorCount, m.device), "device");
+    if (m.cfg.memory_budget_bytes == 0) {
+        size_t free_bytes = 0, total = 0;
+        check(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
+        m.cfg.memory_budget_bytes = free_bytes / 10 * 9;
+    }
+    check(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaMalloc(&m.dev_wraps, sizeof(WrapDev) * m.cfg.max_slots), "cudaMalloc(slots)");
+    check(cudaMalloc(&m.dev_controls, sizeof(WrapControl) * m.cfg.max_slots), "cudaMalloc(controls)");
+    check(cudaMallocHost(&m.host_controls, sizeof(WrapControl) * m.cfg.max_slots), "cudaMallocHost(controls)");
+    m.host_wraps.assign(m.cfg.max_slots, WrapDev{});
+    m.slot_req.assign(m.cfg.max_slots, nullptr);
+    m.slot_nodes.assign(m.cfg.max_slots, 0);
+    int threads = m.cfg.prep_threads;
+    if (threads <= 0) threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / 2);
+    for (int i = 0; i < threads; ++i) m.preppers.emplace_back([&m] { m.prep_loop(); });
+    m.pump_thread = std::thread([&m] { m.pump_loop(); });
+}
+
+Server::~Server() {
+    Impl& m = *impl_;
+    {
+        std::lock_guard<std::mutex> lk(m.mu);
+        m.stop = true;
+    }
+    m.cv_work.notify_all();
+    m.cv_done.notify_all();
+    for (auto& t : m.preppers) t.join();
+    if (m.pump_thread.joinable()) m.pump_thread.join();
+    cudaSetDevice(m.device);
+    cudaStreamSynchronize(m.stream);
+    if (m.graph) cudaGraphExecDestroy(m.graph);
+    m.slot_req.clear();
+    m.requests.clear();
+    m.ready.clear();
+    m.prep_queue.clear();
+    if (m.lbvh_scratch) cudaFree(m.lbvh_scratch);
+    if (m.dev_wraps) cudaFree(m.dev_wraps);
+    if (m.dev_controls) cudaFree(m.dev_controls);
+    if (m.host_controls) cudaFreeHost(m.host_controls);
+    cudaStreamDestroy(m.stream);
+}
+
+long Server::submit(const NricpSolveDesc& desc) {
+    Impl& m = *impl_;
+    validate_settings(desc);
+    auto r = std::make_shared<Impl::Request>();
+    r->wrap = std::make_unique<Wrap>();
+    copy_inputs(*r->wrap, desc);
+    std::lock_guard<std::mutex> lk(m.mu);
+    if (m.stop) throw StateError("the server has stopped");
+    r->id = m.next_id++;
+    r->t_submit = now_seconds();
+    if (m.first_submit < 0.0) m.first_submit = r->t_submit;
+    m.requests[r->id] = r;
+    m.prep_queue.push_back(r);
+    m.submitted += 1;
+    m.cv_work.notify_all();
+    return r->id;
+}
+
+int Server::poll(long id, double* latency_seconds) {
+    Impl& m = *impl_;
+    std::lock_guard<std::mutex> lk(m.mu);
+    auto it = m.requests.find(id);
+    if (it == m.requests.end()) throw InvalidArgument("unknown request " + std::to_string(id));
+    const auto& r = it->second;
+    if (latency_seconds)
+        *latency_seconds = r->state == NRICP_REQUEST_DONE ? r->t_done - r->t_submit : 0.0;
+    return r->state;
+}
+
+bool Server::wait(long id, double timeout_seconds) {
+    Impl& m = *impl_;
+    std::unique_lock<std::mutex> lk(m.mu);
+    auto it = m.requests.find(id);
+    if (it == m.requests.end()) throw InvalidArgument("unknown request " + std::to_string(id));
+    const auto r = it->second;
+    auto finished = [&] {
+        return r->state == NRICP_REQUEST_DONE || r->state == NRICP_REQUEST_FAILED || m.stop;
+    };
+    if (timeout_seconds <= 0.0) {
+        m.cv_done.wait(lk, finished);
+        return true;
+    }
+    return m.cv_done.wait_for(lk, std::chrono::duration<double>(timeout_seconds), finished);
+}
+
+void Server::result(long id, NricpResult* out) {
+    Impl& m = *impl_;
+    std::lock_guard<std::mutex> lk(m.mu);
+    auto it = m.requests.find(id);
+    if (it == m.requests.end()) throw InvalidArgument("unknown request " + std::to_string(id));
+    const auto r = it->second;
+    if (r->state == NRICP_REQUEST_FAILED) {
+        m.requests.erase(it);
+        if (r->invalid) throw InvalidArgument(r->error);
+        throw StateError(r->error);
+    }
+    if (r->state != NRICP_REQUEST_DONE) throw StateError("request " + std::to_string(id) + " is not done");
+    if (out->vertices) std::memcpy(out->vertices, r->vertices.data(), sizeof(double) * r->vertices.size());
+    if (out->rotations) std::memcpy(out->rotations, r->rotations.data(), sizeof(double) * r->rotations.size());
+    if (out->translations)
+        std::memcpy(out->translations, r->translations.data(), sizeof(double) * r->translations.size());
+    if (out->node_positions) std::memcpy(out->node_positions, r->nodes.data(), sizeof(double) * r->nodes.size());
+    if (out->level_nodes)
+        std::memcpy(out->level_nodes, r->level_nodes.data(), sizeof(int32_t) * r->level_nodes.size());
+    out->report_length = r->report.size();
+    if (out->report_json && out->report_capacity > 0) {
+        const size_t n = std::min(r->report.size(), out->report_capacity - 1);
+        std::memcpy(out->report_json, r->report.data(), n);
+        out->report_json[n] = 0;
+    }
+    g_transfers.d2h += sizeof(double) * (r->vertices.size() + r->rotations.size() + r->translations.size());
+    m.requests.erase(it);
+}
+
+NricpServerStats Server::stats() {
+    Impl& m = *impl_;
+    std::lock_guard<std::mutex> lk(m.mu);
+    NricpServerStats s{};
+    s.submitted = m.submitted;
+    s.completed = m.completed;
+    s.failed = m.failed;
+    s.running = m.running;
+    s.waiting = static_cast<long>(m.prep_queue.size() + m.ready.size());
+    s.latency_p50_ms = 1000.0 * percentile(m.latencies, 0.50);
+    s.latency_p99_ms = 1000.0 * percentile(m.latencies, 0.99);
+    double sum = 0.0;
+    for (double x : m.latencies) sum += x;
+    s.latency_mean_ms = m.latencies.empty() ? 0.0 : 1000.0 * sum / m.latencies.size();
+    s.queue_p50_ms = 1000.0 * percentile(m.queue_waits, 0.50);
+    const double span = m.last_done - m.first_submit;
+    s.wraps_per_second = span > 0.0 ? m.completed / span : 0.0;
+    s.ticks = m.ticks;
+    s.launches = m.launches;
+    s.captures = m.captures;
+    s.resident_bytes = m.resident;
+    s.peak_resident_bytes = m.peak;
+    s.slots_used = m.slots_used;
+    return s;
+}
 
 }  // namespace nricp_b200

@@ -17,6 +17,9 @@ namespace nricp_b200 {
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+struct TimeoutError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 struct CapacityError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
@@ -113,5 +116,26 @@ struct TransferCounters {
     unsigned long long h2d = 0, d2h = 0;
 };
 extern thread_local TransferCounters g_transfers;
+
+// Continuous batching on one device: resident wrap slots advanced by the
+// same launches; requests prepared on host threads, admitted by memory
+// budget as slots free up, retired when done (see nricp_server_* ).
+class Server {
+public:
+    explicit Server(const NricpServerConfig& config);
+    ~Server();
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+    long submit(const NricpSolveDesc& desc);
+    int poll(long id, double* latency_seconds);
+    bool wait(long id, double timeout_seconds);
+    void result(long id, NricpResult* out);
+    NricpServerStats stats();
+
+    struct Impl;
+
+private:
+    std::unique_ptr<Impl> impl_;
+};
 
 }  // namespace nricp_b200

@@ -156,6 +156,75 @@ class WrapBatch:
         return dict(zip(keys, list(sizes)))
 
 
+class WrapServer:
+    """Continuous batching on one device (no reference counterpart: the
+    reference solves one wrap per call).  ``submit`` copies and validates a
+    request and returns at once; the request's graph is built on a host
+    thread (cached per template), it is admitted into a free resident slot
+    as soon as the device-memory budget allows, advanced together with
+    every other running wrap, and its result is kept until ``result`` takes
+    it.  Each result is bit-identical to the same wrap solved alone."""
+
+    def __init__(self, memory_budget_bytes: int = 0, max_slots: int = 64,
+                 prep_threads: int = 0, pcg_cluster: int = 0, ticks_per_poll: int = 8):
+        cfg = _abi.ServerConfig()
+        load().nricp_server_default_config(C.byref(cfg))
+        cfg.memory_budget_bytes = int(memory_budget_bytes)
+        cfg.max_slots = int(max_slots)
+        cfg.prep_threads = int(prep_threads)
+        cfg.pcg_cluster = int(pcg_cluster)
+        cfg.ticks_per_poll = int(ticks_per_poll)
+        self._handle = C.c_void_p()
+        check(load().nricp_server_create(C.byref(cfg), C.byref(self._handle)))
+        self._plans: dict[int, tuple[int, list[int]]] = {}
+
+    def close(self) -> None:
+        handle = getattr(self, "_handle", None)
+        if handle:
+            load().nricp_server_destroy(handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, template_points, template_faces, target_points, target_faces,
+               level_settings, route: str = "route_b", **kwargs) -> int:
+        if route not in _ROUTES:
+            raise ValueError(f"the device session runs 'route_b' or 'route_c', not '{route}'")
+        desc = _abi.Desc(template_points, template_faces, target_points, target_faces,
+                         level_settings, route=_ROUTES[route], **kwargs)
+        rid = C.c_long()
+        check(load().nricp_server_submit(self._handle, C.byref(desc.struct), C.byref(rid)))
+        self._plans[rid.value] = (desc.template_points.shape[0], _plan(desc))
+        return rid.value
+
+    def poll(self, request: int) -> tuple[str, float]:
+        """('waiting' | 'running' | 'done' | 'failed', latency in seconds once done)."""
+        status, latency = C.c_int(), C.c_double()
+        check(load().nricp_server_poll(self._handle, request, C.byref(status), C.byref(latency)))
+        return _abi.REQUEST_STATES[status.value], latency.value
+
+    def result(self, request: int, timeout: float | None = None) -> dict:
+        """Waits for the request and returns its result dict (as solve_route_b)."""
+        check(load().nricp_server_wait(self._handle, request, float(timeout or 0.0)))
+        vertices, levels = self._plans[request]
+        out = _abi.ResultBuffers(vertices, levels)
+        check(load().nricp_server_result(self._handle, request, C.byref(out.struct)))
+        del self._plans[request]
+        return out.to_dict()
+
+    def stats(self) -> dict:
+        s = _abi.ServerStats()
+        check(load().nricp_server_stats(self._handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+
 def transfer_counters(reset: bool = False) -> tuple[int, int]:
     """Bytes copied host->device and device->host by this thread's calls."""
     h2d, d2h = C.c_ulonglong(), C.c_ulonglong()

@@ -50,6 +50,8 @@ STRUCTS = {
     "NricpProgress": _abi.Progress,
     "NricpTickRecord": _abi.TickRecord,
     "NricpInspect": _abi.Inspect,
+    "NricpServerConfig": _abi.ServerConfig,
+    "NricpServerStats": _abi.ServerStats,
 }
 
 
