@@ -27,6 +27,9 @@ Printed (one JSON line on rank 0):
                    against the reference's FP64 route A on a sample,
 * ``cpu_baseline`` the reference's own route A (compiled from its sources,
                    oracle/_ref) on the host cores, on a bounded sample,
+* ``served``       the same wraps as requests arriving in Poisson windows
+                   (20 and 80 per second by default) served with continuous
+                   batching: throughput and p50/p99 latency per window,
 * ``single_wrap``  the large single wrap of config 2 (25k vertices onto a
                    393k-triangle target, 2,000 nodes) one at a time.
 
@@ -69,6 +72,11 @@ def parse_args():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-profile", action="store_true")
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-rates", default="20,80",
+                   help="Poisson arrival rates (requests/s) of the serving windows")
+    p.add_argument("--serve-seconds", type=float, default=6.0,
+                   help="length of each serving window (the full protocol: 60)")
     return p.parse_args()
 
 
@@ -311,6 +319,51 @@ def flush_l2():
     del buf
 
 
+def serve_window(server, cases, rate: float, seconds: float, rng) -> dict:
+    """Requests drawn from `cases` arriving as a Poisson process at `rate`
+    per second for `seconds`; latency is submit to result ready."""
+    submitted = []
+    t0 = time.perf_counter()
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        delay = t0 + t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        c = cases[int(rng.integers(len(cases)))]
+        submitted.append((time.perf_counter(), server.submit(*c.args(), **c.options)))
+    latencies, finished = [], []
+    for ts, rid in submitted:
+        state, latency = server.wait(rid, timeout=900.0)
+        if state != "done":
+            raise RuntimeError(f"served request {rid} ended {state}")
+        server.result(rid)
+        latencies.append(1000.0 * latency)
+        finished.append(ts + latency)
+    span = max(finished) - submitted[0][0] if submitted else 0.0
+    out = {"rate_per_s": rate, "seconds": seconds, "requests": len(submitted),
+           "wraps_per_second": len(submitted) / span if span > 0 else 0.0}
+    out.update({f"latency_{k}_ms": v for k, v in percentiles(latencies).items() if k != "n"})
+    return out
+
+
+def run_serving(dp, cases, rates, seconds, seed) -> dict:
+    budget = 120 * 10**9
+    with dp.WrapServer(memory_budget_bytes=budget, max_slots=64) as server:
+        # warm: every template's graph cached, the launch shape captured
+        for rid in [server.submit(*c.args(), **c.options) for c in cases]:
+            server.result(rid, timeout=900.0)
+        rng = np.random.default_rng(seed)
+        windows = [serve_window(server, cases, r, seconds, rng) for r in rates]
+        stats = server.stats()
+    return {"workload": "Poisson arrivals drawn from the 64 config-3 wraps, continuous batching, "
+                        "64 resident slots, 120 GB admission budget",
+            "windows": windows, "graph_captures": stats["captures"],
+            "peak_resident_gb": stats["peak_resident_bytes"] / 1e9}
+
+
 def percentiles(values) -> dict:
     v = sorted(values)
     if not v:
@@ -409,6 +462,14 @@ def run_ours(args, ranks):
                "max_final_energy_rel_error": max(energy_errors),
                "wraps_within_1e-4": sum(1 for e in errors if e <= 1e-4)}
 
+    # ---- serving: continuous batching under Poisson arrivals ----
+    served = None
+    if ranks.rank == 0 and not args.no_serve:
+        rates = [float(x) for x in args.serve_rates.split(",") if x]
+        served = run_serving(dp, cases, rates, args.serve_seconds, args.seed)
+        served["vs_plain"] = {f"{w['rate_per_s']:g}/s": w["wraps_per_second"] / plain
+                              for w in served["windows"]}
+
     # ---- the large single wrap (config 2), one at a time ----
     single = None
     if ranks.rank == 0:
@@ -447,6 +508,7 @@ def run_ours(args, ranks):
         "e2e": e2e,
         "roofline": roof,
         "kernels": detail,
+        "served": served,
         "fit": fit,
         "cpu_baseline": cpu,
         "single_wrap": single,

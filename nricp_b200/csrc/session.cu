@@ -55,6 +55,16 @@ public:
         if (size_ == 0) size_ = 256;
         check(cudaMalloc(&base_, size_), "cudaMalloc(wrap arena)");
     }
+    // Stream-ordered, from `pool`: neither this nor release_async waits for
+    // the device.
+    void allocate(cudaMemPool_t pool, cudaStream_t stream) {
+        if (size_ == 0) size_ = 256;
+        check(cudaMallocFromPoolAsync(&base_, size_, pool, stream), "cudaMallocFromPoolAsync(wrap arena)");
+    }
+    void release_async(cudaStream_t stream) {
+        if (base_) check(cudaFreeAsync(base_, stream), "cudaFreeAsync(wrap arena)");
+        base_ = nullptr;
+    }
     template <typename T>
     T* at(size_t offset) const { return reinterpret_cast<T*>(static_cast<char*>(base_) + offset); }
     size_t size() const { return size_; }
@@ -112,12 +122,9 @@ struct Wrap {
     WrapDev dev{};        // host copy of the descriptor
     WrapControl* control = nullptr;  // device
     WrapControl initial_control{};   // pinned-free host copy used by reset
-    double* identity_rot = nullptr;  // device: identity rotations + initial records
-    LevelRecord* initial_records = nullptr;
-    ~Wrap() {
-        arena.release();
-        if (identity_rot) cudaFree(identity_rot);
-    }
+    double* identity_rot = nullptr;  // device (in the arena): identity rotations
+    LevelRecord* initial_records = nullptr;  // and the level records a run starts from
+    ~Wrap() { arena.release(); }
 };
 
 namespace {
@@ -198,7 +205,8 @@ size_t bytes_of_layout(const LevelLayout& L) {
 
 // Lays out, allocates and fills the wrap's device arena; builds the target's
 // hierarchy.  `control` is this wrap's slot in the batch's control array.
-size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool plan_only = false) {
+size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool plan_only = false,
+                      cudaMemPool_t pool = nullptr) {
     const NricpSolveDesc& d = w.desc;
     const int V = w.V, N = std::max(1, w.max_nodes), B = std::max(1, w.max_offdiag);
     Arena& a = w.arena;
@@ -258,12 +266,33 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_records = a.reserve(sizeof(LevelRecord) * w.levels);
     const size_t o_lstats = a.reserve(sizeof(CorrStats) * w.levels);
     const size_t o_fstats = a.reserve(sizeof(CorrStats));
+    const size_t o_identity = a.reserve(sizeof(double) * 9 * N);
+    const size_t o_init_records = a.reserve(sizeof(LevelRecord) * w.levels);
     if (plan_only) {  // the arena's size only, nothing allocated
-        const size_t bytes = a.size() + sizeof(double) * 9 * N + sizeof(LevelRecord) * w.levels;
+        const size_t bytes = a.size();
         a = Arena();
         return bytes;
     }
-    a.allocate();
+    if (pool) {
+        a.allocate(pool, stream);
+    } else {
+        a.allocate();
+    }
+    {
+        // the state every run starts from: identity rotations, empty records
+        std::vector<double> rot(static_cast<size_t>(N) * 9, 0.0);
+        for (int n = 0; n < N; ++n) rot[n * 9] = rot[n * 9 + 4] = rot[n * 9 + 8] = 1.0;
+        std::vector<LevelRecord> records(w.levels);
+        std::memset(records.data(), 0, sizeof(LevelRecord) * records.size());
+        for (int l = 0; l < w.levels; ++l) {
+            records[l].level = l;
+            records[l].nodes = w.layouts[l].node_count;
+        }
+        w.identity_rot = a.at<double>(o_identity);
+        w.initial_records = a.at<LevelRecord>(o_init_records);
+        upload(w.identity_rot, rot, stream);
+        upload(w.initial_records, records, stream);
+    }
 
     // ---- fill the descriptor ----
     WrapDev& D = w.dev;
@@ -414,23 +443,6 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
 void reset_device(Wrap& w, cudaStream_t stream, void* lbvh_scratch, LbvhExport* lbvh_out) {
     WrapDev& D = w.dev;
     const int V = w.V, N = std::max(1, w.max_nodes);
-    if (w.identity_rot == nullptr) {
-        std::vector<double> rot(static_cast<size_t>(N) * 9, 0.0);
-        for (int n = 0; n < N; ++n) rot[n * 9] = rot[n * 9 + 4] = rot[n * 9 + 8] = 1.0;
-        std::vector<LevelRecord> records(w.levels);
-        std::memset(records.data(), 0, sizeof(LevelRecord) * records.size());
-        for (int l = 0; l < w.levels; ++l) {
-            records[l].level = l;
-            records[l].nodes = w.layouts[l].node_count;
-        }
-        check(cudaMalloc(&w.identity_rot, sizeof(double) * rot.size() + sizeof(LevelRecord) * records.size()),
-              "cudaMalloc(initial state)");
-        check(cudaMemcpy(w.identity_rot, rot.data(), sizeof(double) * rot.size(), cudaMemcpyHostToDevice),
-              "initial state");
-        w.initial_records = reinterpret_cast<LevelRecord*>(w.identity_rot + rot.size());
-        check(cudaMemcpy(w.initial_records, records.data(), sizeof(LevelRecord) * records.size(),
-                         cudaMemcpyHostToDevice), "initial records");
-    }
     check(cudaMemcpyAsync(D.rot[0], w.identity_rot, sizeof(double) * 9 * N, cudaMemcpyDeviceToDevice, stream),
           "init rot");
     check(cudaMemsetAsync(D.trans[0], 0, sizeof(double) * 3 * N, stream), "init trans");
@@ -968,38 +980,49 @@ struct Server::Impl {
         std::string error;
         double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;
         size_t bytes = 0;
+        cudaEvent_t loaded = nullptr;  // the wrap's uploads and hierarchy are on the device
         std::vector<double> vertices, rotations, translations, nodes;
         std::vector<int32_t> level_nodes;
         std::string report;
     };
     using RequestPtr = std::shared_ptr<Request>;
+    // A retired wrap whose arena is freed once `after` (recorded on the tick
+    // stream after its last use) has passed.
+    struct Dead {
+        std::unique_ptr<Wrap> wrap;
+        size_t bytes = 0;
+        cudaEvent_t after = nullptr;
+    };
 
     NricpServerConfig cfg{};
     int device = 0, sms = 148;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;       // ticks, placement, results
+    cudaStream_t load_stream = nullptr;  // allocation, uploads, hierarchy builds, frees
+    cudaMemPool_t pool = nullptr;
     WrapDev* dev_wraps = nullptr;
     WrapControl* dev_controls = nullptr;
     WrapControl* host_controls = nullptr;
+    WrapControl* staging_control = nullptr;  // where a loading wrap's reset writes its control
     std::vector<WrapDev> host_wraps;
-    std::vector<RequestPtr> slot_req;  // the request resident in each slot, running or finished
+    std::vector<RequestPtr> slot_req;    // the running request of each slot, or null
     std::vector<int> slot_nodes;
     int slots_used = 0;
     size_t resident = 0, peak = 0;
-    void* lbvh_scratch = nullptr;
+    void* lbvh_scratch = nullptr;        // on load_stream, from the pool
     size_t lbvh_bytes = 0;
-    TickShape shape{};
-    bool shape_dirty = true;
-    cudaGraphExec_t graph = nullptr;
+    TickShape shape{};                   // size envelope of every wrap placed so far
+    std::map<int, cudaGraphExec_t> graphs;  // one tick graph per running-wrap count
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::map<long, RequestPtr> requests;
-    std::deque<RequestPtr> prep_queue, ready;
+    std::deque<RequestPtr> prep_queue, ready, loaded;
+    std::deque<Dead> graveyard;
     long next_id = 1;
-    int running = 0;
+    int running = 0, loading = 0;
     bool stop = false;
     std::vector<std::thread> preppers;
-    std::thread pump_thread;
+    std::thread pump_thread, loader_thread;
     std::mutex cache_mu;
     std::map<uint64_t, std::shared_ptr<const TemplateEntry>> cache;
 
@@ -1047,6 +1070,7 @@ struct Server::Impl {
         cv_done.notify_all();
     }
 
+    // Host threads: graph and layouts (cached per template), arena size.
     void prep_loop() {
         while (true) {
             RequestPtr r;
@@ -1078,55 +1102,141 @@ struct Server::Impl {
         }
     }
 
+    bool can_load() const {
+        // caller holds `mu`; never more wraps on the device than slots
+        return !ready.empty() && running + loading + static_cast<int>(loaded.size()) < cfg.max_slots;
+    }
+
+    // One thread, its own stream: arenas from the pool, uploads, the target's
+    // hierarchy and the start state, in budget order; and the frees of
+    // retired arenas.  Nothing here waits for the tick stream.
+    void loader_loop() {
+        cudaSetDevice(device);
+        while (true) {
+            RequestPtr r;
+            std::deque<Dead> dead;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] {
+                    return stop || !graveyard.empty() ||
+                           (can_load() && resident + ready.front()->bytes <= cfg.memory_budget_bytes) ||
+                           (!ready.empty() && ready.front()->bytes > cfg.memory_budget_bytes);
+                });
+                if (stop) return;
+                dead.swap(graveyard);
+                while (!ready.empty() && ready.front()->bytes > cfg.memory_budget_bytes) {
+                    RequestPtr big = ready.front();
+                    ready.pop_front();
+                    fail(big, "the wrap needs " + std::to_string(big->bytes) +
+                                  " device bytes, more than the server's budget of " +
+                                  std::to_string(cfg.memory_budget_bytes), false);
+                }
+                if (can_load() && resident + ready.front()->bytes <= cfg.memory_budget_bytes) {
+                    r = ready.front();
+                    ready.pop_front();
+                    resident += r->bytes;
+                    peak = std::max(peak, resident);
+                    loading += 1;
+                }
+            }
+            size_t freed = 0;
+            for (Dead& d : dead) {
+                cudaStreamWaitEvent(load_stream, d.after, 0);
+                d.wrap->arena.release_async(load_stream);
+                cudaEventDestroy(d.after);
+                freed += d.bytes;
+            }
+            if (freed) {
+                std::lock_guard<std::mutex> lk(mu);
+                resident -= freed;
+                cv_work.notify_all();
+            }
+            if (!r) continue;
+            std::string why;
+            try {
+                Wrap& w = *r->wrap;
+                prepare_device(w, staging_control, load_stream, false, pool);
+                const size_t need = lbvh_scratch_bytes(w.F);
+                if (need > lbvh_bytes) {
+                    if (lbvh_scratch) check(cudaFreeAsync(lbvh_scratch, load_stream), "scratch");
+                    lbvh_scratch = nullptr;
+                    check(cudaMallocFromPoolAsync(&lbvh_scratch, need, pool, load_stream), "scratch");
+                    lbvh_bytes = need;
+                }
+                reset_device(w, load_stream, lbvh_scratch, nullptr);
+                check(cudaEventCreateWithFlags(&r->loaded, cudaEventDisableTiming), "event");
+                check(cudaEventRecord(r->loaded, load_stream), "event");
+            } catch (const std::exception& e) {
+                why = e.what();
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            loading -= 1;
+            if (why.empty()) {
+                loaded.push_back(r);
+            } else {
+                resident -= r->bytes;
+                if (r->wrap) r->wrap.reset();
+                fail(r, why, false);
+            }
+            cv_work.notify_all();
+        }
+    }
+
     void grow_shape(const Wrap& w) {
         const TickShape before = shape;
         shape.max_vertices = std::max(shape.max_vertices, w.V);
         shape.max_nodes = std::max(shape.max_nodes, w.max_nodes);
         shape.max_edges = std::max(shape.max_edges, w.max_edges);
         shape.max_pairs = std::max(shape.max_pairs, w.max_pairs);
-        shape.wraps = slots_used;
-        if (std::memcmp(&before, &shape, sizeof shape) != 0) shape_dirty = true;
+        if (std::memcmp(&before, &shape, sizeof shape) != 0) {
+            for (auto& [count, g] : graphs) cudaGraphExecDestroy(g);
+            graphs.clear();
+        }
     }
 
-    void capture() {
-        shape.pcg_groups = 0;
+    // The tick over the first `count` slots (the running wraps are kept in
+    // slots 0 .. count-1), captured once per count and size envelope.
+    cudaGraphExec_t graph_for(int count) {
+        auto it = graphs.find(count);
+        if (it != graphs.end()) return it->second;
+        TickShape t = shape;
+        t.wraps = count;
+        t.pcg_groups = 0;
         const int cluster = cfg.pcg_cluster > 0 ? cfg.pcg_cluster
-                                                : pcg_cluster_size(shape.max_nodes, slots_used, sms);
-        pcg_cluster_size(shape.max_nodes, slots_used, sms);  // enables the launch attributes
-        shape.pcg_cluster = cluster;
-        shape.pcg_shared_bytes = pcg_shared_bytes(slot_nodes.data(), slots_used, cluster);
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
+                                                : pcg_cluster_size(t.max_nodes, count, sms);
+        pcg_cluster_size(t.max_nodes, count, sms);  // enables the launch attributes
+        t.pcg_cluster = cluster;
+        std::vector<int> nodes(count, t.max_nodes);  // any wrap may take any slot
+        t.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), count, cluster);
         cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
-        launch_tick(dev_wraps, shape, stream, nullptr);
+        launch_tick(dev_wraps, t, stream, nullptr);
         check(cudaStreamEndCapture(stream, &g), "capture end");
-        check(cudaGraphInstantiate(&graph, g, 0), "graph instantiate");
+        check(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
         cudaGraphDestroy(g);
         captures += 1;
-        shape_dirty = false;
+        launches_per_tick[count] = tick_kernel_launches(t);
+        graphs[count] = exec;
+        return exec;
     }
+    std::map<int, int> launches_per_tick;
 
-    // Brings an admitted request onto the device in `slot` (pump thread).
-    void place(int slot, const RequestPtr& r, RequestPtr old) {
-        if (old) old->wrap.reset();  // the slot's previous wrap; its results are already copied out
-        old.reset();
+    // Moves the running wrap of slot `from` into the free slot `to`: its
+    // control block (device to device) and its descriptor.
+    void move_slot(int from, int to) {
+        RequestPtr r = slot_req[from];
         Wrap& w = *r->wrap;
-        prepare_device(w, dev_controls + slot, stream);
-        const size_t need = lbvh_scratch_bytes(w.F);
-        if (need > lbvh_bytes) {
-            check(cudaStreamSynchronize(stream), "scratch");
-            if (lbvh_scratch) cudaFree(lbvh_scratch);
-            lbvh_scratch = nullptr;
-            check(cudaMalloc(&lbvh_scratch, need), "cudaMalloc(lbvh scratch)");
-            lbvh_bytes = need;
-        }
-        reset_device(w, stream, lbvh_scratch, nullptr);
-        host_wraps[slot] = w.dev;
-        check(cudaMemcpyAsync(dev_wraps + slot, &host_wraps[slot], sizeof(WrapDev),
-                              cudaMemcpyHostToDevice, stream), "slot descriptor");
-        slot_nodes[slot] = w.max_nodes;
-        grow_shape(w);
+        check(cudaMemcpyAsync(dev_controls + to, dev_controls + from, sizeof(WrapControl),
+                              cudaMemcpyDeviceToDevice, stream), "move control");
+        w.control = dev_controls + to;
+        w.dev.control = w.control;
+        host_wraps[to] = w.dev;
+        check(cudaMemcpyAsync(dev_wraps + to, &host_wraps[to], sizeof(WrapDev), cudaMemcpyHostToDevice,
+                              stream), "move descriptor");
+        host_controls[to] = host_controls[from];
+        slot_req[to] = r;
+        slot_req[from] = nullptr;
     }
 
     void retire(int slot, const RequestPtr& r) {
@@ -1146,89 +1256,89 @@ struct Server::Impl {
         r->report.assign(report.data(), std::min(out.report_length, report.size() - 1));
     }
 
+    // Hands a retired wrap's arena to the loader.  A finished wrap's tick
+    // kernels read only its control block (its slot's entry in dev_controls,
+    // which stays), so the arena can go as soon as the tick stream passes
+    // this point.
+    void bury(const RequestPtr& r) {
+        Dead d;
+        d.bytes = r->bytes;
+        d.wrap = std::move(r->wrap);
+        check(cudaEventCreateWithFlags(&d.after, cudaEventDisableTiming), "event");
+        check(cudaEventRecord(d.after, stream), "event");
+        std::lock_guard<std::mutex> lk(mu);
+        graveyard.push_back(std::move(d));
+        cv_work.notify_all();
+    }
+
+    // The tick thread: places loaded wraps into free slots, launches ticks,
+    // retires finished wraps.
     void pump_loop() {
         cudaSetDevice(device);
         const int per_poll = cfg.ticks_per_poll > 0 ? cfg.ticks_per_poll : 8;
         while (true) {
-            std::vector<std::pair<int, RequestPtr>> admits;
-            std::vector<RequestPtr> evicted;
+            std::vector<std::pair<int, RequestPtr>> placing;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stop || running > 0 || !ready.empty(); });
+                cv_work.wait(lk, [&] { return stop || running > 0 || !loaded.empty(); });
                 if (stop) return;
-                std::vector<bool> taken(cfg.max_slots, false);
-                while (!ready.empty()) {
-                    RequestPtr r = ready.front();
-                    if (r->bytes > cfg.memory_budget_bytes) {
-                        ready.pop_front();
-                        fail(r, "the wrap needs " + std::to_string(r->bytes) +
-                                    " device bytes, more than the server's budget of " +
-                                    std::to_string(cfg.memory_budget_bytes), false);
-                        continue;
-                    }
-                    int slot = -1;
-                    for (int i = 0; i < slots_used && slot < 0; ++i)
-                        if (!taken[i] && (!slot_req[i] || slot_req[i]->state != NRICP_REQUEST_RUNNING))
-                            slot = i;
-                    if (slot < 0 && slots_used < cfg.max_slots) slot = slots_used;
-                    if (slot < 0) break;
-                    const size_t freed = slot_req[slot] ? slot_req[slot]->bytes : 0;
-                    if (resident - freed + r->bytes > cfg.memory_budget_bytes) break;
-                    ready.pop_front();
-                    resident = resident - freed + r->bytes;
-                    peak = std::max(peak, resident);
-                    taken[slot] = true;
+                while (!loaded.empty() && running < cfg.max_slots) {
+                    RequestPtr r = loaded.front();
+                    if (running > 0 && cudaEventQuery(r->loaded) == cudaErrorNotReady) break;
+                    const int slot = running;  // running wraps stay in slots 0 .. running-1
+                    loaded.pop_front();
+                    slot_req[slot] = r;
+                    slots_used = std::max(slots_used, slot + 1);
                     r->state = NRICP_REQUEST_RUNNING;
                     r->t_admit = now_seconds();
                     queue_waits.push_back(r->t_admit - r->t_submit);
                     running += 1;
-                    evicted.push_back(slot_req[slot]);
-                    slot_req[slot] = r;
-                    if (slot == slots_used) slots_used += 1;
-                    admits.emplace_back(slot, r);
+                    placing.emplace_back(slot, r);
                 }
             }
-            for (size_t k = 0; k < admits.size(); ++k) {
-                try {
-                    place(admits[k].first, admits[k].second, std::move(evicted[k]));
-                } catch (const std::exception& e) {
-                    // keep the slot harmless: a finished control, no work
-                    WrapControl done{};
-                    done.phase = kPhaseDone;
-                    host_wraps[admits[k].first].control = dev_controls + admits[k].first;
-                    cudaMemcpyAsync(dev_controls + admits[k].first, &done, sizeof done,
-                                    cudaMemcpyHostToDevice, stream);
-                    cudaMemcpyAsync(dev_wraps + admits[k].first, &host_wraps[admits[k].first],
-                                    sizeof(WrapDev), cudaMemcpyHostToDevice, stream);
-                    cudaStreamSynchronize(stream);
-                    std::lock_guard<std::mutex> lk(mu);
-                    running -= 1;
-                    fail(admits[k].second, e.what(), false);
-                }
-            }
+            int count = 0;
             try {
-                if (shape_dirty) capture();
-                for (int i = 0; i < per_poll; ++i) check(cudaGraphLaunch(graph, stream), "graph launch");
-                check(cudaMemcpyAsync(host_controls, dev_controls, sizeof(WrapControl) * slots_used,
+                for (auto& [slot, r] : placing) {
+                    Wrap& w = *r->wrap;
+                    check(cudaStreamWaitEvent(stream, r->loaded, 0), "wait loaded");
+                    cudaEventDestroy(r->loaded);
+                    r->loaded = nullptr;
+                    w.control = dev_controls + slot;
+                    w.dev.control = w.control;
+                    host_wraps[slot] = w.dev;
+                    check(cudaMemcpyAsync(dev_controls + slot, &w.initial_control, sizeof(WrapControl),
+                                          cudaMemcpyHostToDevice, stream), "slot control");
+                    check(cudaMemcpyAsync(dev_wraps + slot, &host_wraps[slot], sizeof(WrapDev),
+                                          cudaMemcpyHostToDevice, stream), "slot descriptor");
+                    slot_nodes[slot] = w.max_nodes;
+                    grow_shape(w);
+                }
+                count = running_snapshot();
+                cudaGraphExec_t g = graph_for(count);
+                for (int i = 0; i < per_poll; ++i) check(cudaGraphLaunch(g, stream), "graph launch");
+                check(cudaMemcpyAsync(host_controls, dev_controls, sizeof(WrapControl) * count,
                                       cudaMemcpyDeviceToHost, stream), "pull controls");
                 check(cudaStreamSynchronize(stream), "tick");
             } catch (const std::exception& e) {
                 // the device failed under every running request
                 std::lock_guard<std::mutex> lk(mu);
                 for (int i = 0; i < slots_used; ++i)
-                    if (slot_req[i] && slot_req[i]->state == NRICP_REQUEST_RUNNING) {
-                        running -= 1;
+                    if (slot_req[i]) {
                         fail(slot_req[i], e.what(), false);
+                        slot_req[i] = nullptr;
                     }
+                running = 0;
                 stop = true;
                 cv_work.notify_all();
                 return;
             }
             ticks += per_poll;
-            launches += (long)per_poll * tick_kernel_launches(shape);
-            for (int i = 0; i < slots_used; ++i) {
+            launches += (long)per_poll * launches_per_tick[count];
+            std::vector<int> holes;
+            for (int i = 0; i < count; ++i) {
                 RequestPtr r = slot_req[i];
-                if (!r || r->state != NRICP_REQUEST_RUNNING || host_controls[i].phase != kPhaseDone) continue;
+                if (!r || host_controls[i].phase != kPhaseDone) continue;
+                holes.push_back(i);
                 std::string why;
                 if (host_controls[i].error) {
                     why = "a closest-point traversal exceeded its stack; the hierarchy is too deep";
@@ -1239,7 +1349,9 @@ struct Server::Impl {
                         why = e.what();
                     }
                 }
+                bury(r);
                 std::lock_guard<std::mutex> lk(mu);
+                slot_req[i] = nullptr;
                 running -= 1;
                 if (!why.empty()) {
                     fail(r, why, false);
@@ -1251,8 +1363,36 @@ struct Server::Impl {
                 last_done = std::max(last_done, r->t_done);
                 completed += 1;
                 cv_done.notify_all();
+                cv_work.notify_all();
+            }
+            // keep the running wraps in slots 0 .. running-1: the last running
+            // wraps fill the holes the retired ones left
+            try {
+                int last = count - 1;
+                for (int hole : holes) {
+                    while (last > hole && !slot_req[last]) --last;
+                    if (last <= hole) break;
+                    move_slot(last, hole);
+                    --last;
+                }
+            } catch (const std::exception& e) {
+                std::lock_guard<std::mutex> lk(mu);
+                for (int i = 0; i < slots_used; ++i)
+                    if (slot_req[i]) {
+                        fail(slot_req[i], e.what(), false);
+                        slot_req[i] = nullptr;
+                    }
+                running = 0;
+                stop = true;
+                cv_work.notify_all();
+                return;
             }
         }
+    }
+
+    int running_snapshot() {
+        std::lock_guard<std::mutex> lk(mu);
+        return running;
     }
 };
 
@@ -1272,6 +1412,17 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
         m.cfg.memory_budget_bytes = free_bytes / 10 * 9;
     }
     check(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&m.load_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = m.device;
+        check(cudaMemPoolCreate(&m.pool, &props), "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;  // keep freed arenas for the next requests
+        check(cudaMemPoolSetAttribute(m.pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool");
+    }
+    check(cudaMalloc(&m.staging_control, sizeof(WrapControl)), "cudaMalloc(staging control)");
     check(cudaMalloc(&m.dev_wraps, sizeof(WrapDev) * m.cfg.max_slots), "cudaMalloc(slots)");
     check(cudaMalloc(&m.dev_controls, sizeof(WrapControl) * m.cfg.max_slots), "cudaMalloc(controls)");
     check(cudaMallocHost(&m.host_controls, sizeof(WrapControl) * m.cfg.max_slots), "cudaMallocHost(controls)");
@@ -1281,6 +1432,7 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     int threads = m.cfg.prep_threads;
     if (threads <= 0) threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / 2);
     for (int i = 0; i < threads; ++i) m.preppers.emplace_back([&m] { m.prep_loop(); });
+    m.loader_thread = std::thread([&m] { m.loader_loop(); });
     m.pump_thread = std::thread([&m] { m.pump_loop(); });
 }
 
@@ -1294,18 +1446,28 @@ Server::~Server() {
     m.cv_done.notify_all();
     for (auto& t : m.preppers) t.join();
     if (m.pump_thread.joinable()) m.pump_thread.join();
+    if (m.loader_thread.joinable()) m.loader_thread.join();
     cudaSetDevice(m.device);
     cudaStreamSynchronize(m.stream);
-    if (m.graph) cudaGraphExecDestroy(m.graph);
+    cudaStreamSynchronize(m.load_stream);
+    for (auto& [count, g] : m.graphs) cudaGraphExecDestroy(g);
+    for (auto& r : m.loaded)
+        if (r->loaded) cudaEventDestroy(r->loaded);
+    for (auto& d : m.graveyard) cudaEventDestroy(d.after);
+    m.graveyard.clear();
     m.slot_req.clear();
     m.requests.clear();
     m.ready.clear();
+    m.loaded.clear();
     m.prep_queue.clear();
     if (m.lbvh_scratch) cudaFree(m.lbvh_scratch);
+    if (m.staging_control) cudaFree(m.staging_control);
     if (m.dev_wraps) cudaFree(m.dev_wraps);
     if (m.dev_controls) cudaFree(m.dev_controls);
     if (m.host_controls) cudaFreeHost(m.host_controls);
     cudaStreamDestroy(m.stream);
+    cudaStreamDestroy(m.load_stream);
+    if (m.pool) cudaMemPoolDestroy(m.pool);
 }
 
 long Server::submit(const NricpSolveDesc& desc) {
@@ -1390,7 +1552,7 @@ NricpServerStats Server::stats() {
     s.completed = m.completed;
     s.failed = m.failed;
     s.running = m.running;
-    s.waiting = static_cast<long>(m.prep_queue.size() + m.ready.size());
+    s.waiting = static_cast<long>(m.prep_queue.size() + m.ready.size() + m.loaded.size()) + m.loading;
     s.latency_p50_ms = 1000.0 * percentile(m.latencies, 0.50);
     s.latency_p99_ms = 1000.0 * percentile(m.latencies, 0.99);
     double sum = 0.0;

@@ -210,6 +210,11 @@ class WrapServer:
         check(load().nricp_server_poll(self._handle, request, C.byref(status), C.byref(latency)))
         return _abi.REQUEST_STATES[status.value], latency.value
 
+    def wait(self, request: int, timeout: float | None = None) -> tuple[str, float]:
+        """Blocks until the request is done or failed; returns poll()."""
+        check(load().nricp_server_wait(self._handle, request, float(timeout or 0.0)))
+        return self.poll(request)
+
     def result(self, request: int, timeout: float | None = None) -> dict:
         """Waits for the request and returns its result dict (as solve_route_b)."""
         check(load().nricp_server_wait(self._handle, request, float(timeout or 0.0)))
