@@ -72,6 +72,8 @@ def parse_args():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-profile", action="store_true")
+    p.add_argument("--instances", type=int, default=INSTANCES,
+                   help="wraps in the batch (config 3 has 64; fewer for profiling captures)")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--serve-rates", default="20,80",
                    help="Poisson arrival rates (requests/s) of the serving windows")
@@ -95,10 +97,10 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def make_cases(seed: int):
+def make_cases(seed: int, instances: int = INSTANCES):
     from nricp_b200 import synthetic as S
 
-    return S.config3(seed, instances=INSTANCES, workers=min(16, host_cores()))
+    return S.config3(seed, instances=instances, workers=min(16, host_cores()))
 
 
 def reference_options(options: dict) -> dict:
@@ -383,7 +385,7 @@ def run_ours(args, ranks):
     from nricp_b200 import synthetic as S
 
     torch.cuda.set_device(ranks.local)
-    cases = make_cases(args.seed + ranks.rank)
+    cases = make_cases(args.seed + ranks.rank, args.instances)
     tuples = [(*c.args(), c.options) for c in cases]
 
     # ---- value: the batch, device-resident ----
