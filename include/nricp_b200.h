@@ -321,14 +321,16 @@ void nricp_server_destroy(NricpServer* server);
 
 /* build_template_graph(...) (bindings.cpp:886-925), one level: the
  * normalisation, the sampled nodes, the bindings (stride NRICP_MAX_SLOTS) and
- * the k-NN edges of `level`. */
+ * the k-NN edges of `level`.  `use_device` (the reference's own flag) builds
+ * it on the GPU, bit-identical to the host build. */
 int nricp_template_graph_level(const double* points, int count, int levels,
                                int nodes_initial, int growth, int max_nodes,
                                int edge_neighbours, int level, double* center,
                                double* scale, int32_t* template_indices,
                                double* node_positions, int32_t* bind_nodes,
                                double* bind_weights, int32_t* bind_counts,
-                               int32_t* edges, int edge_capacity, int* edge_count);
+                               int32_t* edges, int edge_capacity, int* edge_count,
+                               int use_device);
 
 /* closest_points(...) (bindings.cpp:1004-1044 -> src/cuda/lbvh.cu:439-533):
  * nearest target point, interpolated normal, distance and triangle per query,

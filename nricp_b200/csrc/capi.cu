@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "host.hpp"
 #include "kernels.cuh"
+#include "graph_build.hpp"
 #include "session.hpp"
 
 using namespace nricp_b200;
@@ -347,12 +348,28 @@ int nricp_template_graph_level(const double* points, int count, int levels, int 
                                double* center, double* scale, int32_t* template_indices,
                                double* node_positions, int32_t* bind_nodes, double* bind_weights,
                                int32_t* bind_counts, int32_t* edges, int edge_capacity,
-                               int* edge_count) {
+                               int* edge_count, int use_device) {
     return guarded([&] {
         if (count <= 0) throw InvalidArgument("invalid mesh: mesh has no vertices");
         if (max_nodes > NRICP_MAX_SLOTS) throw InvalidArgument("max_nodes_per_vertex exceeds 8");
-        const TemplateGraph g = build_template_graph(points, count, levels, nodes_initial, growth,
-                                                     max_nodes, edge_neighbours);
+        TemplateGraph g;
+        if (use_device && device_graph_supported(edge_neighbours)) {
+            require_device();
+            cudaStream_t stream;
+            check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+            try {
+                g = std::move(device_template_graphs(
+                    {GraphRequest{points, count, levels, nodes_initial, growth, max_nodes, edge_neighbours}},
+                    stream)[0]);
+            } catch (...) {
+                cudaStreamDestroy(stream);
+                throw;
+            }
+            cudaStreamDestroy(stream);
+        } else {
+            g = build_template_graph(points, count, levels, nodes_initial, growth, max_nodes,
+                                     edge_neighbours);
+        }
         if (level < 0 || level >= static_cast<int>(g.levels.size()))
             throw InvalidArgument("level out of range");
         const GraphLevel& L = g.levels[level];

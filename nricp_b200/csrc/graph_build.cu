@@ -1,0 +1,394 @@
+// The template graphs of many wraps at once on the device: farthest-point
+// seeds, the nearest-node bindings of every vertex and the k-NN node edges of
+// every level (src/core/graph.cpp:41-76, src/core/sampling.cpp:17-143).
+//
+// Every value is the host build's to the bit: the same FP64 operations in the
+// same order, each rounded on its own (no contraction), and the same tie
+// rules -- the first maximum for the seeds, (squared distance, index) for the
+// bindings, (distance, index) for the edges.  Only the scan orders differ,
+// and none of the rules depends on them.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "graph_build.hpp"
+#include "session.hpp"
+
+namespace nricp_b200 {
+
+namespace {
+
+constexpr int kFpsThreads = 1024;
+constexpr int kBindThreads = 128;
+constexpr int kTile = 512;            // nodes staged in shared memory per pass
+constexpr int kMaxEdgeNeighbours = 16;
+
+__device__ inline double sq_rn(const double* a, const double* b) {  // sampling.cpp:17-19
+    const double x = __dsub_rn(a[0], b[0]), y = __dsub_rn(a[1], b[1]), z = __dsub_rn(a[2], b[2]);
+    return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+// (value, index) with the larger value winning and the lower index breaking ties.
+__device__ inline void arg_max(double& v, int& i, double ov, int oi) {
+    if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+}
+
+// One block per template: seeds[0] = 0, then repeatedly the point farthest
+// from all seeds so far (sampling.cpp:47-88).
+__global__ void __launch_bounds__(kFpsThreads) k_fps(const double* __restrict__ points,
+                                                     const long* __restrict__ point_offset,
+                                                     const int* __restrict__ point_count,
+                                                     const int* __restrict__ seed_count,
+                                                     const long* __restrict__ seed_offset,
+                                                     double* __restrict__ nearest_all,
+                                                     int* __restrict__ seeds_all) {
+    const int t = blockIdx.x;
+    const int n = point_count[t];
+    const int count = min(seed_count[t], n);
+    if (n <= 0 || count <= 0) return;
+    const double* p = points + point_offset[t] * 3;
+    double* nearest = nearest_all + point_offset[t];
+    int* seeds = seeds_all + seed_offset[t];
+    __shared__ double red_v[kFpsThreads / 32];
+    __shared__ int red_i[kFpsThreads / 32];
+    __shared__ int chosen_s;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto block_arg_max = [&](double v, int i) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+            arg_max(v, i, ov, oi);
+        }
+        if (lane == 0) { red_v[warp] = v; red_i[warp] = i; }
+        __syncthreads();
+        if (warp == 0) {
+            v = lane < kFpsThreads / 32 ? red_v[lane] : -1.0;
+            i = lane < kFpsThreads / 32 ? red_i[lane] : 0x7fffffff;
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+                arg_max(v, i, ov, oi);
+            }
+            if (lane == 0) chosen_s = i;
+        }
+        __syncthreads();
+        return chosen_s;
+    };
+    if (threadIdx.x == 0) seeds[0] = 0;
+    double c[3] = {p[0], p[1], p[2]};
+    double bv = -1.0;
+    int bi = 0x7fffffff;
+    for (int i = threadIdx.x; i < n; i += kFpsThreads) {
+        const double d = sq_rn(p + (long)i * 3, c);
+        nearest[i] = d;
+        arg_max(bv, bi, d, i);
+    }
+    int best = block_arg_max(bv, bi);
+    for (int k = 1; k < count; ++k) {
+        if (threadIdx.x == 0) seeds[k] = best;
+        c[0] = p[(long)best * 3];
+        c[1] = p[(long)best * 3 + 1];
+        c[2] = p[(long)best * 3 + 2];
+        bv = -1.0;
+        bi = 0x7fffffff;
+        for (int i = threadIdx.x; i < n; i += kFpsThreads) {
+            const double d = sq_rn(p + (long)i * 3, c);
+            const double m = nearest[i] < d ? nearest[i] : d;
+            nearest[i] = m;
+            arg_max(bv, bi, m, i);
+        }
+        best = block_arg_max(bv, bi);
+    }
+}
+
+// (sq, idx) kept sorted ascending, at most `capacity` entries, entries offered
+// in increasing index (sampling.cpp:23-42).
+__device__ inline void keep(double* sq, int* idx, int& held, int capacity, double value, int entry) {
+    if (held == capacity && !(value < sq[capacity - 1] || (value == sq[capacity - 1] && entry < idx[capacity - 1])))
+        return;
+    int at = held < capacity ? held++ : capacity - 1;
+    while (at > 0 && (sq[at - 1] > value || (sq[at - 1] == value && idx[at - 1] > entry))) {
+        sq[at] = sq[at - 1];
+        idx[at] = idx[at - 1];
+        --at;
+    }
+    sq[at] = value;
+    idx[at] = entry;
+}
+
+// Thread per (template, vertex) for one level: its `support` nearest nodes
+// and weights (1 - d / d_max)^2, normalised (sampling.cpp:90-143).
+__global__ void __launch_bounds__(kBindThreads) k_bind(const double* __restrict__ points,
+                                                       const long* __restrict__ point_offset,
+                                                       const int* __restrict__ point_count,
+                                                       const int* __restrict__ seeds_all,
+                                                       const long* __restrict__ seed_offset,
+                                                       const int* __restrict__ level_nodes,
+                                                       const int* __restrict__ support_of,
+                                                       const long* __restrict__ bind_offset,
+                                                       int* __restrict__ bind_nodes,
+                                                       double* __restrict__ bind_weights) {
+    const int t = blockIdx.y;
+    const int n = point_count[t], nc = level_nodes[t];
+    if (nc <= 0 || (long)blockIdx.x * kBindThreads >= n) return;
+    const int v = blockIdx.x * kBindThreads + threadIdx.x;
+    const double* p = points + point_offset[t] * 3;
+    const int* seeds = seeds_all + seed_offset[t];
+    const int support = support_of[t];
+    __shared__ double tile[kTile * 3];
+    double sq[NRICP_MAX_SLOTS];
+    int idx[NRICP_MAX_SLOTS];
+    int held = 0;
+    double q[3] = {0.0, 0.0, 0.0};
+    if (v < n) { q[0] = p[(long)v * 3]; q[1] = p[(long)v * 3 + 1]; q[2] = p[(long)v * 3 + 2]; }
+    for (int base = 0; base < nc; base += kTile) {
+        const int m = min(kTile, nc - base);
+        __syncthreads();
+        for (int j = threadIdx.x; j < m * 3; j += kBindThreads) {
+            const int node = base + j / 3;
+            tile[j] = p[(long)seeds[node] * 3 + j % 3];
+        }
+        __syncthreads();
+        if (v < n)
+            for (int j = 0; j < m; ++j) keep(sq, idx, held, support, sq_rn(q, tile + j * 3), base + j);
+    }
+    if (v >= n) return;
+    const long at = bind_offset[t] + (long)v * NRICP_MAX_SLOTS;
+    const double dmax = __dsqrt_rn(sq[support - 1]);
+    double w[NRICP_MAX_SLOTS];
+    double total = 0.0;
+    for (int s = 0; s < support; ++s) {
+        const double distance = __dsqrt_rn(sq[s]);
+        const double ratio = dmax > 0.0 ? __ddiv_rn(distance, dmax) : 0.0;
+        const double falloff = __dsub_rn(1.0, ratio);
+        w[s] = __dmul_rn(falloff, falloff);
+        total = __dadd_rn(total, w[s]);
+    }
+    for (int s = 0; s < NRICP_MAX_SLOTS; ++s) {
+        bind_nodes[at + s] = s < support ? idx[s] : -1;
+        bind_weights[at + s] =
+            s < support ? (total > 0.0 ? __ddiv_rn(w[s], total) : __ddiv_rn(1.0, (double)support)) : 0.0;
+    }
+}
+
+// Thread per (template, node) for one level: the `taken` nearest other nodes
+// by (distance, index) (graph.cpp:11-39).
+__global__ void __launch_bounds__(kBindThreads) k_neighbours(const double* __restrict__ points,
+                                                             const long* __restrict__ point_offset,
+                                                             const int* __restrict__ seeds_all,
+                                                             const long* __restrict__ seed_offset,
+                                                             const int* __restrict__ level_nodes,
+                                                             const int* __restrict__ taken_of,
+                                                             const long* __restrict__ edge_offset,
+                                                             int* __restrict__ neighbours) {
+    const int t = blockIdx.y;
+    const int nc = level_nodes[t];
+    if ((long)blockIdx.x * kBindThreads >= nc) return;
+    const int i = blockIdx.x * kBindThreads + threadIdx.x;
+    const double* p = points + point_offset[t] * 3;
+    const int* seeds = seeds_all + seed_offset[t];
+    const int taken = taken_of[t];
+    __shared__ double tile[kTile * 3];
+    double dist[kMaxEdgeNeighbours];
+    int idx[kMaxEdgeNeighbours];
+    int held = 0;
+    double q[3] = {0.0, 0.0, 0.0};
+    if (i < nc) {
+        const long s = seeds[i];
+        q[0] = p[s * 3]; q[1] = p[s * 3 + 1]; q[2] = p[s * 3 + 2];
+    }
+    for (int base = 0; base < nc; base += kTile) {
+        const int m = min(kTile, nc - base);
+        __syncthreads();
+        for (int j = threadIdx.x; j < m * 3; j += kBindThreads) tile[j] = p[(long)seeds[base + j / 3] * 3 + j % 3];
+        __syncthreads();
+        if (i < nc && taken > 0)
+            for (int j = 0; j < m; ++j) {
+                const int o = base + j;
+                if (o == i) continue;
+                const double x = __dsub_rn(q[0], tile[j * 3]), y = __dsub_rn(q[1], tile[j * 3 + 1]),
+                             z = __dsub_rn(q[2], tile[j * 3 + 2]);
+                const double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+                keep(dist, idx, held, taken, d, o);
+            }
+    }
+    if (i >= nc) return;
+    for (int k = 0; k < taken; ++k) neighbours[edge_offset[t] + (long)i * taken + k] = idx[k];
+}
+
+int blocks(long n, int threads) { return static_cast<int>((n + threads - 1) / threads); }
+
+template <typename T>
+T* to_device(const std::vector<T>& v, std::vector<void*>& owned, cudaStream_t stream) {
+    T* d = nullptr;
+    check(cudaMalloc(&d, sizeof(T) * std::max<size_t>(1, v.size())), "cudaMalloc(graph build)");
+    owned.push_back(d);
+    if (!v.empty())
+        check(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, stream), "upload");
+    return d;
+}
+
+}  // namespace
+
+bool device_graph_supported(int edge_neighbours) { return edge_neighbours <= kMaxEdgeNeighbours; }
+
+std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest>& requests,
+                                                  cudaStream_t stream) {
+    const int W = static_cast<int>(requests.size());
+    std::vector<TemplateGraph> out(W);
+    if (W == 0) return out;
+    // host: normalisation (mesh.cpp:174-187) and the sizes of every level
+    std::vector<double> points;
+    std::vector<long> point_offset(W), seed_offset(W);
+    std::vector<int> point_count(W), seed_count(W);
+    std::vector<std::vector<int>> level_sizes(W);
+    long total_points = 0, total_seeds = 0;
+    int max_levels = 0, max_points = 0;
+    for (int t = 0; t < W; ++t) {
+        const GraphRequest& r = requests[t];
+        TemplateGraph& g = out[t];
+        compute_normalization(r.points, r.count, g.center, &g.scale);
+        const std::vector<double> norm = normalized(r.points, r.count, g.center, g.scale);
+        points.insert(points.end(), norm.begin(), norm.end());
+        point_offset[t] = total_points;
+        point_count[t] = r.count;
+        total_points += r.count;
+        const int levels = std::max(1, r.levels);
+        int most = 0;
+        for (int l = 0; l < levels; ++l) {
+            level_sizes[t].push_back(level_node_count(l, r.nodes_initial, r.growth, r.count));
+            most = std::max(most, level_sizes[t].back());
+        }
+        most = std::min(most, r.count);
+        seed_offset[t] = total_seeds;
+        seed_count[t] = most;
+        total_seeds += most;
+        max_levels = std::max(max_levels, levels);
+        max_points = std::max(max_points, r.count);
+    }
+    std::vector<void*> owned;
+    double* d_points = to_device(points, owned, stream);
+    long* d_point_offset = to_device(point_offset, owned, stream);
+    int* d_point_count = to_device(point_count, owned, stream);
+    int* d_seed_count = to_device(seed_count, owned, stream);
+    long* d_seed_offset = to_device(seed_offset, owned, stream);
+    double* d_nearest = nullptr;
+    int* d_seeds = nullptr;
+    check(cudaMalloc(&d_nearest, sizeof(double) * std::max<long>(1, total_points)), "cudaMalloc(graph build)");
+    owned.push_back(d_nearest);
+    check(cudaMalloc(&d_seeds, sizeof(int) * std::max<long>(1, total_seeds)), "cudaMalloc(graph build)");
+    owned.push_back(d_seeds);
+    k_fps<<<W, kFpsThreads, 0, stream>>>(d_points, d_point_offset, d_point_count, d_seed_count,
+                                         d_seed_offset, d_nearest, d_seeds);
+    check(cudaGetLastError(), "farthest-point seeds");
+    std::vector<int> seeds(std::max<long>(1, total_seeds));
+    check(cudaMemcpyAsync(seeds.data(), d_seeds, sizeof(int) * seeds.size(), cudaMemcpyDeviceToHost, stream),
+          "download seeds");
+
+    // per level: bindings and neighbour lists of every template in one launch each
+    std::vector<std::vector<int32_t>> bind_nodes(max_levels), neighbours(max_levels);
+    std::vector<std::vector<double>> bind_weights(max_levels);
+    std::vector<std::vector<long>> edge_offsets(max_levels);
+    std::vector<std::vector<int>> takens(max_levels), supports(max_levels);
+    const long bind_entries = total_points * NRICP_MAX_SLOTS;
+    int32_t* d_bind_nodes = nullptr;
+    double* d_bind_weights = nullptr;
+    check(cudaMalloc(&d_bind_nodes, sizeof(int32_t) * std::max<long>(1, bind_entries)), "cudaMalloc(graph build)");
+    owned.push_back(d_bind_nodes);
+    check(cudaMalloc(&d_bind_weights, sizeof(double) * std::max<long>(1, bind_entries)), "cudaMalloc(graph build)");
+    owned.push_back(d_bind_weights);
+    std::vector<long> bind_offset(W);
+    for (int t = 0; t < W; ++t) bind_offset[t] = point_offset[t] * NRICP_MAX_SLOTS;
+    long* d_bind_offset = to_device(bind_offset, owned, stream);
+    for (int l = 0; l < max_levels; ++l) {
+        std::vector<int> nodes(W, 0), support(W, 1), taken(W, 0);
+        std::vector<long> eoff(W, 0);
+        long edge_total = 0;
+        int max_nodes = 0;
+        for (int t = 0; t < W; ++t) {
+            const GraphRequest& r = requests[t];
+            if (l >= static_cast<int>(level_sizes[t].size())) continue;
+            nodes[t] = std::min(level_sizes[t][l], seed_count[t]);
+            support[t] = std::max(1, std::min({r.max_nodes, nodes[t], NRICP_MAX_SLOTS}));
+            taken[t] = nodes[t] > 1 && r.edge_neighbours > 0 ? std::min(r.edge_neighbours, nodes[t] - 1) : 0;
+            eoff[t] = edge_total;
+            edge_total += static_cast<long>(nodes[t]) * taken[t];
+            max_nodes = std::max(max_nodes, nodes[t]);
+        }
+        int* d_nodes = to_device(nodes, owned, stream);
+        int* d_support = to_device(support, owned, stream);
+        int* d_taken = to_device(taken, owned, stream);
+        long* d_eoff = to_device(eoff, owned, stream);
+        int* d_neigh = nullptr;
+        check(cudaMalloc(&d_neigh, sizeof(int) * std::max<long>(1, edge_total)), "cudaMalloc(graph build)");
+        owned.push_back(d_neigh);
+        k_bind<<<dim3(blocks(max_points, kBindThreads), W), kBindThreads, 0, stream>>>(
+            d_points, d_point_offset, d_point_count, d_seeds, d_seed_offset, d_nodes, d_support,
+            d_bind_offset, d_bind_nodes, d_bind_weights);
+        check(cudaGetLastError(), "bindings");
+        if (max_nodes > 0)
+            k_neighbours<<<dim3(blocks(max_nodes, kBindThreads), W), kBindThreads, 0, stream>>>(
+                d_points, d_point_offset, d_seeds, d_seed_offset, d_nodes, d_taken, d_eoff, d_neigh);
+        check(cudaGetLastError(), "node edges");
+        bind_nodes[l].resize(std::max<long>(1, bind_entries));
+        bind_weights[l].resize(std::max<long>(1, bind_entries));
+        neighbours[l].resize(std::max<long>(1, edge_total));
+        check(cudaMemcpyAsync(bind_nodes[l].data(), d_bind_nodes, sizeof(int32_t) * bind_nodes[l].size(),
+                              cudaMemcpyDeviceToHost, stream), "download bindings");
+        check(cudaMemcpyAsync(bind_weights[l].data(), d_bind_weights, sizeof(double) * bind_weights[l].size(),
+                              cudaMemcpyDeviceToHost, stream), "download bindings");
+        check(cudaMemcpyAsync(neighbours[l].data(), d_neigh, sizeof(int) * neighbours[l].size(),
+                              cudaMemcpyDeviceToHost, stream), "download edges");
+        // the next level's bindings reuse the device buffer: wait for the copy
+        check(cudaStreamSynchronize(stream), "graph build");
+        edge_offsets[l] = eoff;
+        takens[l] = taken;
+        supports[l] = support;
+    }
+    check(cudaStreamSynchronize(stream), "graph build");
+    for (void* p : owned) cudaFree(p);
+
+    // host: the graphs in the host build's form
+    for (int t = 0; t < W; ++t) {
+        TemplateGraph& g = out[t];
+        const int levels = static_cast<int>(level_sizes[t].size());
+        for (int l = 0; l < levels; ++l) {
+            GraphLevel level;
+            const int n = std::min(level_sizes[t][l], seed_count[t]);
+            level.template_index.assign(seeds.begin() + seed_offset[t], seeds.begin() + seed_offset[t] + n);
+            level.rest.resize(static_cast<size_t>(n) * 3);
+            for (int i = 0; i < n; ++i)
+                for (int k = 0; k < 3; ++k)
+                    level.rest[i * 3 + k] = points[(point_offset[t] + level.template_index[i]) * 3 + k];
+            level.bindings.resize(point_count[t]);
+            for (int v = 0; v < point_count[t]; ++v) {
+                Binding& b = level.bindings[v];
+                const long at = (point_offset[t] + v) * NRICP_MAX_SLOTS;
+                for (int s = 0; s < NRICP_MAX_SLOTS; ++s) {
+                    b.nodes[s] = bind_nodes[l][at + s];
+                    b.weights[s] = bind_weights[l][at + s];
+                }
+                b.count = supports[l][t];
+            }
+            const int taken = takens[l][t];
+            std::vector<std::pair<int, int>> pairs;
+            pairs.reserve(static_cast<size_t>(n) * taken);
+            for (int i = 0; i < n; ++i)
+                for (int k = 0; k < taken; ++k) {
+                    const int o = neighbours[l][edge_offsets[l][t] + static_cast<long>(i) * taken + k];
+                    pairs.emplace_back(std::min(i, o), std::max(i, o));
+                }
+            std::sort(pairs.begin(), pairs.end());
+            pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+            level.edges.reserve(pairs.size() * 2);
+            for (auto& p : pairs) {
+                level.edges.push_back(p.first);
+                level.edges.push_back(p.second);
+            }
+            g.levels.push_back(std::move(level));
+        }
+    }
+    return out;
+}
+
+}  // namespace nricp_b200

@@ -24,6 +24,7 @@
 #include "../../include/nricp_b200.h"
 #include "common.cuh"
 #include "host.hpp"
+#include "graph_build.hpp"
 #include "kernels.cuh"
 #include "session.hpp"
 
@@ -169,17 +170,24 @@ void copy_inputs(Wrap& w, const NricpSolveDesc& d) {
     w.desc.landmark_count = w.L;
 }
 
-void prepare_host(Wrap& w) {
+void check_graph_capacity(const Wrap& w) {
     const NricpSolveDesc& d = w.desc;
-    const int k = d.max_nodes_per_vertex > 0 ? d.max_nodes_per_vertex : 4;
-    const int edge_k = d.edge_neighbours > 0 ? d.edge_neighbours : 4;
     const int finest = level_node_count(std::max(1, d.graph_levels) - 1, d.nodes_initial, d.growth, w.V);
     if (finest > pcg_max_nodes())
         throw CapacityError("the finest graph level has " + std::to_string(finest) +
                             " nodes; the device solve supports at most " +
                             std::to_string(pcg_max_nodes()));
-    w.graph = build_template_graph(d.template_points, w.V, d.graph_levels, d.nodes_initial,
-                                   d.growth, k, edge_k);
+}
+
+GraphRequest graph_request(const Wrap& w) {
+    const NricpSolveDesc& d = w.desc;
+    return GraphRequest{w.template_in.data(), w.V, d.graph_levels, d.nodes_initial, d.growth,
+                        d.max_nodes_per_vertex > 0 ? d.max_nodes_per_vertex : 4,
+                        d.edge_neighbours > 0 ? d.edge_neighbours : 4};
+}
+
+// The level layouts and size envelope of a wrap whose graph is built.
+void finish_host(Wrap& w) {
     w.levels = static_cast<int>(w.graph.levels.size());
     w.layouts.clear();
     for (int l = 0; l < w.levels; ++l) {
@@ -190,6 +198,15 @@ void prepare_host(Wrap& w) {
         w.max_pairs = std::max(w.max_pairs, L.pair_count);
         w.max_offdiag = std::max(w.max_offdiag, L.edge_count + L.pair_count);
     }
+}
+
+// The host build: graph (bit-identical to the reference's) and layouts.
+void prepare_host(Wrap& w) {
+    check_graph_capacity(w);
+    const GraphRequest r = graph_request(w);
+    w.graph = build_template_graph(r.points, r.count, r.levels, r.nodes_initial, r.growth, r.max_nodes,
+                                   r.edge_neighbours);
+    finish_host(w);
 }
 
 size_t bytes_of_layout(const LevelLayout& L) {
@@ -500,31 +517,19 @@ Batch::~Batch() {
     if (stream_) cudaStreamDestroy(stream_);
 }
 
-namespace {
-std::unique_ptr<Wrap> make_wrap(const NricpSolveDesc& desc) {
-    NricpSolveDesc d = desc;
-    validate_settings(d);
-    auto w = std::make_unique<Wrap>();
-    const double t0 = now_seconds();
-    copy_inputs(*w, d);
-    prepare_host(*w);
-    w->setup_seconds = now_seconds() - t0;
-    return w;
-}
-}  // namespace
 
-void Batch::add(const NricpSolveDesc& desc) { wraps_.push_back(make_wrap(desc)); }
+void Batch::add(const NricpSolveDesc& desc) { add_all(&desc, 1); }
 
 void Batch::add_all(const NricpSolveDesc* descs, int count) {
-    // the wraps' host preparation is independent: one wrap per host thread
-    // (a single wrap keeps the threads for its own graph build)
+    // Inputs copied and checked on the host's cores (one wrap per thread),
+    // every template graph built in one device pass (bit-identical to the
+    // host build), then the level layouts on the host's cores again.
     std::vector<std::unique_ptr<Wrap>> prepared(count);
     std::vector<int> kind(count, 0);
     std::vector<std::string> message(count);
-#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
-    for (int i = 0; i < count; ++i) {
+    auto guarded_step = [&](int i, auto&& step) {
         try {
-            prepared[i] = make_wrap(descs[i]);
+            step();
         } catch (const InvalidArgument& e) {
             kind[i] = 1;
             message[i] = e.what();
@@ -537,14 +542,50 @@ void Batch::add_all(const NricpSolveDesc* descs, int count) {
             kind[i] = 4;
             message[i] = e.what();
         }
+    };
+    auto raise_first = [&] {
+        for (int i = 0; i < count; ++i) {
+            if (kind[i] == 1) throw InvalidArgument(message[i]);
+            if (kind[i] == 2) throw CapacityError(message[i]);
+            if (kind[i] == 3) throw std::bad_alloc();
+            if (kind[i] == 4) throw std::runtime_error(message[i]);
+        }
+    };
+    const double t0 = now_seconds();
+#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
+    for (int i = 0; i < count; ++i)
+        guarded_step(i, [&] {
+            NricpSolveDesc d = descs[i];
+            validate_settings(d);
+            auto w = std::make_unique<Wrap>();
+            copy_inputs(*w, d);
+            check_graph_capacity(*w);
+            prepared[i] = std::move(w);
+        });
+    raise_first();
+    bool device = true;
+    for (const auto& w : prepared) device = device && device_graph_supported(graph_request(*w).edge_neighbours);
+    if (device) {
+        std::vector<GraphRequest> requests;
+        for (const auto& w : prepared) requests.push_back(graph_request(*w));
+        std::vector<TemplateGraph> graphs = device_template_graphs(requests, stream_);
+        for (int i = 0; i < count; ++i) prepared[i]->graph = std::move(graphs[i]);
     }
-    for (int i = 0; i < count; ++i) {
-        if (kind[i] == 1) throw InvalidArgument(message[i]);
-        if (kind[i] == 2) throw CapacityError(message[i]);
-        if (kind[i] == 3) throw std::bad_alloc();
-        if (kind[i] == 4) throw std::runtime_error(message[i]);
+#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
+    for (int i = 0; i < count; ++i)
+        guarded_step(i, [&] {
+            if (device) {
+                finish_host(*prepared[i]);
+            } else {
+                prepare_host(*prepared[i]);
+            }
+        });
+    raise_first();
+    const double spent = (now_seconds() - t0) / std::max(1, count);
+    for (auto& w : prepared) {
+        w->setup_seconds = spent;
+        wraps_.push_back(std::move(w));
     }
-    for (auto& w : prepared) wraps_.push_back(std::move(w));
 }
 
 void Batch::upload_all(LbvhExport* lbvh_out) {

@@ -395,8 +395,9 @@ def build_template_graph(points, faces, levels: int = 4, nodes_initial: int = 10
                          growth: int = 2, max_nodes_per_vertex: int = 4,
                          use_device: bool = False, edge_neighbours: int = 4) -> dict:
     """The cached template side: nodes, bindings and edges per level
-    (bindings.cpp:886-925).  Built with the reference's FP64 rules, so it is
-    identical to the reference's graph whichever `use_device` says."""
+    (bindings.cpp:886-925).  Built with the reference's FP64 rules on the
+    host, or with `use_device` on the GPU -- bit-identical either way, as
+    the reference requires of its device build (tests/test_graph_parity.py)."""
     p, f = _points(points, "points"), _faces(faces, "faces")
     report = validate_mesh(p, f)
     if not report["ok"]:
@@ -423,7 +424,7 @@ def build_template_graph(points, faces, levels: int = 4, nodes_initial: int = 10
             P(p, C.c_double), n, level_count, nodes_initial, growth, max_nodes_per_vertex,
             edge_neighbours, level, P(center, C.c_double), C.byref(scale), P(idx, C.c_int32),
             P(pos, C.c_double), P(bn, C.c_int32), P(bw, C.c_double), P(bc, C.c_int32),
-            P(edges, C.c_int32), cap, C.byref(count)))
+            P(edges, C.c_int32), cap, C.byref(count), int(bool(use_device))))
         support = max(4, int(max_nodes_per_vertex))
         out_levels.append({
             "node_positions": pos,
