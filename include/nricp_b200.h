@@ -244,10 +244,11 @@ int nricp_batch_step(NricpBatch* batch, double* device_ms);
 
 /* No reference counterpart.  Cluster size of the batch's linear solve: a
  * power of two from 1 to 16 gives every wrap that many CTAs in one launch;
- * 0 (the default) gives each wrap its own size (about 128 nodes per CTA), one
- * launch per size class, the classes running side by side; -s (s = 1..4)
- * halves those per-wrap sizes s times.  Every choice gives bit-identical
- * results; it trades one wrap's latency against the batch's throughput.
+ * 0 gives each wrap its own size (about 128 nodes per CTA), one launch per
+ * size class, the classes running side by side; -s (s = 1..4) halves those
+ * per-wrap sizes s times.  A new batch starts at the smallest s whose classes
+ * need at most three CTAs per SM.  Every choice gives bit-identical results;
+ * it trades one wrap's latency against the batch's throughput.
  * *cluster_out (may be NULL) receives the largest size in effect. */
 int nricp_batch_tune(NricpBatch* batch, int pcg_cluster, int* cluster_out);
 /* Per-tick records of wrap 0 from the last nricp_batch_profile. */
@@ -286,7 +287,10 @@ typedef struct NricpServerConfig {
     size_t memory_budget_bytes;  /* device bytes resident wraps may hold; 0: 90 % of free memory */
     int max_slots;               /* wraps resident at once (1..1024) */
     int prep_threads;            /* host threads preparing requests; 0: half the cores */
-    int pcg_cluster;             /* solve cluster size, a power of two up to 16; 0: by load */
+    int pcg_cluster;             /* solve cluster: > 0 one size (a power of two up to 16) for every
+                                    slot; 0 (the default) per-wrap latency classes, halved once
+                                    when the running wraps would need more than three CTAs per
+                                    SM; -s (1..4) latency classes always halved s times */
     int ticks_per_poll;          /* ticks launched between looks at the wraps' progress */
 } NricpServerConfig;
 typedef struct NricpServerStats {
@@ -295,6 +299,7 @@ typedef struct NricpServerStats {
     double queue_p50_ms;                                     /* submit -> admitted */
     double wraps_per_second;     /* completed / (last completion - first submission) */
     long ticks, launches, captures;
+    double busy_seconds;         /* device time of the tick launches */
     size_t resident_bytes, peak_resident_bytes;
     int slots_used;
 } NricpServerStats;

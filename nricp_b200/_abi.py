@@ -145,6 +145,7 @@ class ServerStats(C.Structure):
         ("latency_mean_ms", C.c_double), ("queue_p50_ms", C.c_double),
         ("wraps_per_second", C.c_double),
         ("ticks", C.c_long), ("launches", C.c_long), ("captures", C.c_long),
+        ("busy_seconds", C.c_double),
         ("resident_bytes", C.c_size_t), ("peak_resident_bytes", C.c_size_t),
         ("slots_used", C.c_int),
     ]

@@ -17,7 +17,7 @@ CSRC = HERE / "csrc"
 LIB = HERE / "libnricp_b200.so"
 SOURCES = ["host.cpp", "lbvh.cu", "wrap_kernels.cu", "graph_build.cu", "session.cu", "capi.cu",
            "static_scratch.cu"]
-HEADERS = ["common.cuh", "kernels.cuh", "host.hpp", "session.hpp", "graph_build.hpp"]
+HEADERS = ["common.cuh", "kernels.cuh", "host.hpp", "session.hpp", "graph_build.hpp", "staging.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -13,6 +13,7 @@
 
 #include "graph_build.hpp"
 #include "session.hpp"
+#include "staging.hpp"
 
 namespace nricp_b200 {
 
@@ -278,104 +279,130 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
     owned.push_back(d_nearest);
     check(cudaMalloc(&d_seeds, sizeof(int) * std::max<long>(1, total_seeds)), "cudaMalloc(graph build)");
     owned.push_back(d_seeds);
+    // every level's sizes, on the host
+    struct LevelPlan {
+        std::vector<int> nodes, support, taken;
+        std::vector<long> eoff;
+        long edge_total = 0;
+        int max_nodes = 0;
+    };
+    std::vector<LevelPlan> plan(max_levels);
+    long all_edges = 0;
+    std::vector<long> edge_base(max_levels + 1, 0);
+    for (int l = 0; l < max_levels; ++l) {
+        LevelPlan& p = plan[l];
+        p.nodes.assign(W, 0);
+        p.support.assign(W, 1);
+        p.taken.assign(W, 0);
+        p.eoff.assign(W, 0);
+        for (int t = 0; t < W; ++t) {
+            const GraphRequest& r = requests[t];
+            if (l >= static_cast<int>(level_sizes[t].size())) continue;
+            p.nodes[t] = std::min(level_sizes[t][l], seed_count[t]);
+            p.support[t] = std::max(1, std::min({r.max_nodes, p.nodes[t], NRICP_MAX_SLOTS}));
+            p.taken[t] = p.nodes[t] > 1 && r.edge_neighbours > 0 ? std::min(r.edge_neighbours, p.nodes[t] - 1) : 0;
+            p.eoff[t] = p.edge_total;
+            p.edge_total += static_cast<long>(p.nodes[t]) * p.taken[t];
+            p.max_nodes = std::max(p.max_nodes, p.nodes[t]);
+        }
+        edge_base[l + 1] = edge_base[l] + std::max<long>(1, p.edge_total);
+        all_edges = edge_base[l + 1];
+    }
+
+    // the downloads land in page-locked memory: seeds, then per level the
+    // bindings' nodes and weights, then every level's neighbour lists
+    const long bind_entries = std::max<long>(1, total_points * NRICP_MAX_SLOTS);
+    const size_t seed_bytes = (sizeof(int) * std::max<long>(1, total_seeds) + 255) & ~size_t(255);
+    const size_t level_bytes = (sizeof(int32_t) + sizeof(double)) * bind_entries;
+    StagingLease lease(seed_bytes + level_bytes * max_levels + sizeof(int) * all_edges);
+    int* seeds = reinterpret_cast<int*>(lease.data());
+    auto host_nodes = [&](int l) {
+        return reinterpret_cast<int32_t*>(lease.data() + seed_bytes + level_bytes * l);
+    };
+    auto host_weights = [&](int l) {
+        return reinterpret_cast<double*>(lease.data() + seed_bytes + level_bytes * l + sizeof(int32_t) * bind_entries);
+    };
+    int* host_neigh = reinterpret_cast<int*>(lease.data() + seed_bytes + level_bytes * max_levels);
+
     k_fps<<<W, kFpsThreads, 0, stream>>>(d_points, d_point_offset, d_point_count, d_seed_count,
                                          d_seed_offset, d_nearest, d_seeds);
     check(cudaGetLastError(), "farthest-point seeds");
-    std::vector<int> seeds(std::max<long>(1, total_seeds));
-    check(cudaMemcpyAsync(seeds.data(), d_seeds, sizeof(int) * seeds.size(), cudaMemcpyDeviceToHost, stream),
-          "download seeds");
+    check(cudaMemcpyAsync(seeds, d_seeds, sizeof(int) * std::max<long>(1, total_seeds), cudaMemcpyDeviceToHost,
+                          stream), "download seeds");
 
     // per level: bindings and neighbour lists of every template in one launch each
-    std::vector<std::vector<int32_t>> bind_nodes(max_levels), neighbours(max_levels);
-    std::vector<std::vector<double>> bind_weights(max_levels);
-    std::vector<std::vector<long>> edge_offsets(max_levels);
-    std::vector<std::vector<int>> takens(max_levels), supports(max_levels);
-    const long bind_entries = total_points * NRICP_MAX_SLOTS;
     int32_t* d_bind_nodes = nullptr;
     double* d_bind_weights = nullptr;
-    check(cudaMalloc(&d_bind_nodes, sizeof(int32_t) * std::max<long>(1, bind_entries)), "cudaMalloc(graph build)");
+    int* d_neigh = nullptr;
+    check(cudaMalloc(&d_bind_nodes, sizeof(int32_t) * bind_entries * max_levels), "cudaMalloc(graph build)");
     owned.push_back(d_bind_nodes);
-    check(cudaMalloc(&d_bind_weights, sizeof(double) * std::max<long>(1, bind_entries)), "cudaMalloc(graph build)");
+    check(cudaMalloc(&d_bind_weights, sizeof(double) * bind_entries * max_levels), "cudaMalloc(graph build)");
     owned.push_back(d_bind_weights);
+    check(cudaMalloc(&d_neigh, sizeof(int) * all_edges), "cudaMalloc(graph build)");
+    owned.push_back(d_neigh);
     std::vector<long> bind_offset(W);
     for (int t = 0; t < W; ++t) bind_offset[t] = point_offset[t] * NRICP_MAX_SLOTS;
     long* d_bind_offset = to_device(bind_offset, owned, stream);
     for (int l = 0; l < max_levels; ++l) {
-        std::vector<int> nodes(W, 0), support(W, 1), taken(W, 0);
-        std::vector<long> eoff(W, 0);
-        long edge_total = 0;
-        int max_nodes = 0;
-        for (int t = 0; t < W; ++t) {
-            const GraphRequest& r = requests[t];
-            if (l >= static_cast<int>(level_sizes[t].size())) continue;
-            nodes[t] = std::min(level_sizes[t][l], seed_count[t]);
-            support[t] = std::max(1, std::min({r.max_nodes, nodes[t], NRICP_MAX_SLOTS}));
-            taken[t] = nodes[t] > 1 && r.edge_neighbours > 0 ? std::min(r.edge_neighbours, nodes[t] - 1) : 0;
-            eoff[t] = edge_total;
-            edge_total += static_cast<long>(nodes[t]) * taken[t];
-            max_nodes = std::max(max_nodes, nodes[t]);
-        }
-        int* d_nodes = to_device(nodes, owned, stream);
-        int* d_support = to_device(support, owned, stream);
-        int* d_taken = to_device(taken, owned, stream);
-        long* d_eoff = to_device(eoff, owned, stream);
-        int* d_neigh = nullptr;
-        check(cudaMalloc(&d_neigh, sizeof(int) * std::max<long>(1, edge_total)), "cudaMalloc(graph build)");
-        owned.push_back(d_neigh);
+        const LevelPlan& p = plan[l];
+        int* d_nodes = to_device(p.nodes, owned, stream);
+        int* d_support = to_device(p.support, owned, stream);
+        int* d_taken = to_device(p.taken, owned, stream);
+        long* d_eoff = to_device(p.eoff, owned, stream);
+        int32_t* level_nodes = d_bind_nodes + bind_entries * l;
+        double* level_weights = d_bind_weights + bind_entries * l;
+        int* level_neigh = d_neigh + edge_base[l];
         k_bind<<<dim3(blocks(max_points, kBindThreads), W), kBindThreads, 0, stream>>>(
             d_points, d_point_offset, d_point_count, d_seeds, d_seed_offset, d_nodes, d_support,
-            d_bind_offset, d_bind_nodes, d_bind_weights);
+            d_bind_offset, level_nodes, level_weights);
         check(cudaGetLastError(), "bindings");
-        if (max_nodes > 0)
-            k_neighbours<<<dim3(blocks(max_nodes, kBindThreads), W), kBindThreads, 0, stream>>>(
-                d_points, d_point_offset, d_seeds, d_seed_offset, d_nodes, d_taken, d_eoff, d_neigh);
+        if (p.max_nodes > 0)
+            k_neighbours<<<dim3(blocks(p.max_nodes, kBindThreads), W), kBindThreads, 0, stream>>>(
+                d_points, d_point_offset, d_seeds, d_seed_offset, d_nodes, d_taken, d_eoff, level_neigh);
         check(cudaGetLastError(), "node edges");
-        bind_nodes[l].resize(std::max<long>(1, bind_entries));
-        bind_weights[l].resize(std::max<long>(1, bind_entries));
-        neighbours[l].resize(std::max<long>(1, edge_total));
-        check(cudaMemcpyAsync(bind_nodes[l].data(), d_bind_nodes, sizeof(int32_t) * bind_nodes[l].size(),
-                              cudaMemcpyDeviceToHost, stream), "download bindings");
-        check(cudaMemcpyAsync(bind_weights[l].data(), d_bind_weights, sizeof(double) * bind_weights[l].size(),
-                              cudaMemcpyDeviceToHost, stream), "download bindings");
-        check(cudaMemcpyAsync(neighbours[l].data(), d_neigh, sizeof(int) * neighbours[l].size(),
-                              cudaMemcpyDeviceToHost, stream), "download edges");
-        // the next level's bindings reuse the device buffer: wait for the copy
-        check(cudaStreamSynchronize(stream), "graph build");
-        edge_offsets[l] = eoff;
-        takens[l] = taken;
-        supports[l] = support;
+        check(cudaMemcpyAsync(host_nodes(l), level_nodes, sizeof(int32_t) * bind_entries, cudaMemcpyDeviceToHost,
+                              stream), "download bindings");
+        check(cudaMemcpyAsync(host_weights(l), level_weights, sizeof(double) * bind_entries, cudaMemcpyDeviceToHost,
+                              stream), "download bindings");
+        if (p.edge_total > 0)
+            check(cudaMemcpyAsync(host_neigh + edge_base[l], level_neigh, sizeof(int) * p.edge_total,
+                                  cudaMemcpyDeviceToHost, stream), "download edges");
     }
     check(cudaStreamSynchronize(stream), "graph build");
     for (void* p : owned) cudaFree(p);
 
-    // host: the graphs in the host build's form
+    // host: the graphs in the host build's form, one template per thread
+#pragma omp parallel for schedule(dynamic, 1) if (W > 1)
     for (int t = 0; t < W; ++t) {
         TemplateGraph& g = out[t];
         const int levels = static_cast<int>(level_sizes[t].size());
         for (int l = 0; l < levels; ++l) {
             GraphLevel level;
             const int n = std::min(level_sizes[t][l], seed_count[t]);
-            level.template_index.assign(seeds.begin() + seed_offset[t], seeds.begin() + seed_offset[t] + n);
+            level.template_index.assign(seeds + seed_offset[t], seeds + seed_offset[t] + n);
             level.rest.resize(static_cast<size_t>(n) * 3);
             for (int i = 0; i < n; ++i)
                 for (int k = 0; k < 3; ++k)
                     level.rest[i * 3 + k] = points[(point_offset[t] + level.template_index[i]) * 3 + k];
             level.bindings.resize(point_count[t]);
+            const int32_t* nodes = host_nodes(l);
+            const double* weights = host_weights(l);
             for (int v = 0; v < point_count[t]; ++v) {
                 Binding& b = level.bindings[v];
                 const long at = (point_offset[t] + v) * NRICP_MAX_SLOTS;
                 for (int s = 0; s < NRICP_MAX_SLOTS; ++s) {
-                    b.nodes[s] = bind_nodes[l][at + s];
-                    b.weights[s] = bind_weights[l][at + s];
+                    b.nodes[s] = nodes[at + s];
+                    b.weights[s] = weights[at + s];
                 }
-                b.count = supports[l][t];
+                b.count = plan[l].support[t];
             }
-            const int taken = takens[l][t];
+            const int taken = plan[l].taken[t];
+            const int* neigh = host_neigh + edge_base[l] + plan[l].eoff[t];
             std::vector<std::pair<int, int>> pairs;
             pairs.reserve(static_cast<size_t>(n) * taken);
             for (int i = 0; i < n; ++i)
                 for (int k = 0; k < taken; ++k) {
-                    const int o = neighbours[l][edge_offsets[l][t] + static_cast<long>(i) * taken + k];
+                    const int o = neigh[static_cast<long>(i) * taken + k];
                     pairs.emplace_back(std::min(i, o), std::max(i, o));
                 }
             std::sort(pairs.begin(), pairs.end());

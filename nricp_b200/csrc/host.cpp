@@ -385,6 +385,11 @@ LevelLayout build_layout(const TemplateGraph& graph, int level, int V) {
     // fused_assembly.cpp:68-79), grouped by (a, b)
     struct PairEntry { int a, b, code; };
     std::vector<PairEntry> entries;
+    {
+        size_t most = 0;
+        for (int v = 0; v < V; ++v) most += static_cast<size_t>(L.bind_counts[v]) * (L.bind_counts[v] - 1) / 2;
+        entries.reserve(most);
+    }
     for (int v = 0; v < V; ++v) {
         const int c = L.bind_counts[v];
         for (int x = 0; x < c; ++x)
@@ -397,9 +402,18 @@ LevelLayout build_layout(const TemplateGraph& graph, int level, int V) {
                                    v * 64 + (xf ? x : y) * 8 + (xf ? y : x)});
             }
     }
-    std::stable_sort(entries.begin(), entries.end(), [](const PairEntry& l, const PairEntry& r) {
-        return l.a != r.a ? l.a < r.a : l.b < r.b;
-    });
+    // stable order by (a, b): two stable counting passes, by b then by a
+    {
+        std::vector<PairEntry> by_b(entries.size());
+        std::vector<int64_t> start(N + 1, 0);
+        for (const PairEntry& e : entries) start[e.b + 1]++;
+        for (int n = 0; n < N; ++n) start[n + 1] += start[n];
+        for (const PairEntry& e : entries) by_b[start[e.b]++] = e;
+        std::fill(start.begin(), start.end(), 0);
+        for (const PairEntry& e : by_b) start[e.a + 1]++;
+        for (int n = 0; n < N; ++n) start[n + 1] += start[n];
+        for (const PairEntry& e : by_b) entries[start[e.a]++] = e;
+    }
     L.pair_begin.push_back(0);
     for (size_t i = 0; i < entries.size(); ++i) {
         if (i == 0 || entries[i].a != entries[i - 1].a || entries[i].b != entries[i - 1].b) {

@@ -27,6 +27,7 @@
 #include "graph_build.hpp"
 #include "kernels.cuh"
 #include "session.hpp"
+#include "staging.hpp"
 
 namespace nricp_b200 {
 
@@ -69,6 +70,7 @@ public:
     template <typename T>
     T* at(size_t offset) const { return reinterpret_cast<T*>(static_cast<char*>(base_) + offset); }
     size_t size() const { return size_; }
+    void* base() const { return base_; }
     void release() {
         if (base_) cudaFree(base_);
         base_ = nullptr;
@@ -103,6 +105,46 @@ void upload(T* dst, const std::vector<T>& src, cudaStream_t stream) {
     }
 }
 
+// Where a wrap's inputs go: straight to the device (a copy each, in stream
+// order), or into a host staging area laid out like the arena's input
+// prefix, which the caller then copies in one piece.
+struct InputSink {
+    cudaStream_t stream = nullptr;
+    char* staging = nullptr;       // host image of the arena's input prefix
+    const char* arena = nullptr;   // the arena's device base
+    template <typename T>
+    void put(T* dst, const std::vector<T>& src) const {
+        if (src.empty()) return;
+        if (staging) {
+            std::memcpy(staging + (reinterpret_cast<const char*>(dst) - arena), src.data(), sizeof(T) * src.size());
+        } else {
+            upload(dst, src, stream);
+        }
+    }
+};
+
+// Device memory of batches: a stream-ordered pool per device that keeps up
+// to 8 GB between batches, so that repeated batches allocate and free their
+// arenas without waiting for the device.
+cudaMemPool_t batch_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = 8ull << 30;
+    check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool");
+    pools[device] = pool;
+    return pool;
+}
+
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -125,6 +167,7 @@ struct Wrap {
     WrapControl initial_control{};   // pinned-free host copy used by reset
     double* identity_rot = nullptr;  // device (in the arena): identity rotations
     LevelRecord* initial_records = nullptr;  // and the level records a run starts from
+    size_t input_bytes = 0;          // the arena's prefix that holds the inputs
     ~Wrap() { arena.release(); }
 };
 
@@ -186,18 +229,22 @@ GraphRequest graph_request(const Wrap& w) {
                         d.edge_neighbours > 0 ? d.edge_neighbours : 4};
 }
 
-// The level layouts and size envelope of a wrap whose graph is built.
-void finish_host(Wrap& w) {
-    w.levels = static_cast<int>(w.graph.levels.size());
-    w.layouts.clear();
-    for (int l = 0; l < w.levels; ++l) {
-        w.layouts.push_back(build_layout(w.graph, l, w.V));
-        const LevelLayout& L = w.layouts.back();
+// The size envelope of a wrap whose layouts are built.
+void envelope(Wrap& w) {
+    for (const LevelLayout& L : w.layouts) {
         w.max_nodes = std::max(w.max_nodes, L.node_count);
         w.max_edges = std::max(w.max_edges, L.edge_count);
         w.max_pairs = std::max(w.max_pairs, L.pair_count);
         w.max_offdiag = std::max(w.max_offdiag, L.edge_count + L.pair_count);
     }
+}
+
+// The level layouts and size envelope of a wrap whose graph is built.
+void finish_host(Wrap& w) {
+    w.levels = static_cast<int>(w.graph.levels.size());
+    w.layouts.clear();
+    for (int l = 0; l < w.levels; ++l) w.layouts.push_back(build_layout(w.graph, l, w.V));
+    envelope(w);
 }
 
 // The host build: graph (bit-identical to the reference's) and layouts.
@@ -220,10 +267,15 @@ size_t bytes_of_layout(const LevelLayout& L) {
                               L.transfer_counts.size());
 }
 
-// Lays out, allocates and fills the wrap's device arena; builds the target's
-// hierarchy.  `control` is this wrap's slot in the batch's control array.
+// Lays out, allocates and fills the wrap's device arena: the inputs first
+// (template, target, level layouts, start state: the prefix of
+// w.input_bytes), then the hierarchy and the solver's state and scratch.
+// `control` is this wrap's slot in the batch's control array.  With
+// `staging`, the inputs are written there at their arena offsets and the
+// caller copies the prefix; otherwise each is copied on `stream`.  The
+// target's hierarchy is reset_device's.
 size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool plan_only = false,
-                      cudaMemPool_t pool = nullptr) {
+                      cudaMemPool_t pool = nullptr, char* staging = nullptr) {
     const NricpSolveDesc& d = w.desc;
     const int V = w.V, N = std::max(1, w.max_nodes), B = std::max(1, w.max_offdiag);
     Arena& a = w.arena;
@@ -241,11 +293,15 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_tgt = a.reserve(sizeof(double) * 3 * w.Vt);
     const size_t o_tgt_normals = a.reserve(sizeof(double) * 3 * w.Vt);
     const size_t o_tgt_faces = a.reserve(sizeof(int32_t) * 3 * w.F);
-    const size_t o_bvh_nodes = a.reserve(sizeof(float4) * 4 * std::max(1, w.F - 1));
-    const size_t o_bvh_leaves = a.reserve(sizeof(float4) * kLeafFloat4s * w.F);
     // levels
     std::vector<size_t> level_base(w.levels);
     for (int l = 0; l < w.levels; ++l) level_base[l] = a.reserve(bytes_of_layout(w.layouts[l]));
+    const size_t o_identity = a.reserve(sizeof(double) * 9 * N);
+    const size_t o_init_records = a.reserve(sizeof(LevelRecord) * w.levels);
+    w.input_bytes = a.size();
+    // the target's hierarchy
+    const size_t o_bvh_nodes = a.reserve(sizeof(float4) * 4 * std::max(1, w.F - 1));
+    const size_t o_bvh_leaves = a.reserve(sizeof(float4) * kLeafFloat4s * w.F);
     // state and scratch
     size_t o_rot[2], o_trans[2], o_diag[2], o_rhs[2], o_off[2];
     for (int i = 0; i < 2; ++i) {
@@ -283,8 +339,6 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_records = a.reserve(sizeof(LevelRecord) * w.levels);
     const size_t o_lstats = a.reserve(sizeof(CorrStats) * w.levels);
     const size_t o_fstats = a.reserve(sizeof(CorrStats));
-    const size_t o_identity = a.reserve(sizeof(double) * 9 * N);
-    const size_t o_init_records = a.reserve(sizeof(LevelRecord) * w.levels);
     if (plan_only) {  // the arena's size only, nothing allocated
         const size_t bytes = a.size();
         a = Arena();
@@ -295,6 +349,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     } else {
         a.allocate();
     }
+    const InputSink in{stream, staging, a.at<char>(0)};
     {
         // the state every run starts from: identity rotations, empty records
         std::vector<double> rot(static_cast<size_t>(N) * 9, 0.0);
@@ -307,8 +362,8 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
         }
         w.identity_rot = a.at<double>(o_identity);
         w.initial_records = a.at<LevelRecord>(o_init_records);
-        upload(w.identity_rot, rot, stream);
-        upload(w.initial_records, records, stream);
+        in.put(w.identity_rot, rot);
+        in.put(w.initial_records, records);
     }
 
     // ---- fill the descriptor ----
@@ -367,17 +422,17 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.bvh_nodes = a.at<float4>(o_bvh_nodes);
     D.bvh_leaves = a.at<float4>(o_bvh_leaves);
     D.rank_window = static_cast<float>(kRankWindow * target_diagonal(tgt));
-    upload(const_cast<double*>(D.tpl), tpl, stream);
-    upload(const_cast<int32_t*>(D.tpl_faces), w.template_faces, stream);
-    upload(const_cast<int32_t*>(D.vf_begin), vf_begin, stream);
-    upload(const_cast<int32_t*>(D.vf_faces), vf_list, stream);
-    if (D.mask) upload(const_cast<uint8_t*>(D.mask), w.mask, stream);
-    upload(const_cast<double*>(D.lm_target), lm_target, stream);
-    upload(const_cast<uint8_t*>(D.lm_flag), lm_flag, stream);
-    upload(const_cast<int32_t*>(D.lm_vertices), w.landmark_indices, stream);
-    upload(const_cast<double*>(D.tgt_points), tgt, stream);
-    upload(const_cast<double*>(D.tgt_normals), tgt_normals, stream);
-    upload(const_cast<int32_t*>(D.tgt_faces), w.target_faces, stream);
+    in.put(const_cast<double*>(D.tpl), tpl);
+    in.put(const_cast<int32_t*>(D.tpl_faces), w.template_faces);
+    in.put(const_cast<int32_t*>(D.vf_begin), vf_begin);
+    in.put(const_cast<int32_t*>(D.vf_faces), vf_list);
+    if (D.mask) in.put(const_cast<uint8_t*>(D.mask), w.mask);
+    in.put(const_cast<double*>(D.lm_target), lm_target);
+    in.put(const_cast<uint8_t*>(D.lm_flag), lm_flag);
+    in.put(const_cast<int32_t*>(D.lm_vertices), w.landmark_indices);
+    in.put(const_cast<double*>(D.tgt_points), tgt);
+    in.put(const_cast<double*>(D.tgt_normals), tgt_normals);
+    in.put(const_cast<int32_t*>(D.tgt_faces), w.target_faces);
 
     for (int l = 0; l < w.levels; ++l) {
         const LevelLayout& L = w.layouts[l];
@@ -387,7 +442,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
             using T = typename std::decay_t<decltype(vec)>::value_type;
             T* p = reinterpret_cast<T*>(base);
             base += (sizeof(T) * vec.size() + 255) & ~size_t(255);
-            upload(p, vec, stream);
+            in.put(p, vec);
             return p;
         };
         G.node_count = L.node_count;
@@ -503,6 +558,11 @@ Batch::Batch() {
 Batch::~Batch() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (pool_) {  // back to the pool in stream order, without a device-wide wait
+        for (auto& w : wraps_) w->arena.release_async(stream_);
+        if (lbvh_scratch_) cudaFreeAsync(lbvh_scratch_, stream_);
+        lbvh_scratch_ = nullptr;
+    }
     wraps_.clear();
     if (dev_wraps_) cudaFree(dev_wraps_);
     if (dev_controls_) cudaFree(dev_controls_);
@@ -571,16 +631,37 @@ void Batch::add_all(const NricpSolveDesc* descs, int count) {
         std::vector<TemplateGraph> graphs = device_template_graphs(requests, stream_);
         for (int i = 0; i < count; ++i) prepared[i]->graph = std::move(graphs[i]);
     }
-#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
-    for (int i = 0; i < count; ++i)
-        guarded_step(i, [&] {
-            if (device) {
-                finish_host(*prepared[i]);
-            } else {
-                prepare_host(*prepared[i]);
+    if (device) {
+        // the layouts: one task per (wrap, level), the largest first
+        std::vector<std::pair<int, int>> tasks;
+        for (int i = 0; i < count; ++i) {
+            Wrap& w = *prepared[i];
+            w.levels = static_cast<int>(w.graph.levels.size());
+            w.layouts.assign(w.levels, LevelLayout{});
+            for (int l = 0; l < w.levels; ++l) tasks.emplace_back(i, l);
+        }
+        auto work = [&](const std::pair<int, int>& t) {
+            return static_cast<long>(prepared[t.first]->V) * (t.second + 1);
+        };
+        std::stable_sort(tasks.begin(), tasks.end(), [&](const auto& x, const auto& y) { return work(x) > work(y); });
+        std::vector<std::string> failure(tasks.size());
+#pragma omp parallel for schedule(dynamic, 1) if (tasks.size() > 1)
+        for (long k = 0; k < static_cast<long>(tasks.size()); ++k) {
+            Wrap& w = *prepared[tasks[k].first];
+            try {
+                w.layouts[tasks[k].second] = build_layout(w.graph, tasks[k].second, w.V);
+            } catch (const std::exception& e) {
+                failure[k] = e.what();
             }
-        });
-    raise_first();
+        }
+        for (size_t k = 0; k < tasks.size(); ++k)
+            if (!failure[k].empty()) throw std::runtime_error(failure[k]);
+        for (auto& w : prepared) envelope(*w);
+    } else {
+#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
+        for (int i = 0; i < count; ++i) guarded_step(i, [&] { prepare_host(*prepared[i]); });
+        raise_first();
+    }
     const double spent = (now_seconds() - t0) / std::max(1, count);
     for (auto& w : prepared) {
         w->setup_seconds = spent;
@@ -590,33 +671,59 @@ void Batch::add_all(const NricpSolveDesc* descs, int count) {
 
 void Batch::upload_all(LbvhExport* lbvh_out) {
     const int W = static_cast<int>(wraps_.size());
+    const double t0 = now_seconds();
+    int device = 0;
+    check(cudaGetDevice(&device), "device");
+    pool_ = batch_pool(device);
     check(cudaMalloc(&dev_controls_, sizeof(WrapControl) * W), "cudaMalloc(controls)");
     check(cudaMallocHost(&host_controls_, sizeof(WrapControl) * W), "cudaMallocHost(controls)");
     size_t scratch_bytes = 0;
     for (const auto& w : wraps_) scratch_bytes = std::max(scratch_bytes, lbvh_scratch_bytes(w->F));
-    check(cudaMalloc(&lbvh_scratch_, scratch_bytes), "cudaMalloc(lbvh scratch)");
+    check(cudaMallocFromPoolAsync(&lbvh_scratch_, scratch_bytes, pool_, stream_), "cudaMallocFromPoolAsync(scratch)");
+    // every wrap's input prefix, staged side by side in page-locked memory
+    // on the host's cores, then one copy per wrap
+    std::vector<size_t> offset(W + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1) if (W > 1)
+    for (int i = 0; i < W; ++i) prepare_device(*wraps_[i], nullptr, nullptr, true);
+    for (int i = 0; i < W; ++i) offset[i + 1] = offset[i] + ((wraps_[i]->input_bytes + 255) & ~size_t(255));
+    StagingLease staging(offset[W]);
+    std::vector<std::string> failure(W);
+#pragma omp parallel for schedule(dynamic, 1) if (W > 1)
+    for (int i = 0; i < W; ++i) {
+        try {
+            check(cudaSetDevice(device), "cudaSetDevice");  // this host thread's current device
+            prepare_device(*wraps_[i], dev_controls_ + i, stream_, false, pool_, staging.data() + offset[i]);
+        } catch (const std::exception& e) {
+            failure[i] = e.what();
+        }
+    }
+    for (int i = 0; i < W; ++i)
+        if (!failure[i].empty()) throw std::runtime_error(failure[i]);
     shape_ = TickShape{};
     shape_.wraps = W;
     for (int i = 0; i < W; ++i) {
         Wrap& w = *wraps_[i];
-        const double t0 = now_seconds();
-        prepare_device(w, dev_controls_ + i, stream_);
+        check(cudaMemcpyAsync(w.arena.base(), staging.data() + offset[i], w.input_bytes, cudaMemcpyHostToDevice,
+                              stream_), "upload inputs");
+        g_transfers.h2d += w.input_bytes;
         reset_device(w, stream_, lbvh_scratch_, i == 0 ? lbvh_out : nullptr);
-        w.setup_seconds += now_seconds() - t0;
         shape_.max_vertices = std::max(shape_.max_vertices, w.V);
         shape_.max_nodes = std::max(shape_.max_nodes, w.max_nodes);
         shape_.max_edges = std::max(shape_.max_edges, w.max_edges);
         shape_.max_pairs = std::max(shape_.max_pairs, w.max_pairs);
     }
-    set_pcg_cluster(0);
+    set_pcg_cluster(default_pcg_cluster());
     check(cudaMalloc(&dev_wraps_, sizeof(WrapDev) * W), "cudaMalloc(wraps)");
     std::vector<WrapDev> host(W);
     for (int i = 0; i < W; ++i) host[i] = wraps_[i]->dev;
     check(cudaMemcpyAsync(dev_wraps_, host.data(), sizeof(WrapDev) * W, cudaMemcpyHostToDevice, stream_),
           "upload wraps");
-    check(cudaStreamSynchronize(stream_), "prepare");
+    check(cudaStreamSynchronize(stream_), "prepare");  // the staging lease ends after this
     const double t = now_seconds();
-    for (auto& w : wraps_) w->solve_started = t;
+    for (auto& w : wraps_) {
+        w->setup_seconds += (t - t0) / std::max(1, W);
+        w->solve_started = t;
+    }
 }
 
 void Batch::reset() {
@@ -648,6 +755,23 @@ bool Batch::all_done() const {
     for (size_t i = 0; i < wraps_.size(); ++i)
         if (host_controls_[i].phase != kPhaseDone) return false;
     return true;
+}
+
+// Per-wrap latency classes, halved until every class launch together needs
+// at most three CTAs per SM (-s for nricp_batch_tune).  On the 64 uneven
+// wraps of the benchmark that is one halving: the classes' CTAs then run in
+// under three rounds of the SMs, while a second halving lengthens every
+// solve iteration more than it saves.
+int Batch::default_pcg_cluster() const {
+    int device = 0, sms = 148;
+    check(cudaGetDevice(&device), "device");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device");
+    for (int shift = 0; shift < 4; ++shift) {
+        long ctas = 0;
+        for (const auto& w : wraps_) ctas += std::max(1, pcg_latency_cluster(w->max_nodes) >> shift);
+        if (ctas <= 3L * sms) return -shift;
+    }
+    return -4;
 }
 
 void Batch::set_pcg_cluster(int cluster) {
@@ -886,33 +1010,51 @@ std::vector<double> evaluate_host(const Wrap& w, const std::vector<double>& rot,
     return out;
 }
 
-// Result of one wrap in the caller's units (route_result_to_dict,
-// src/python/bindings.cpp:674-710), from its control `c` as last pulled.
-void write_result(const Wrap& w, const WrapControl& c, cudaStream_t stream, NricpResult* out) {
+// What a finished (or paused) wrap's result needs from the device.
+struct WrapDownload {
+    WrapControl control{};
+    std::vector<double> rot, trans;
+    std::vector<LevelRecord> records;
+    std::vector<CorrStats> lstats;
+    CorrStats fstats{};
+};
+
+WrapDownload download_result(const Wrap& w, const WrapControl& c, cudaStream_t stream) {
+    WrapDownload d;
+    d.control = c;
     const int level = std::min(c.level, w.levels - 1);
     const int N = w.layouts[level].node_count;
-    std::vector<double> rot(static_cast<size_t>(N) * 9), trans(static_cast<size_t>(N) * 3);
-    check(cudaMemcpyAsync(rot.data(), w.dev.rot[c.state], sizeof(double) * rot.size(),
+    d.rot.resize(static_cast<size_t>(N) * 9);
+    d.trans.resize(static_cast<size_t>(N) * 3);
+    d.records.resize(w.levels);
+    d.lstats.resize(w.levels);
+    check(cudaMemcpyAsync(d.rot.data(), w.dev.rot[c.state], sizeof(double) * d.rot.size(),
                           cudaMemcpyDeviceToHost, stream), "download rot");
-    check(cudaMemcpyAsync(trans.data(), w.dev.trans[c.state], sizeof(double) * trans.size(),
+    check(cudaMemcpyAsync(d.trans.data(), w.dev.trans[c.state], sizeof(double) * d.trans.size(),
                           cudaMemcpyDeviceToHost, stream), "download trans");
-    std::vector<LevelRecord> records(w.levels);
-    std::vector<CorrStats> lstats(w.levels);
-    CorrStats fstats;
-    check(cudaMemcpyAsync(records.data(), w.dev.records, sizeof(LevelRecord) * w.levels,
+    check(cudaMemcpyAsync(d.records.data(), w.dev.records, sizeof(LevelRecord) * w.levels,
                           cudaMemcpyDeviceToHost, stream), "download records");
-    check(cudaMemcpyAsync(lstats.data(), w.dev.level_stats, sizeof(CorrStats) * w.levels,
+    check(cudaMemcpyAsync(d.lstats.data(), w.dev.level_stats, sizeof(CorrStats) * w.levels,
                           cudaMemcpyDeviceToHost, stream), "download stats");
-    check(cudaMemcpyAsync(&fstats, w.dev.final_stats, sizeof(CorrStats), cudaMemcpyDeviceToHost,
+    check(cudaMemcpyAsync(&d.fstats, w.dev.final_stats, sizeof(CorrStats), cudaMemcpyDeviceToHost,
                           stream), "download stats");
     check(cudaStreamSynchronize(stream), "download");
-    g_transfers.d2h += sizeof(double) * (rot.size() + trans.size()) +
-                       sizeof(LevelRecord) * records.size() + sizeof(CorrStats) * (lstats.size() + 1) +
-                       sizeof(WrapControl);
-    const std::vector<double> vertices = evaluate_host(w, rot, trans, level);
+    g_transfers.d2h += sizeof(double) * (d.rot.size() + d.trans.size()) +
+                       sizeof(LevelRecord) * d.records.size() +
+                       sizeof(CorrStats) * (d.lstats.size() + 1) + sizeof(WrapControl);
+    return d;
+}
+
+// Result of one wrap in the caller's units (route_result_to_dict,
+// src/python/bindings.cpp:674-710), from its downloaded state; host only.
+void compose_result(const Wrap& w, const WrapDownload& d, NricpResult* out) {
+    const WrapControl& c = d.control;
+    const int level = std::min(c.level, w.levels - 1);
+    const int N = w.layouts[level].node_count;
+    const std::vector<double> vertices = evaluate_host(w, d.rot, d.trans, level);
     if (out->vertices) std::memcpy(out->vertices, vertices.data(), sizeof(double) * vertices.size());
-    if (out->rotations) std::memcpy(out->rotations, rot.data(), sizeof(double) * rot.size());
-    if (out->translations) std::memcpy(out->translations, trans.data(), sizeof(double) * trans.size());
+    if (out->rotations) std::memcpy(out->rotations, d.rot.data(), sizeof(double) * d.rot.size());
+    if (out->translations) std::memcpy(out->translations, d.trans.data(), sizeof(double) * d.trans.size());
     if (out->node_positions)
         std::memcpy(out->node_positions, w.layouts[level].rest.data(), sizeof(double) * 3 * N);
     if (out->level_nodes)
@@ -922,11 +1064,11 @@ void write_result(const Wrap& w, const WrapControl& c, cudaStream_t stream, Nric
     std::vector<LevelView> views;
     const int shown = c.phase == kPhaseDone || c.phase == kPhaseFinal ? w.levels : c.level + 1;
     for (int l = 0; l < shown && l < w.levels; ++l) {
-        const LevelRecord& r = records[l];
+        const LevelRecord& r = d.records[l];
         views.push_back({l, r.nodes, r.outer_iterations, r.inner_iterations, r.converged,
                          r.energy_start, r.energy_end, r.correspondence_mean});
     }
-    const CorrStats& s = c.phase == kPhaseDone ? fstats : lstats[std::max(0, c.level - 1)];
+    const CorrStats& s = c.phase == kPhaseDone ? d.fstats : d.lstats[std::max(0, c.level - 1)];
     const StatsView stats{s.total, s.accepted, s.rejected_distance, s.rejected_normal,
                           s.rejected_slope, s.rejected_masked, s.mean, s.p95, s.max};
     const std::string json = report_json(c.route == 0 ? "route_b" : "route_c", "float",
@@ -938,6 +1080,10 @@ void write_result(const Wrap& w, const WrapControl& c, cudaStream_t stream, Nric
         std::memcpy(out->report_json, json.data(), n);
         out->report_json[n] = 0;
     }
+}
+
+void write_result(const Wrap& w, const WrapControl& c, cudaStream_t stream, NricpResult* out) {
+    compose_result(w, download_result(w, c, stream), out);
 }
 
 }  // namespace
@@ -1022,6 +1168,7 @@ struct Server::Impl {
         double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;
         size_t bytes = 0;
         cudaEvent_t loaded = nullptr;  // the wrap's uploads and hierarchy are on the device
+        std::unique_ptr<WrapDownload> download;  // a finished wrap's state, for the finisher
         std::vector<double> vertices, rotations, translations, nodes;
         std::vector<int32_t> level_nodes;
         std::string report;
@@ -1030,7 +1177,7 @@ struct Server::Impl {
     // A retired wrap whose arena is freed once `after` (recorded on the tick
     // stream after its last use) has passed.
     struct Dead {
-        std::unique_ptr<Wrap> wrap;
+        Arena arena;
         size_t bytes = 0;
         cudaEvent_t after = nullptr;
     };
@@ -1038,36 +1185,50 @@ struct Server::Impl {
     NricpServerConfig cfg{};
     int device = 0, sms = 148;
     cudaStream_t stream = nullptr;       // ticks, placement, results
-    cudaStream_t load_stream = nullptr;  // allocation, uploads, hierarchy builds, frees
+    static constexpr int kLoaders = 4;
+    cudaStream_t load_streams[kLoaders] = {};  // allocation, uploads, hierarchy builds, frees
     cudaMemPool_t pool = nullptr;
     WrapDev* dev_wraps = nullptr;
     WrapControl* dev_controls = nullptr;
     WrapControl* host_controls = nullptr;
-    WrapControl* staging_control = nullptr;  // where a loading wrap's reset writes its control
+    WrapControl* staging_controls = nullptr;  // where each loader's reset writes its wrap's control
     std::vector<WrapDev> host_wraps;
     std::vector<RequestPtr> slot_req;    // the running request of each slot, or null
     std::vector<int> slot_nodes;
     int slots_used = 0;
     size_t resident = 0, peak = 0;
-    void* lbvh_scratch = nullptr;        // on load_stream, from the pool
-    size_t lbvh_bytes = 0;
+    void* lbvh_scratch[kLoaders] = {};   // each loader's, on its stream, from the pool
+    size_t lbvh_bytes[kLoaders] = {};
     TickShape shape{};                   // size envelope of every wrap placed so far
     std::map<int, cudaGraphExec_t> graphs;  // one tick graph per running-wrap count
+
+    // Per-class solve launches: class g (cluster size class_top >> g) reads
+    // its slots from row g of class_index, -1 past its members; the rows are
+    // rewritten whenever the running set changes.
+    int class_top = 0, class_count = 0;  // 0 classes: one uniform launch
+    int* class_index = nullptr;          // class_count x max_slots, device
+    std::vector<int> class_rows;         // what class_index holds now
+    cudaStream_t class_streams[5] = {};
+    cudaEvent_t class_fork = nullptr, class_join[5] = {};
 
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::map<long, RequestPtr> requests;
     std::deque<RequestPtr> prep_queue, ready, loaded;
     std::deque<Dead> graveyard;
+    std::deque<RequestPtr> finishing;
     long next_id = 1;
     int running = 0, loading = 0;
     bool stop = false;
     std::vector<std::thread> preppers;
-    std::thread pump_thread, loader_thread;
+    std::thread pump_thread, finisher_thread;
+    std::vector<std::thread> loader_threads;
     std::mutex cache_mu;
     std::map<uint64_t, std::shared_ptr<const TemplateEntry>> cache;
 
     long submitted = 0, completed = 0, failed = 0, ticks = 0, launches = 0, captures = 0;
+    double busy_seconds = 0.0;
+    cudaEvent_t tick_begin = nullptr, tick_end = nullptr;
     std::vector<double> latencies, queue_waits;
     double first_submit = -1.0, last_done = 0.0;
 
@@ -1148,11 +1309,12 @@ struct Server::Impl {
         return !ready.empty() && running + loading + static_cast<int>(loaded.size()) < cfg.max_slots;
     }
 
-    // One thread, its own stream: arenas from the pool, uploads, the target's
-    // hierarchy and the start state, in budget order; and the frees of
-    // retired arenas.  Nothing here waits for the tick stream.
-    void loader_loop() {
+    // Loader threads, each on its own stream: arenas from the pool, uploads,
+    // the target's hierarchy and the start state, in budget order; and the
+    // frees of retired arenas.  Nothing here waits for the tick stream.
+    void loader_loop(int k) {
         cudaSetDevice(device);
+        cudaStream_t load_stream = load_streams[k];
         while (true) {
             RequestPtr r;
             std::deque<Dead> dead;
@@ -1183,7 +1345,7 @@ struct Server::Impl {
             size_t freed = 0;
             for (Dead& d : dead) {
                 cudaStreamWaitEvent(load_stream, d.after, 0);
-                d.wrap->arena.release_async(load_stream);
+                d.arena.release_async(load_stream);
                 cudaEventDestroy(d.after);
                 freed += d.bytes;
             }
@@ -1196,15 +1358,15 @@ struct Server::Impl {
             std::string why;
             try {
                 Wrap& w = *r->wrap;
-                prepare_device(w, staging_control, load_stream, false, pool);
+                prepare_device(w, staging_controls + k, load_stream, false, pool);
                 const size_t need = lbvh_scratch_bytes(w.F);
-                if (need > lbvh_bytes) {
-                    if (lbvh_scratch) check(cudaFreeAsync(lbvh_scratch, load_stream), "scratch");
-                    lbvh_scratch = nullptr;
-                    check(cudaMallocFromPoolAsync(&lbvh_scratch, need, pool, load_stream), "scratch");
-                    lbvh_bytes = need;
+                if (need > lbvh_bytes[k]) {
+                    if (lbvh_scratch[k]) check(cudaFreeAsync(lbvh_scratch[k], load_stream), "scratch");
+                    lbvh_scratch[k] = nullptr;
+                    check(cudaMallocFromPoolAsync(&lbvh_scratch[k], need, pool, load_stream), "scratch");
+                    lbvh_bytes[k] = need;
                 }
-                reset_device(w, load_stream, lbvh_scratch, nullptr);
+                reset_device(w, load_stream, lbvh_scratch[k], nullptr);
                 check(cudaEventCreateWithFlags(&r->loaded, cudaEventDisableTiming), "event");
                 check(cudaEventRecord(r->loaded, load_stream), "event");
             } catch (const std::exception& e) {
@@ -1243,12 +1405,29 @@ struct Server::Impl {
         TickShape t = shape;
         t.wraps = count;
         t.pcg_groups = 0;
-        const int cluster = cfg.pcg_cluster > 0 ? cfg.pcg_cluster
-                                                : pcg_cluster_size(t.max_nodes, count, sms);
         pcg_cluster_size(t.max_nodes, count, sms);  // enables the launch attributes
-        t.pcg_cluster = cluster;
-        std::vector<int> nodes(count, t.max_nodes);  // any wrap may take any slot
-        t.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), count, cluster);
+        if (class_count == 0) {
+            t.pcg_cluster = cfg.pcg_cluster;
+            std::vector<int> nodes(count, t.max_nodes);  // any wrap may take any slot
+            t.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), count, t.pcg_cluster);
+        } else {
+            // every class launch covers `count` entries; a class's shared
+            // memory is what its largest possible member would use
+            for (int g = 0; g < class_count; ++g) {
+                const int cluster = class_top >> g;
+                const int nodes = std::min(t.max_nodes, class_node_bound(cluster));
+                t.pcg_group_cluster[g] = cluster;
+                t.pcg_group_count[g] = count;
+                t.pcg_group_shared[g] = pcg_shared_bytes(&nodes, 1, cluster);
+                t.pcg_group_index[g] = class_index + static_cast<size_t>(g) * cfg.max_slots;
+                t.pcg_streams[g] = class_streams[g];
+                t.pcg_join[g] = class_join[g];
+            }
+            t.pcg_fork = class_fork;
+            t.pcg_groups = class_count;
+            t.pcg_cluster = class_top;
+            t.pcg_shared_bytes = t.pcg_group_shared[0];
+        }
         cudaGraph_t g = nullptr;
         cudaGraphExec_t exec = nullptr;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
@@ -1262,6 +1441,43 @@ struct Server::Impl {
         return exec;
     }
     std::map<int, int> launches_per_tick;
+
+    // A wrap's class is its latency cluster halved `shift` times: a fixed
+    // shift (pcg_cluster < 0), or by load (0) -- none while the running
+    // wraps' latency clusters fit three CTAs per SM, else one.
+    int max_shift() const { return cfg.pcg_cluster < 0 ? -cfg.pcg_cluster : 1; }
+    int shift_for(int count) const {
+        if (cfg.pcg_cluster < 0) return -cfg.pcg_cluster;
+        long ctas = 0;
+        for (int i = 0; i < count; ++i) ctas += pcg_latency_cluster(slot_nodes[i]);
+        return ctas <= 3L * sms ? 0 : 1;
+    }
+    static int class_of(int nodes, int shift) { return std::max(1, pcg_latency_cluster(nodes) >> shift); }
+    // The most nodes a wrap of class `cluster` can have: its latency cluster
+    // is at most cluster << max_shift, which covers up to 128 nodes per CTA
+    // below 16.
+    int class_node_bound(int cluster) const {
+        const int latency = cluster << max_shift();
+        return latency >= 16 ? pcg_max_nodes() : latency * 128;
+    }
+
+    // Rewrites the class rows for the running wraps in slots 0 .. count-1
+    // (tick stream order: the next tick reads them).
+    void upload_classes(int count) {
+        if (class_count == 0) return;
+        std::vector<int> rows(static_cast<size_t>(class_count) * cfg.max_slots, -1);
+        std::vector<int> fill(class_count, 0);
+        const int shift = shift_for(count);
+        for (int i = 0; i < count; ++i) {
+            int g = 0;
+            while ((class_top >> g) > class_of(slot_nodes[i], shift)) ++g;
+            rows[static_cast<size_t>(g) * cfg.max_slots + fill[g]++] = i;
+        }
+        if (rows == class_rows) return;
+        class_rows = rows;
+        check(cudaMemcpyAsync(class_index, class_rows.data(), sizeof(int) * class_rows.size(),
+                              cudaMemcpyHostToDevice, stream), "solve classes");
+    }
 
     // Moves the running wrap of slot `from` into the free slot `to`: its
     // control block (device to device) and its descriptor.
@@ -1280,9 +1496,15 @@ struct Server::Impl {
         slot_req[from] = nullptr;
     }
 
+    // Downloads a finished wrap's result buffers (tick thread); the host
+    // work -- vertices in FP64, the report -- is the finisher's.
     void retire(int slot, const RequestPtr& r) {
+        r->wrap->solve_seconds = now_seconds() - r->t_admit;
+        r->download = std::make_unique<WrapDownload>(download_result(*r->wrap, host_controls[slot], stream));
+    }
+
+    void compose(const RequestPtr& r) {
         Wrap& w = *r->wrap;
-        const WrapControl& c = host_controls[slot];
         const int N = w.layouts.back().node_count;
         r->vertices.assign(static_cast<size_t>(w.V) * 3, 0.0);
         r->rotations.assign(static_cast<size_t>(N) * 9, 0.0);
@@ -1292,9 +1514,40 @@ struct Server::Impl {
         std::vector<char> report(1 << 20);
         NricpResult out{r->vertices.data(), r->rotations.data(), r->translations.data(),
                         r->nodes.data(), r->level_nodes.data(), report.data(), report.size(), 0};
-        w.solve_seconds = now_seconds() - r->t_admit;
-        write_result(w, c, stream, &out);
+        compose_result(w, *r->download, &out);
         r->report.assign(report.data(), std::min(out.report_length, report.size() - 1));
+    }
+
+    void finish_loop() {
+        while (true) {
+            RequestPtr r;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stop || !finishing.empty(); });
+                if (stop) return;
+                r = finishing.front();
+                finishing.pop_front();
+            }
+            std::string why;
+            try {
+                compose(r);
+            } catch (const std::exception& e) {
+                why = e.what();
+            }
+            r->download.reset();
+            r->wrap.reset();  // host side; the arena went back to the pool at retirement
+            std::lock_guard<std::mutex> lk(mu);
+            if (!why.empty()) {
+                fail(r, why, false);
+                continue;
+            }
+            r->state = NRICP_REQUEST_DONE;
+            r->t_done = now_seconds();
+            latencies.push_back(r->t_done - r->t_submit);
+            last_done = std::max(last_done, r->t_done);
+            completed += 1;
+            cv_done.notify_all();
+        }
     }
 
     // Hands a retired wrap's arena to the loader.  A finished wrap's tick
@@ -1304,7 +1557,8 @@ struct Server::Impl {
     void bury(const RequestPtr& r) {
         Dead d;
         d.bytes = r->bytes;
-        d.wrap = std::move(r->wrap);
+        d.arena = r->wrap->arena;  // the device arena leaves; the host side stays for the finisher
+        r->wrap->arena = Arena();
         check(cudaEventCreateWithFlags(&d.after, cudaEventDisableTiming), "event");
         check(cudaEventRecord(d.after, stream), "event");
         std::lock_guard<std::mutex> lk(mu);
@@ -1355,8 +1609,11 @@ struct Server::Impl {
                     grow_shape(w);
                 }
                 count = running_snapshot();
+                upload_classes(count);
                 cudaGraphExec_t g = graph_for(count);
+                check(cudaEventRecord(tick_begin, stream), "event");
                 for (int i = 0; i < per_poll; ++i) check(cudaGraphLaunch(g, stream), "graph launch");
+                check(cudaEventRecord(tick_end, stream), "event");
                 check(cudaMemcpyAsync(host_controls, dev_controls, sizeof(WrapControl) * count,
                                       cudaMemcpyDeviceToHost, stream), "pull controls");
                 check(cudaStreamSynchronize(stream), "tick");
@@ -1373,8 +1630,11 @@ struct Server::Impl {
                 cv_work.notify_all();
                 return;
             }
+            float tick_ms = 0.0f;
+            cudaEventElapsedTime(&tick_ms, tick_begin, tick_end);
             ticks += per_poll;
             launches += (long)per_poll * launches_per_tick[count];
+            busy_seconds += 1e-3 * tick_ms;
             std::vector<int> holes;
             for (int i = 0; i < count; ++i) {
                 RequestPtr r = slot_req[i];
@@ -1395,15 +1655,11 @@ struct Server::Impl {
                 slot_req[i] = nullptr;
                 running -= 1;
                 if (!why.empty()) {
+                    r->wrap.reset();
                     fail(r, why, false);
                     continue;
                 }
-                r->state = NRICP_REQUEST_DONE;
-                r->t_done = now_seconds();
-                latencies.push_back(r->t_done - r->t_submit);
-                last_done = std::max(last_done, r->t_done);
-                completed += 1;
-                cv_done.notify_all();
+                finishing.push_back(r);
                 cv_work.notify_all();
             }
             // keep the running wraps in slots 0 .. running-1: the last running
@@ -1442,9 +1698,9 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     m.cfg = config;
     if (m.cfg.max_slots <= 0 || m.cfg.max_slots > 1024)
         throw InvalidArgument("max_slots is " + std::to_string(m.cfg.max_slots) + "; it must be 1 to 1024");
-    if (m.cfg.pcg_cluster != 0 && (m.cfg.pcg_cluster < 0 || m.cfg.pcg_cluster > 16 ||
-                                  (m.cfg.pcg_cluster & (m.cfg.pcg_cluster - 1)) != 0))
+    if (m.cfg.pcg_cluster > 0 && (m.cfg.pcg_cluster > 16 || (m.cfg.pcg_cluster & (m.cfg.pcg_cluster - 1)) != 0))
         throw InvalidArgument("the solve's cluster size is a power of two from 1 to 16");
+    if (m.cfg.pcg_cluster < -4) throw InvalidArgument("the solve's class shift is 0 to 4");
     check(cudaGetDevice(&m.device), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&m.sms, cudaDevAttrMultiProcessorCount, m.device), "device");
     if (m.cfg.memory_budget_bytes == 0) {
@@ -1453,7 +1709,8 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
         m.cfg.memory_budget_bytes = free_bytes / 10 * 9;
     }
     check(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    check(cudaStreamCreateWithFlags(&m.load_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int k = 0; k < Impl::kLoaders; ++k)
+        check(cudaStreamCreateWithFlags(&m.load_streams[k], cudaStreamNonBlocking), "cudaStreamCreate");
     {
         cudaMemPoolProps props = {};
         props.allocType = cudaMemAllocationTypePinned;
@@ -1463,7 +1720,21 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
         uint64_t keep = UINT64_MAX;  // keep freed arenas for the next requests
         check(cudaMemPoolSetAttribute(m.pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool");
     }
-    check(cudaMalloc(&m.staging_control, sizeof(WrapControl)), "cudaMalloc(staging control)");
+    check(cudaMalloc(&m.staging_controls, sizeof(WrapControl) * Impl::kLoaders), "cudaMalloc(staging control)");
+    check(cudaEventCreate(&m.tick_begin), "event");
+    check(cudaEventCreate(&m.tick_end), "event");
+    if (m.cfg.pcg_cluster <= 0) {
+        m.class_top = m.cfg.pcg_cluster < 0 ? std::max(1, 16 >> m.max_shift()) : 16;
+        for (int c = m.class_top; c >= 1; c /= 2) m.class_count += 1;
+        check(cudaMalloc(&m.class_index, sizeof(int) * m.class_count * m.cfg.max_slots), "cudaMalloc(classes)");
+        check(cudaMemset(m.class_index, 0xff, sizeof(int) * m.class_count * m.cfg.max_slots), "classes");
+        m.class_rows.assign(static_cast<size_t>(m.class_count) * m.cfg.max_slots, -1);
+        for (int g = 1; g < m.class_count; ++g) {
+            check(cudaStreamCreateWithFlags(&m.class_streams[g], cudaStreamNonBlocking), "stream");
+            check(cudaEventCreateWithFlags(&m.class_join[g], cudaEventDisableTiming), "event");
+        }
+        check(cudaEventCreateWithFlags(&m.class_fork, cudaEventDisableTiming), "event");
+    }
     check(cudaMalloc(&m.dev_wraps, sizeof(WrapDev) * m.cfg.max_slots), "cudaMalloc(slots)");
     check(cudaMalloc(&m.dev_controls, sizeof(WrapControl) * m.cfg.max_slots), "cudaMalloc(controls)");
     check(cudaMallocHost(&m.host_controls, sizeof(WrapControl) * m.cfg.max_slots), "cudaMallocHost(controls)");
@@ -1473,7 +1744,8 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     int threads = m.cfg.prep_threads;
     if (threads <= 0) threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / 2);
     for (int i = 0; i < threads; ++i) m.preppers.emplace_back([&m] { m.prep_loop(); });
-    m.loader_thread = std::thread([&m] { m.loader_loop(); });
+    for (int k = 0; k < Impl::kLoaders; ++k) m.loader_threads.emplace_back([&m, k] { m.loader_loop(k); });
+    m.finisher_thread = std::thread([&m] { m.finish_loop(); });
     m.pump_thread = std::thread([&m] { m.pump_loop(); });
 }
 
@@ -1487,10 +1759,12 @@ Server::~Server() {
     m.cv_done.notify_all();
     for (auto& t : m.preppers) t.join();
     if (m.pump_thread.joinable()) m.pump_thread.join();
-    if (m.loader_thread.joinable()) m.loader_thread.join();
+    for (auto& t : m.loader_threads) t.join();
+    if (m.finisher_thread.joinable()) m.finisher_thread.join();
+    m.finishing.clear();
     cudaSetDevice(m.device);
     cudaStreamSynchronize(m.stream);
-    cudaStreamSynchronize(m.load_stream);
+    for (int k = 0; k < Impl::kLoaders; ++k) cudaStreamSynchronize(m.load_streams[k]);
     for (auto& [count, g] : m.graphs) cudaGraphExecDestroy(g);
     for (auto& r : m.loaded)
         if (r->loaded) cudaEventDestroy(r->loaded);
@@ -1501,13 +1775,22 @@ Server::~Server() {
     m.ready.clear();
     m.loaded.clear();
     m.prep_queue.clear();
-    if (m.lbvh_scratch) cudaFree(m.lbvh_scratch);
-    if (m.staging_control) cudaFree(m.staging_control);
+    for (int k = 0; k < Impl::kLoaders; ++k)
+        if (m.lbvh_scratch[k]) cudaFree(m.lbvh_scratch[k]);
+    if (m.staging_controls) cudaFree(m.staging_controls);
+    if (m.class_index) cudaFree(m.class_index);
+    for (int g = 1; g < 5; ++g) {
+        if (m.class_streams[g]) cudaStreamDestroy(m.class_streams[g]);
+        if (m.class_join[g]) cudaEventDestroy(m.class_join[g]);
+    }
+    if (m.class_fork) cudaEventDestroy(m.class_fork);
+    if (m.tick_begin) cudaEventDestroy(m.tick_begin);
+    if (m.tick_end) cudaEventDestroy(m.tick_end);
     if (m.dev_wraps) cudaFree(m.dev_wraps);
     if (m.dev_controls) cudaFree(m.dev_controls);
     if (m.host_controls) cudaFreeHost(m.host_controls);
     cudaStreamDestroy(m.stream);
-    cudaStreamDestroy(m.load_stream);
+    for (int k = 0; k < Impl::kLoaders; ++k) cudaStreamDestroy(m.load_streams[k]);
     if (m.pool) cudaMemPoolDestroy(m.pool);
 }
 
@@ -1605,6 +1888,7 @@ NricpServerStats Server::stats() {
     s.ticks = m.ticks;
     s.launches = m.launches;
     s.captures = m.captures;
+    s.busy_seconds = m.busy_seconds;
     s.resident_bytes = m.resident;
     s.peak_resident_bytes = m.peak;
     s.slots_used = m.slots_used;

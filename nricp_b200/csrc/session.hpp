@@ -71,6 +71,7 @@ public:
     // per size class, the classes in parallel; -s: the same classes halved s
     // times.  Every choice gives bit-identical results.
     void set_pcg_cluster(int cluster);
+    int default_pcg_cluster() const;
     void pull_controls();
     bool all_done() const;
     void finish();
@@ -99,6 +100,7 @@ private:
     WrapDev* dev_wraps_ = nullptr;
     WrapControl* dev_controls_ = nullptr;
     void* lbvh_scratch_ = nullptr;  // hierarchy build scratch, shared by the wraps' builds
+    cudaMemPool_t pool_ = nullptr;  // the arenas' and the scratch's (batch_pool)
     int* pcg_index_ = nullptr;      // wraps ordered by solve class (device)
     cudaStream_t pcg_streams_[5] = {};
     cudaEvent_t pcg_join_[5] = {};

@@ -705,7 +705,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
                                                      const int* __restrict__ index,
                                                      int budget_floats) {
     cg::cluster_group cluster = cg::this_cluster();
-    const WrapDev& w = wraps[index ? index[blockIdx.y] : blockIdx.y];
+    const int slot = index ? index[blockIdx.y] : (int)blockIdx.y;
+    if (slot < 0) return;  // an empty entry of a class launch; uniform across the cluster
+    const WrapDev& w = wraps[slot];
     const WrapControl c = *w.control;
     if (c.phase != kPhaseSolve) return;  // uniform across the cluster
     const LevelDev& L = w.levels[c.level];
@@ -1067,7 +1069,7 @@ __device__ inline F3 node_offset32(const WrapDev& w, const LevelDev& L, int node
     return mul3f(w.rot32 + node * 9, {(float)p.x, (float)p.y, (float)p.z});
 }
 
-__global__ void __launch_bounds__(kNodeThreads) k_node_assemble(const WrapDev* __restrict__ wraps) {
+__global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
     if (!computes_energy(c)) return;
@@ -1206,7 +1208,7 @@ __device__ inline void store_block_pair(float* out, const LevelDev& L, int k, co
 
 // Warp per node pair: lanes stride over the vertices the two nodes share,
 // each lane keeps a 6x6 block in registers, one butterfly reduction.
-__global__ void __launch_bounds__(kNodeThreads) k_pair_assemble(const WrapDev* __restrict__ wraps) {
+__global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
     if (!assembles(c)) return;

@@ -115,9 +115,10 @@ class WrapBatch:
 
     def tune(self, pcg_cluster: int = 0) -> int:
         """Cluster size of the linear solve: a power of two up to 16 for every
-        wrap, 0 (default) for each wrap's own size in per-class launches, -s
-        for those sizes halved s times.  Returns the largest size in effect;
-        results are bit-identical for every choice."""
+        wrap, 0 for each wrap's own size in per-class launches, -s for those
+        sizes halved s times (a new batch starts at the smallest s whose
+        classes need at most three CTAs per SM).  Returns the largest size in
+        effect; results are bit-identical for every choice."""
         out = C.c_int()
         check(load().nricp_batch_tune(self._handle, int(pcg_cluster), C.byref(out)))
         return out.value

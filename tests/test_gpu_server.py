@@ -36,12 +36,14 @@ def _same(a, b):
     assert ja["correspondence"] == jb["correspondence"]
 
 
-@pytest.mark.parametrize("route", ["route_b", "route_c"])
-def test_served_results_equal_the_wraps_solved_alone(dp, device, route):
+# pcg_cluster: 0 latency classes halved by load (the default), -1 always
+# halved once, 4 one cluster size for every slot
+@pytest.mark.parametrize("route,cluster", [("route_b", 0), ("route_c", 0), ("route_b", -1), ("route_b", 4)])
+def test_served_results_equal_the_wraps_solved_alone(dp, device, route, cluster):
     cases = _cases()
     solve = dp.solve_route_b if route == "route_b" else dp.solve_route_c
     alone = [solve(*c.args(), **c.options) for c in cases]
-    with dp.WrapServer(max_slots=8) as server:
+    with dp.WrapServer(max_slots=8, pcg_cluster=cluster) as server:
         ids = [server.submit(*cases[0].args(), route=route, **cases[0].options),
                server.submit(*cases[1].args(), route=route, **cases[1].options)]
         # later arrivals join while the first ones are running
