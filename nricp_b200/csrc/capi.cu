@@ -337,7 +337,7 @@ int nricp_batch_solve(const NricpSolveDesc* descs, int count, NricpResult* resul
         batch.add_all(descs, count);
         batch.upload_all();
         batch.run();
-        for (int i = 0; i < count; ++i) batch.result(i, &results[i]);
+        batch.results(results);
     });
 }
 

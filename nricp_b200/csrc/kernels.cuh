@@ -21,7 +21,11 @@ size_t lbvh_scratch_bytes(int triangle_count);
 uint32_t lbvh_build(const double* points, const int32_t* faces, int triangle_count,
                     void* scratch, float4* nodes, float4* leaves, cudaStream_t stream,
                     LbvhExport* out);
-void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaStream_t stream);
+// The closest-point query of every querying wrap: with `counter` (a device
+// int), one queue of vertices over a grid that fits on the device at once;
+// without, a block row per wrap.
+void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaStream_t stream,
+                  int* counter = nullptr);
 void launch_closest_points(const WrapDev* wrap, const double* queries, int count, double* points,
                            double* normals, double* distances, int32_t* triangles, int* overflow,
                            cudaStream_t stream);
@@ -47,6 +51,7 @@ struct TickShape {
     const int* pcg_group_index[5];       // device: wrap indices of the group
     cudaStream_t pcg_streams[5];         // branch streams (index 0 unused)
     cudaEvent_t pcg_fork, pcg_join[5];
+    int* query_counter;                  // device: the query queue's next item (null: no queue)
 };
 
 // Device timing hooks for the dominant kernels (CUDA events on the launching

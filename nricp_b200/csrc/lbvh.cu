@@ -598,15 +598,14 @@ __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* o
     return best_tri;
 }
 
-// One correspondence per template vertex, with the filters in the order the
+__device__ inline bool queries(int phase) {
+    return phase == kPhaseTransfer || phase == kPhaseRefresh || phase == kPhaseFinal;
+}
+
+// The correspondence of template vertex v, with the filters in the order the
 // reference applies them (correspondence.cpp:35-80) and the reweighting of
 // route_a.cpp:19-38.
-__global__ void k_query(const WrapDev* __restrict__ wraps) {
-    const WrapDev& w = wraps[blockIdx.y];
-    const WrapControl c = *w.control;
-    if (!(c.phase == kPhaseTransfer || c.phase == kPhaseRefresh || c.phase == kPhaseFinal)) return;
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= w.V) return;
+__device__ void query_vertex(const WrapDev& w, int level, int v) {
     uint8_t code = 0;
     D3 point = {0, 0, 0}, normal = {0, 0, 0};
     double distance = 0.0, robust = 1.0;
@@ -643,8 +642,8 @@ __global__ void k_query(const WrapDev* __restrict__ wraps) {
             if (code == 0) {
                 const D3 o = vsub(q, point);
                 const double squared = vdot(o, o);
-                const double threshold = w.robust_threshold[c.level];
-                robust = threshold > 0.0 ? robust_weight(w.robust_kernel[c.level], squared, threshold) : 1.0;
+                const double threshold = w.robust_threshold[level];
+                robust = threshold > 0.0 ? robust_weight(w.robust_kernel[level], squared, threshold) : 1.0;
             }
         } else {
             code = 1;
@@ -656,6 +655,61 @@ __global__ void k_query(const WrapDev* __restrict__ wraps) {
     w.corr_triangle[v] = tri;
     w.corr_code[v] = code;
     w.robust[v] = robust;
+}
+
+// Thread per vertex, block row per wrap.
+__global__ void k_query(const WrapDev* __restrict__ wraps) {
+    const WrapDev& w = wraps[blockIdx.y];
+    const WrapControl c = *w.control;
+    if (!queries(c.phase)) return;
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= w.V) return;
+    query_vertex(w, c.level, v);
+}
+
+// The same work as one queue: the vertices of every querying wrap, in wrap
+// then vertex order, handed out 32 at a time to whichever warp is free.  A
+// walk's length varies a lot from vertex to vertex, so fixed blocks hold an
+// SM until their slowest warp ends; here a warp that ends takes the next 32.
+// The grid is what fits on the device at once; `counter` starts at 0.
+__global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__ wraps, int wrap_count,
+                                                    int* __restrict__ counter) {
+    extern __shared__ int first[];  // wrap_count + 1: each querying wrap's first item
+    for (int i = threadIdx.x; i < wrap_count; i += blockDim.x)
+        first[i + 1] = queries(wraps[i].control->phase) ? wraps[i].V : 0;
+    __syncthreads();
+    if (threadIdx.x < 32) {  // inclusive scan by warp 0, 32 wraps at a time
+        const int lane = threadIdx.x;
+        int carry = 0;
+        for (int base = 0; base < wrap_count; base += 32) {
+            int x = base + lane < wrap_count ? first[base + lane + 1] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (base + lane < wrap_count) first[base + lane + 1] = carry + x;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) first[0] = 0;
+    }
+    __syncthreads();
+    const int total = first[wrap_count];
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const int item = base + lane;
+        if (item >= total) continue;
+        int lo = 0, hi = wrap_count - 1;  // the last wrap whose first item is <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first[mid] <= item) lo = mid; else hi = mid - 1;
+        }
+        const WrapDev& w = wraps[lo];
+        query_vertex(w, w.control->level, item - first[lo]);
+    }
 }
 
 // Stand-alone query over a prepared hierarchy (parity tests and the
@@ -691,9 +745,23 @@ __global__ void k_closest_points(const WrapDev* __restrict__ wraps, const double
     out_triangles[i] = tri;
 }
 
-void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaStream_t stream) {
-    dim3 grid(blocks_for(max_vertices, 128), wrap_count);
-    k_query<<<grid, 128, 0, stream>>>(wraps);
+void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaStream_t stream, int* counter) {
+    if (!counter) {
+        dim3 grid(blocks_for(max_vertices, 128), wrap_count);
+        k_query<<<grid, 128, 0, stream>>>(wraps);
+        return;
+    }
+    static int resident = 0;  // blocks of the queue that fit on the device at once
+    if (resident == 0) {
+        int device = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_queue, 128, sizeof(int) * 1025);
+        resident = sms * (per_sm > 0 ? per_sm : 1);
+        if (resident <= 0) resident = 1;
+    }
+    cudaMemsetAsync(counter, 0, sizeof(int), stream);
+    k_query_queue<<<resident, 128, sizeof(int) * (wrap_count + 1), stream>>>(wraps, wrap_count, counter);
 }
 
 void launch_closest_points(const WrapDev* wrap, const double* queries, int count,

@@ -564,6 +564,7 @@ Batch::~Batch() {
         lbvh_scratch_ = nullptr;
     }
     wraps_.clear();
+    if (query_counter_) cudaFree(query_counter_);
     if (dev_wraps_) cudaFree(dev_wraps_);
     if (dev_controls_) cudaFree(dev_controls_);
     if (lbvh_scratch_) cudaFree(lbvh_scratch_);
@@ -701,6 +702,8 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
         if (!failure[i].empty()) throw std::runtime_error(failure[i]);
     shape_ = TickShape{};
     shape_.wraps = W;
+    check(cudaMalloc(&query_counter_, sizeof(int)), "cudaMalloc(query queue)");
+    shape_.query_counter = query_counter_;
     for (int i = 0; i < W; ++i) {
         Wrap& w = *wraps_[i];
         check(cudaMemcpyAsync(w.arena.base(), staging.data() + offset[i], w.input_bytes, cudaMemcpyHostToDevice,
@@ -1090,6 +1093,25 @@ void write_result(const Wrap& w, const WrapControl& c, cudaStream_t stream, Nric
 
 void Batch::result(int i, NricpResult* out) { write_result(*wraps_[i], host_controls_[i], stream_, out); }
 
+void Batch::results(NricpResult* outs) {
+    const int W = static_cast<int>(wraps_.size());
+    std::vector<WrapDownload> downloads;
+    downloads.reserve(W);
+    for (int i = 0; i < W; ++i) downloads.push_back(download_result(*wraps_[i], host_controls_[i], stream_));
+    // vertices in FP64 and the reports, on the host's cores
+    std::vector<std::string> failure(W);
+#pragma omp parallel for schedule(dynamic, 1) if (W > 1)
+    for (int i = 0; i < W; ++i) {
+        try {
+            compose_result(*wraps_[i], downloads[i], &outs[i]);
+        } catch (const std::exception& e) {
+            failure[i] = e.what();
+        }
+    }
+    for (int i = 0; i < W; ++i)
+        if (!failure[i].empty()) throw std::runtime_error(failure[i]);
+}
+
 std::vector<double> Batch::evaluate_host(int i, const std::vector<double>& rot,
                                          const std::vector<double>& trans, int level) const {
     return nricp_b200::evaluate_host(*wraps_[i], rot, trans, level);
@@ -1229,6 +1251,7 @@ struct Server::Impl {
     long submitted = 0, completed = 0, failed = 0, ticks = 0, launches = 0, captures = 0;
     double busy_seconds = 0.0;
     cudaEvent_t tick_begin = nullptr, tick_end = nullptr;
+    int* query_counter = nullptr;        // the query queue's next item
     std::vector<double> latencies, queue_waits;
     double first_submit = -1.0, last_done = 0.0;
 
@@ -1722,6 +1745,8 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     }
     check(cudaMalloc(&m.staging_controls, sizeof(WrapControl) * Impl::kLoaders), "cudaMalloc(staging control)");
     check(cudaEventCreate(&m.tick_begin), "event");
+    check(cudaMalloc(&m.query_counter, sizeof(int)), "cudaMalloc(query queue)");
+    m.shape.query_counter = m.query_counter;
     check(cudaEventCreate(&m.tick_end), "event");
     if (m.cfg.pcg_cluster <= 0) {
         m.class_top = m.cfg.pcg_cluster < 0 ? std::max(1, 16 >> m.max_shift()) : 16;
@@ -1785,6 +1810,7 @@ Server::~Server() {
     }
     if (m.class_fork) cudaEventDestroy(m.class_fork);
     if (m.tick_begin) cudaEventDestroy(m.tick_begin);
+    if (m.query_counter) cudaFree(m.query_counter);
     if (m.tick_end) cudaEventDestroy(m.tick_end);
     if (m.dev_wraps) cudaFree(m.dev_wraps);
     if (m.dev_controls) cudaFree(m.dev_controls);

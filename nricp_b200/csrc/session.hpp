@@ -81,6 +81,8 @@ public:
     // The current system of wrap `i` and the state it was assembled at.
     void inspect(int i, NricpInspect* out);
     void result(int i, NricpResult* out);
+    // Every wrap's result: downloads in turn, then the host work in parallel.
+    void results(NricpResult* outs);
     void current_vertices(int i, double* out);
     int finest_nodes(int i) const;
     int levels(int i) const;
@@ -101,6 +103,7 @@ private:
     WrapControl* dev_controls_ = nullptr;
     void* lbvh_scratch_ = nullptr;  // hierarchy build scratch, shared by the wraps' builds
     cudaMemPool_t pool_ = nullptr;  // the arenas' and the scratch's (batch_pool)
+    int* query_counter_ = nullptr;  // the query queue's next item
     int* pcg_index_ = nullptr;      // wraps ordered by solve class (device)
     cudaStream_t pcg_streams_[5] = {};
     cudaEvent_t pcg_join_[5] = {};

@@ -1481,7 +1481,7 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     k_evaluate<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
     k_normals<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
     if (timers && timers->active) cudaEventRecord(timers->query_begin, stream);
-    launch_query(wraps, W, s.max_vertices, stream);
+    launch_query(wraps, W, s.max_vertices, stream, s.query_counter);
     if (timers && timers->active) cudaEventRecord(timers->query_end, stream);
     k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 1);
     if (timers && timers->active) cudaEventRecord(timers->assemble_begin, stream);
