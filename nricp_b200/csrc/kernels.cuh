@@ -52,6 +52,9 @@ struct TickShape {
     cudaStream_t pcg_streams[5];         // branch streams (index 0 unused)
     cudaEvent_t pcg_fork, pcg_join[5];
     int* query_counter;                  // device: the query queue's next item (null: no queue)
+    // The refresh chain's branch (null: one chain on the tick's stream).
+    cudaStream_t side_stream;
+    cudaEvent_t side_fork, side_join;
 };
 
 // Device timing hooks for the dominant kernels (CUDA events on the launching

@@ -565,6 +565,9 @@ Batch::~Batch() {
     }
     wraps_.clear();
     if (query_counter_) cudaFree(query_counter_);
+    if (side_stream_) cudaStreamDestroy(side_stream_);
+    if (side_fork_) cudaEventDestroy(side_fork_);
+    if (side_join_) cudaEventDestroy(side_join_);
     if (dev_wraps_) cudaFree(dev_wraps_);
     if (dev_controls_) cudaFree(dev_controls_);
     if (lbvh_scratch_) cudaFree(lbvh_scratch_);
@@ -704,6 +707,14 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
     shape_.wraps = W;
     check(cudaMalloc(&query_counter_, sizeof(int)), "cudaMalloc(query queue)");
     shape_.query_counter = query_counter_;
+    if (!side_stream_) {
+        check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "stream");
+        check(cudaEventCreateWithFlags(&side_fork_, cudaEventDisableTiming), "event");
+        check(cudaEventCreateWithFlags(&side_join_, cudaEventDisableTiming), "event");
+    }
+    shape_.side_stream = side_stream_;
+    shape_.side_fork = side_fork_;
+    shape_.side_join = side_join_;
     for (int i = 0; i < W; ++i) {
         Wrap& w = *wraps_[i];
         check(cudaMemcpyAsync(w.arena.base(), staging.data() + offset[i], w.input_bytes, cudaMemcpyHostToDevice,
@@ -1747,6 +1758,9 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     check(cudaEventCreate(&m.tick_begin), "event");
     check(cudaMalloc(&m.query_counter, sizeof(int)), "cudaMalloc(query queue)");
     m.shape.query_counter = m.query_counter;
+    check(cudaStreamCreateWithFlags(&m.shape.side_stream, cudaStreamNonBlocking), "stream");
+    check(cudaEventCreateWithFlags(&m.shape.side_fork, cudaEventDisableTiming), "event");
+    check(cudaEventCreateWithFlags(&m.shape.side_join, cudaEventDisableTiming), "event");
     check(cudaEventCreate(&m.tick_end), "event");
     if (m.cfg.pcg_cluster <= 0) {
         m.class_top = m.cfg.pcg_cluster < 0 ? std::max(1, 16 >> m.max_shift()) : 16;
@@ -1811,6 +1825,9 @@ Server::~Server() {
     if (m.class_fork) cudaEventDestroy(m.class_fork);
     if (m.tick_begin) cudaEventDestroy(m.tick_begin);
     if (m.query_counter) cudaFree(m.query_counter);
+    if (m.shape.side_stream) cudaStreamDestroy(m.shape.side_stream);
+    if (m.shape.side_fork) cudaEventDestroy(m.shape.side_fork);
+    if (m.shape.side_join) cudaEventDestroy(m.shape.side_join);
     if (m.tick_end) cudaEventDestroy(m.tick_end);
     if (m.dev_wraps) cudaFree(m.dev_wraps);
     if (m.dev_controls) cudaFree(m.dev_controls);

@@ -104,6 +104,8 @@ private:
     void* lbvh_scratch_ = nullptr;  // hierarchy build scratch, shared by the wraps' builds
     cudaMemPool_t pool_ = nullptr;  // the arenas' and the scratch's (batch_pool)
     int* query_counter_ = nullptr;  // the query queue's next item
+    cudaStream_t side_stream_ = nullptr;  // the tick's refresh branch
+    cudaEvent_t side_fork_ = nullptr, side_join_ = nullptr;
     int* pcg_index_ = nullptr;      // wraps ordered by solve class (device)
     cudaStream_t pcg_streams_[5] = {};
     cudaEvent_t pcg_join_[5] = {};

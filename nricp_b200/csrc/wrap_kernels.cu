@@ -954,10 +954,12 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
 // deformation evaluation (deformation.cpp:55-68) and the deformed template's
 // vertex normals (mesh.cpp:71-88)
 // ---------------------------------------------------------------------------
-__global__ void k_evaluate(const WrapDev* __restrict__ wraps) {
+// part: 0 every wrap, 1 the wraps in a solve, 2 the others.
+__global__ void k_evaluate(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
     if (c.phase == kPhaseDone || !has_candidate(c)) return;
+    if ((part == 1 && c.phase != kPhaseSolve) || (part == 2 && c.phase == kPhaseSolve)) return;
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= w.V) return;
     const LevelDev& L = w.levels[c.level];
@@ -1441,8 +1443,30 @@ int blocks_of(long n, int threads) { return (int)((n + threads - 1) / threads); 
 void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
                  KernelTimers* timers) {
     const int W = s.wraps;
+    const dim3 vertex_grid(blocks_of(s.max_vertices, kVertexThreads), W);
     k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 0);
-    k_prologue<<<dim3(blocks_of(s.max_nodes, 128), W), 128, 0, stream>>>(wraps);
+    // A wrap is either in a solve or in a refresh-like phase, never both in
+    // one tick, and the two chains touch different wraps: the solve chain
+    // (Horn fit, PCG, candidate evaluation) and the refresh chain (warm start,
+    // evaluation, normals, closest points) run as parallel branches when a
+    // side stream is given, and join before the assembly.
+    const bool split = s.side_stream != nullptr;
+    cudaStream_t refresh = stream;
+    if (split) {
+        cudaEventRecord(s.side_fork, stream);
+        cudaStreamWaitEvent(s.side_stream, s.side_fork, 0);
+        refresh = s.side_stream;
+    }
+    k_prologue<<<dim3(blocks_of(s.max_nodes, 128), W), 128, 0, refresh>>>(wraps);
+    if (split) {
+        k_evaluate<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps, 2);
+        k_normals<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps);
+        if (timers && timers->active) cudaEventRecord(timers->query_begin, refresh);
+        launch_query(wraps, W, s.max_vertices, refresh, s.query_counter);
+        if (timers && timers->active) cudaEventRecord(timers->query_end, refresh);
+        k_stats<<<dim3(1, W), kStatsThreads, 0, refresh>>>(wraps, 1);
+        cudaEventRecord(s.side_join, refresh);
+    }
     const dim3 warp_grid(blocks_of((long)s.max_nodes * 32, kNodeThreads), W);
     k_c_fit<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
     k_c_rhs<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
@@ -1478,12 +1502,17 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
         for (int g = 1; g < s.pcg_groups; ++g) cudaStreamWaitEvent(stream, s.pcg_join[g], 0);
     }
     if (timers && timers->active) cudaEventRecord(timers->pcg_end, stream);
-    k_evaluate<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
-    k_normals<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
-    if (timers && timers->active) cudaEventRecord(timers->query_begin, stream);
-    launch_query(wraps, W, s.max_vertices, stream, s.query_counter);
-    if (timers && timers->active) cudaEventRecord(timers->query_end, stream);
-    k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 1);
+    if (split) {
+        k_evaluate<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps, 1);
+        cudaStreamWaitEvent(stream, s.side_join, 0);
+    } else {
+        k_evaluate<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps, 0);
+        k_normals<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps);
+        if (timers && timers->active) cudaEventRecord(timers->query_begin, stream);
+        launch_query(wraps, W, s.max_vertices, stream, s.query_counter);
+        if (timers && timers->active) cudaEventRecord(timers->query_end, stream);
+        k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 1);
+    }
     if (timers && timers->active) cudaEventRecord(timers->assemble_begin, stream);
     k_residual<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
     k_node_assemble<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
@@ -1497,7 +1526,7 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
 }
 
 int tick_kernel_launches(const TickShape& s) {
-    return (s.max_pairs > 0 ? 14 : 13) + (s.pcg_groups > 0 ? s.pcg_groups : 1);
+    return (s.max_pairs > 0 ? 14 : 13) + (s.pcg_groups > 0 ? s.pcg_groups : 1) + (s.side_stream ? 1 : 0);
 }
 
 // Cluster size of the solve for one wrap of `nodes` nodes on its own: a
