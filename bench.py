@@ -293,6 +293,8 @@ def roofline(batch, peak_gbs: float) -> tuple[dict, dict]:
                   "algorithmic_gb": nbytes[k] / 1e9,
                   "gbs": nbytes[k] / (ms[k] * 1e-3) / 1e9 if ms[k] > 0 else 0.0} for k in ms}
     detail["ticks"] = launches
+    detail["timing"] = ("CUDA events per kernel group on a re-run whose ticks run the solve and refresh "
+                        "branches one after the other; the timed step runs them side by side")
     detail["tick_ms_total"] = total_tick
     detail["work"] = work
     line = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak_gbs,

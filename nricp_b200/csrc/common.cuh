@@ -97,7 +97,7 @@ struct WrapControl {
     int pcg_iterations;
     int error;            // sticky device error (traversal overflow, ...)
     int steps;            // ticks that did work for this wrap
-    int pad;
+    int tick_phase;       // the phase at the start of the current tick
     double damping;
     double energy;              // accepted energy with the current correspondences
     double energy_parts[kEnergyKinds];

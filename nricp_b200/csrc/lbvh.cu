@@ -661,7 +661,7 @@ __device__ void query_vertex(const WrapDev& w, int level, int v) {
 __global__ void k_query(const WrapDev* __restrict__ wraps) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
-    if (!queries(c.phase)) return;
+    if (!queries(c.tick_phase)) return;
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= w.V) return;
     query_vertex(w, c.level, v);
@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__
                                                     int* __restrict__ counter) {
     extern __shared__ int first[];  // wrap_count + 1: each querying wrap's first item
     for (int i = threadIdx.x; i < wrap_count; i += blockDim.x)
-        first[i + 1] = queries(wraps[i].control->phase) ? wraps[i].V : 0;
+        first[i + 1] = queries(wraps[i].control->tick_phase) ? wraps[i].V : 0;
     __syncthreads();
     if (threadIdx.x < 32) {  // inclusive scan by warp 0, 32 wraps at a time
         const int lane = threadIdx.x;

@@ -30,6 +30,13 @@ constexpr int kEdgeThreads = 128;
 constexpr int kPcgThreads = 512;
 constexpr int kStatsThreads = 512;
 
+// Which branch of a tick handles a wrap: part 0 every wrap (one chain), 1 the
+// wraps that started the tick in a solve, 2 the others.  The phase at the
+// tick's start decides, so a wrap that one branch's decision moves on is not
+// picked up by the other branch in the same tick.
+__device__ inline bool in_part(const WrapControl& c, int part) {
+    return part == 0 || (part == 1) == (c.tick_phase == kPhaseSolve);
+}
 __device__ inline bool refresh_like(int phase) {
     return phase == kPhaseTransfer || phase == kPhaseRefresh || phase == kPhaseFinal;
 }
@@ -210,13 +217,16 @@ __device__ inline void add_rank_one(float* d, const float* u, float coef) {
 // ---------------------------------------------------------------------------
 // statistics (deform_ops.cu:135-182 / correspondence.cpp:82-94)
 // ---------------------------------------------------------------------------
+// The statistics pass at a tick's start (final_mode 0) also takes the tick's
+// phase snapshot.
 __global__ void k_stats(const WrapDev* __restrict__ wraps, int final_mode) {
     const WrapDev& w = wraps[blockIdx.y * gridDim.x + blockIdx.x];
     const WrapControl c = *w.control;
+    if (!final_mode && threadIdx.x == 0) w.control->tick_phase = c.phase;
     CorrStats* target = nullptr;
     int level = -1;
     if (final_mode) {
-        if (c.phase != kPhaseFinal) return;
+        if (c.tick_phase != kPhaseFinal || c.phase != kPhaseFinal) return;
         target = w.final_stats;
     } else {
         if (c.stats_pending == 0) return;
@@ -315,9 +325,10 @@ __global__ void k_stats(const WrapDev* __restrict__ wraps, int final_mode) {
 // ---------------------------------------------------------------------------
 // node prologue: level warm start (deformation.cpp:141-203) and FP32 copies
 // ---------------------------------------------------------------------------
-__global__ void k_prologue(const WrapDev* __restrict__ wraps) {
+__global__ void k_prologue(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (!refresh_like(c.phase)) return;
     const LevelDev& L = w.levels[c.level];
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -439,9 +450,10 @@ constexpr double kRotationRelaxation = 0.2;  // local_global.cu:18
 // Warp per node: the correlation of the influences that mention the node
 // (bound vertices' data and landmark rows, edges it is the first endpoint of),
 // Horn's rotation, and the under-relaxed update into the candidate buffer.
-__global__ void k_c_fit(const WrapDev* __restrict__ wraps) {
+__global__ void k_c_fit(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (c.phase != kPhaseSolve || c.route != 1) return;
     const LevelDev& L = w.levels[c.level];
     const int node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -503,9 +515,10 @@ __global__ void k_c_fit(const WrapDev* __restrict__ wraps) {
 
 // Warp per node: the translation-only right-hand side with the fitted
 // rotations (local_global.cu:317-438); the rotation half is exactly zero.
-__global__ void k_c_rhs(const WrapDev* __restrict__ wraps) {
+__global__ void k_c_rhs(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (c.phase != kPhaseSolve || c.route != 1) return;
     const LevelDev& L = w.levels[c.level];
     const int node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -709,7 +722,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
     if (slot < 0) return;  // an empty entry of a class launch; uniform across the cluster
     const WrapDev& w = wraps[slot];
     const WrapControl c = *w.control;
-    if (c.phase != kPhaseSolve) return;  // uniform across the cluster
+    if (c.tick_phase != kPhaseSolve || c.phase != kPhaseSolve) return;  // uniform across the cluster
     const LevelDev& L = w.levels[c.level];
     const int N = L.node_count;
     const int rank = (int)cluster.block_rank();
@@ -954,12 +967,11 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
 // deformation evaluation (deformation.cpp:55-68) and the deformed template's
 // vertex normals (mesh.cpp:71-88)
 // ---------------------------------------------------------------------------
-// part: 0 every wrap, 1 the wraps in a solve, 2 the others.
 __global__ void k_evaluate(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (c.phase == kPhaseDone || !has_candidate(c)) return;
-    if ((part == 1 && c.phase != kPhaseSolve) || (part == 2 && c.phase == kPhaseSolve)) return;
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= w.V) return;
     const LevelDev& L = w.levels[c.level];
@@ -981,9 +993,10 @@ __global__ void k_evaluate(const WrapDev* __restrict__ wraps, int part) {
     w.deformed32[v] = make_float4((float)sum.x, (float)sum.y, (float)sum.z, 0.0f);
 }
 
-__global__ void k_normals(const WrapDev* __restrict__ wraps) {
+__global__ void k_normals(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (!refresh_like(c.phase)) return;
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= w.V) return;
@@ -1005,9 +1018,10 @@ __global__ void k_normals(const WrapDev* __restrict__ wraps) {
 // per-vertex residuals, the data and landmark energies (FP64), and the FP32
 // residual records the assembly reads (fused_assembly.cpp:185-216, 262-280)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __restrict__ wraps) {
+__global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (!computes_energy(c)) return;
     if ((long)blockIdx.x * blockDim.x >= w.V) return;
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1071,9 +1085,10 @@ __device__ inline F3 node_offset32(const WrapDev& w, const LevelDev& L, int node
     return mul3f(w.rot32 + node * 9, {(float)p.x, (float)p.y, (float)p.z});
 }
 
-__global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps) {
+__global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (!computes_energy(c)) return;
     const bool build = assembles(c);
     const LevelDev& L = w.levels[c.level];
@@ -1210,9 +1225,10 @@ __device__ inline void store_block_pair(float* out, const LevelDev& L, int k, co
 
 // Warp per node pair: lanes stride over the vertices the two nodes share,
 // each lane keeps a 6x6 block in registers, one butterfly reduction.
-__global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps) {
+__global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (!assembles(c)) return;
     const LevelDev& L = w.levels[c.level];
     const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1264,9 +1280,10 @@ __global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev
     if (lane == 0) store_block_pair(w.offdiag[1 - c.system], L, L.edge_count + p, blk);
 }
 
-__global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps) {
+__global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
+    if (!in_part(c, part)) return;
     if (!computes_energy(c)) return;
     const LevelDev& L = w.levels[c.level];
     if ((long)blockIdx.x * blockDim.x >= L.edge_count) return;
@@ -1317,9 +1334,10 @@ __device__ inline double relative_change(double before, double after) {  // rout
     return (before - after) / fmax(fabs(before), 1e-12);
 }
 
-__global__ void k_decide(const WrapDev* __restrict__ wraps) {
+__global__ void k_decide(const WrapDev* __restrict__ wraps, int part) {
     const WrapDev& w = wraps[blockIdx.x];
     WrapControl* ctl = w.control;
+    if (part != 0 && (part == 1) != (ctl->tick_phase == kPhaseSolve)) return;
     const int phase = ctl->phase;
     if (phase == kPhaseDone) return;
     __shared__ double scratch[33];
@@ -1444,33 +1462,40 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
                  KernelTimers* timers) {
     const int W = s.wraps;
     const dim3 vertex_grid(blocks_of(s.max_vertices, kVertexThreads), W);
+    const dim3 warp_grid(blocks_of((long)s.max_nodes * 32, kNodeThreads), W);
+    const dim3 pair_grid(blocks_of((long)s.max_pairs * 32, kNodeThreads), W);
+    const dim3 edge_grid(blocks_of(s.max_edges > 0 ? s.max_edges : 1, kEdgeThreads), W);
+    const bool timed = timers && timers->active;
+    // statistics of a finished level, and every wrap's phase at the tick's start
     k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 0);
-    // A wrap is either in a solve or in a refresh-like phase, never both in
-    // one tick, and the two chains touch different wraps: the solve chain
-    // (Horn fit, PCG, candidate evaluation) and the refresh chain (warm start,
-    // evaluation, normals, closest points) run as parallel branches when a
-    // side stream is given, and join before the assembly.
-    const bool split = s.side_stream != nullptr;
-    cudaStream_t refresh = stream;
+    // A wrap that starts the tick in a solve runs the solve chain (Horn fit,
+    // PCG, candidate evaluation, energy and system, decision); any other runs
+    // the refresh chain (warm start, evaluation, normals, closest points,
+    // energy and system, decision).  The chains touch different wraps, so
+    // with a side stream they run as two parallel branches of the tick.  A
+    // timed tick runs them one after the other, so that each kernel group's
+    // time is its own.
+    const bool split = s.side_stream != nullptr && !timed;
+    const int solve_part = split ? 1 : 0, refresh_part = split ? 2 : 0;
+    cudaStream_t refresh = split ? s.side_stream : stream;
+    auto assemble_and_decide = [&](int part, cudaStream_t on) {
+        if (timed) cudaEventRecord(timers->assemble_begin, on);
+        k_residual<<<vertex_grid, kVertexThreads, 0, on>>>(wraps, part);
+        k_node_assemble<<<warp_grid, kNodeThreads, 0, on>>>(wraps, part);
+        if (s.max_pairs > 0) k_pair_assemble<<<pair_grid, kNodeThreads, 0, on>>>(wraps, part);
+        k_edge_assemble<<<edge_grid, kEdgeThreads, 0, on>>>(wraps, part);
+        if (timed) cudaEventRecord(timers->assemble_end, on);
+        k_decide<<<W, 256, 0, on>>>(wraps, part);
+    };
     if (split) {
         cudaEventRecord(s.side_fork, stream);
-        cudaStreamWaitEvent(s.side_stream, s.side_fork, 0);
-        refresh = s.side_stream;
+        cudaStreamWaitEvent(refresh, s.side_fork, 0);
     }
-    k_prologue<<<dim3(blocks_of(s.max_nodes, 128), W), 128, 0, refresh>>>(wraps);
-    if (split) {
-        k_evaluate<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps, 2);
-        k_normals<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps);
-        if (timers && timers->active) cudaEventRecord(timers->query_begin, refresh);
-        launch_query(wraps, W, s.max_vertices, refresh, s.query_counter);
-        if (timers && timers->active) cudaEventRecord(timers->query_end, refresh);
-        k_stats<<<dim3(1, W), kStatsThreads, 0, refresh>>>(wraps, 1);
-        cudaEventRecord(s.side_join, refresh);
-    }
-    const dim3 warp_grid(blocks_of((long)s.max_nodes * 32, kNodeThreads), W);
-    k_c_fit<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
-    k_c_rhs<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
-    if (timers && timers->active) cudaEventRecord(timers->pcg_begin, stream);
+
+    // ---- the solve chain ----
+    k_c_fit<<<warp_grid, kNodeThreads, 0, stream>>>(wraps, solve_part);
+    k_c_rhs<<<warp_grid, kNodeThreads, 0, stream>>>(wraps, solve_part);
+    if (timed) cudaEventRecord(timers->pcg_begin, stream);
     auto launch_pcg = [&](int cluster, int count, int shared, const int* index, cudaStream_t on) {
         cudaLaunchConfig_t config = {};
         config.gridDim = dim3(cluster, count);
@@ -1501,32 +1526,31 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
                    s.pcg_group_index[0], stream);
         for (int g = 1; g < s.pcg_groups; ++g) cudaStreamWaitEvent(stream, s.pcg_join[g], 0);
     }
-    if (timers && timers->active) cudaEventRecord(timers->pcg_end, stream);
+    if (timed) cudaEventRecord(timers->pcg_end, stream);
     if (split) {
-        k_evaluate<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps, 1);
-        cudaStreamWaitEvent(stream, s.side_join, 0);
-    } else {
-        k_evaluate<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps, 0);
-        k_normals<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps);
-        if (timers && timers->active) cudaEventRecord(timers->query_begin, stream);
-        launch_query(wraps, W, s.max_vertices, stream, s.query_counter);
-        if (timers && timers->active) cudaEventRecord(timers->query_end, stream);
-        k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 1);
+        k_evaluate<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps, solve_part);
+        assemble_and_decide(solve_part, stream);
     }
-    if (timers && timers->active) cudaEventRecord(timers->assemble_begin, stream);
-    k_residual<<<dim3(blocks_of(s.max_vertices, kVertexThreads), W), kVertexThreads, 0, stream>>>(wraps);
-    k_node_assemble<<<warp_grid, kNodeThreads, 0, stream>>>(wraps);
-    if (s.max_pairs > 0)
-        k_pair_assemble<<<dim3(blocks_of((long)s.max_pairs * 32, kNodeThreads), W), kNodeThreads, 0,
-                          stream>>>(wraps);
-    k_edge_assemble<<<dim3(blocks_of(s.max_edges > 0 ? s.max_edges : 1, kEdgeThreads), W),
-                      kEdgeThreads, 0, stream>>>(wraps);
-    if (timers && timers->active) cudaEventRecord(timers->assemble_end, stream);
-    k_decide<<<W, 256, 0, stream>>>(wraps);
+
+    // ---- the refresh chain ----
+    k_prologue<<<dim3(blocks_of(s.max_nodes, 128), W), 128, 0, refresh>>>(wraps, refresh_part);
+    k_evaluate<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps, refresh_part);
+    k_normals<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps, refresh_part);
+    if (timed) cudaEventRecord(timers->query_begin, refresh);
+    launch_query(wraps, W, s.max_vertices, refresh, s.query_counter);
+    if (timed) cudaEventRecord(timers->query_end, refresh);
+    k_stats<<<dim3(1, W), kStatsThreads, 0, refresh>>>(wraps, 1);
+    assemble_and_decide(refresh_part, refresh);
+    if (split) {
+        cudaEventRecord(s.side_join, refresh);
+        cudaStreamWaitEvent(stream, s.side_join, 0);
+    }
 }
 
 int tick_kernel_launches(const TickShape& s) {
-    return (s.max_pairs > 0 ? 14 : 13) + (s.pcg_groups > 0 ? s.pcg_groups : 1) + (s.side_stream ? 1 : 0);
+    // an untimed tick with a side stream assembles and decides in each branch
+    const int per_chain = (s.max_pairs > 0 ? 5 : 4) + 1;  // residual, node, pair, edge, decide; evaluate
+    return (s.max_pairs > 0 ? 14 : 13) + (s.pcg_groups > 0 ? s.pcg_groups : 1) + (s.side_stream ? per_chain : 0);
 }
 
 // Cluster size of the solve for one wrap of `nodes` nodes on its own: a
