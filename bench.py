@@ -75,6 +75,8 @@ def parse_args():
     p.add_argument("--instances", type=int, default=INSTANCES,
                    help="wraps in the batch (config 3 has 64; fewer for profiling captures)")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--batch-only", action="store_true",
+                   help="only the batched value (for profiler captures of its launches)")
     p.add_argument("--serve-rates", default="20,80",
                    help="Poisson arrival rates (requests/s) of the serving windows")
     p.add_argument("--serve-seconds", type=float, default=6.0,
@@ -415,6 +417,12 @@ def run_ours(args, ranks):
     total_ms = ranks.max(sum(step_ms))
     wraps = ranks.sum(float(args.steps * len(cases)))
     value = wraps / (total_ms * 1e-3)
+    if args.batch_only:
+        if ranks.rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ranks.world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+                              "gpu_launches": launches, "batch_only": True}), flush=True)
+        return
 
     # ---- plain: the same wraps one at a time through the same engine ----
     plain_ms = []

@@ -37,6 +37,7 @@ struct TickShape {
     int max_nodes;
     int max_edges;
     int max_pairs;
+    int route_c;         // some wrap solves by route C (else its Horn-fit kernels are not launched)
     int energy_blocks;   // vertex-pass blocks per wrap (partials written)
     int edge_blocks;
     int node_blocks;

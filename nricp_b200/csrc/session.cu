@@ -725,6 +725,7 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
         shape_.max_nodes = std::max(shape_.max_nodes, w.max_nodes);
         shape_.max_edges = std::max(shape_.max_edges, w.max_edges);
         shape_.max_pairs = std::max(shape_.max_pairs, w.max_pairs);
+        if (w.desc.route == NRICP_ROUTE_C) shape_.route_c = 1;
     }
     set_pcg_cluster(default_pcg_cluster());
     check(cudaMalloc(&dev_wraps_, sizeof(WrapDev) * W), "cudaMalloc(wraps)");
@@ -1425,6 +1426,7 @@ struct Server::Impl {
         shape.max_nodes = std::max(shape.max_nodes, w.max_nodes);
         shape.max_edges = std::max(shape.max_edges, w.max_edges);
         shape.max_pairs = std::max(shape.max_pairs, w.max_pairs);
+        if (w.desc.route == NRICP_ROUTE_C) shape.route_c = 1;
         if (std::memcmp(&before, &shape, sizeof shape) != 0) {
             for (auto& [count, g] : graphs) cudaGraphExecDestroy(g);
             graphs.clear();

@@ -37,6 +37,51 @@ constexpr int kStatsThreads = 512;
 __device__ inline bool in_part(const WrapControl& c, int part) {
     return part == 0 || (part == 1) == (c.tick_phase == kPhaseSolve);
 }
+__device__ inline int blocks_of_dev(long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+// Most wraps of a batch are smaller than the largest, and in any tick only
+// some of them have work for a given kernel; a grid sized for the largest wrap
+// times the wraps launches mostly blocks that return at once.  Instead a
+// kernel's work is a list of virtual blocks -- block x of wrap y, exactly the
+// blocks the full grid would run to some effect -- which a grid that fits on
+// the device walks in order.  Each virtual block does the same work, with
+// the same reductions and the same partial slots, as that block of the full
+// grid, so results do not change.  need(w) gives the virtual blocks of wrap w
+// (0: none this tick); body(wrap index, x) runs one.  The launch gives
+// (wrap_count + 1) ints of dynamic shared memory.
+template <typename Need, typename Body>
+__device__ __forceinline__ void over_virtual_blocks(const WrapDev* __restrict__ wraps, int wrap_count, Need need,
+                                                    Body body) {
+    extern __shared__ int first[];  // each wrap's first virtual block
+    for (int i = threadIdx.x; i < wrap_count; i += blockDim.x) first[i + 1] = need(wraps[i]);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // inclusive scan by warp 0, 32 wraps at a time
+        const int lane = threadIdx.x;
+        int carry = 0;
+        for (int base = 0; base < wrap_count; base += 32) {
+            int x = base + lane < wrap_count ? first[base + lane + 1] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (base + lane < wrap_count) first[base + lane + 1] = carry + x;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) first[0] = 0;
+    }
+    __syncthreads();
+    const int total = first[wrap_count];
+    for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+        int lo = 0, hi = wrap_count - 1;  // the last wrap whose first block is <= vb
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first[mid] <= vb) lo = mid; else hi = mid - 1;
+        }
+        body(lo, vb - first[lo]);
+        __syncthreads();  // shared memory of one virtual block before the next
+    }
+}
+
 __device__ inline bool refresh_like(int phase) {
     return phase == kPhaseTransfer || phase == kPhaseRefresh || phase == kPhaseFinal;
 }
@@ -325,13 +370,12 @@ __global__ void k_stats(const WrapDev* __restrict__ wraps, int final_mode) {
 // ---------------------------------------------------------------------------
 // node prologue: level warm start (deformation.cpp:141-203) and FP32 copies
 // ---------------------------------------------------------------------------
-__global__ void k_prologue(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_prologue_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (!refresh_like(c.phase)) return;
     const LevelDev& L = w.levels[c.level];
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = bx * blockDim.x + threadIdx.x;
     if (n >= L.node_count) return;
     double R[9];
     if (c.phase == kPhaseTransfer) {
@@ -383,6 +427,16 @@ __global__ void k_prologue(const WrapDev* __restrict__ wraps, int part) {
         for (int i = 0; i < 9; ++i) R[i] = src[i];
     }
     for (int i = 0; i < 9; ++i) w.rot32[n * 9 + i] = (float)R[i];
+}
+
+__global__ void k_prologue(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? (refresh_like(c.phase) ? blocks_of_dev(w.levels[c.level].node_count, 128) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_prologue_body(wraps[wi], part, bx); });
 }
 
 // ---------------------------------------------------------------------------
@@ -450,13 +504,12 @@ constexpr double kRotationRelaxation = 0.2;  // local_global.cu:18
 // Warp per node: the correlation of the influences that mention the node
 // (bound vertices' data and landmark rows, edges it is the first endpoint of),
 // Horn's rotation, and the under-relaxed update into the candidate buffer.
-__global__ void k_c_fit(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_c_fit_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (c.phase != kPhaseSolve || c.route != 1) return;
     const LevelDev& L = w.levels[c.level];
-    const int node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int node = (bx * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (node >= L.node_count) return;
     const double* wt = w.weights[c.level];
@@ -513,15 +566,24 @@ __global__ void k_c_fit(const WrapDev* __restrict__ wraps, int part) {
     }
 }
 
+__global__ void k_c_fit(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? ((c.phase == kPhaseSolve && c.route == 1) ? blocks_of_dev(w.levels[c.level].node_count * 32, kNodeThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_c_fit_body(wraps[wi], part, bx); });
+}
+
 // Warp per node: the translation-only right-hand side with the fitted
 // rotations (local_global.cu:317-438); the rotation half is exactly zero.
-__global__ void k_c_rhs(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_c_rhs_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (c.phase != kPhaseSolve || c.route != 1) return;
     const LevelDev& L = w.levels[c.level];
-    const int node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int node = (bx * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (node >= L.node_count) return;
     const double* wt = w.weights[c.level];
@@ -579,6 +641,16 @@ __global__ void k_c_rhs(const WrapDev* __restrict__ wraps, int part) {
         r[4] = (float)(local[1] - wt[3] * t.y);
         r[5] = (float)(local[2] - wt[3] * t.z);
     }
+}
+
+__global__ void k_c_rhs(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? ((c.phase == kPhaseSolve && c.route == 1) ? blocks_of_dev(w.levels[c.level].node_count * 32, kNodeThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_c_rhs_body(wraps[wi], part, bx); });
 }
 
 // ---------------------------------------------------------------------------
@@ -967,12 +1039,11 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
 // deformation evaluation (deformation.cpp:55-68) and the deformed template's
 // vertex normals (mesh.cpp:71-88)
 // ---------------------------------------------------------------------------
-__global__ void k_evaluate(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_evaluate_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (c.phase == kPhaseDone || !has_candidate(c)) return;
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx * blockDim.x + threadIdx.x;
     if (v >= w.V) return;
     const LevelDev& L = w.levels[c.level];
     const int buf = eval_buffer(c);
@@ -993,12 +1064,21 @@ __global__ void k_evaluate(const WrapDev* __restrict__ wraps, int part) {
     w.deformed32[v] = make_float4((float)sum.x, (float)sum.y, (float)sum.z, 0.0f);
 }
 
-__global__ void k_normals(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__global__ void k_evaluate(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? ((c.phase != kPhaseDone && has_candidate(c)) ? blocks_of_dev(w.V, kVertexThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_evaluate_body(wraps[wi], part, bx); });
+}
+
+__device__ __forceinline__ void k_normals_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (!refresh_like(c.phase)) return;
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = bx * blockDim.x + threadIdx.x;
     if (v >= w.V) return;
     D3 n = {0.0, 0.0, 0.0};
     for (int i = w.vf_begin[v]; i < w.vf_begin[v + 1]; ++i) {
@@ -1014,17 +1094,26 @@ __global__ void k_normals(const WrapDev* __restrict__ wraps, int part) {
     store_d3(w.qnormals, v, n);
 }
 
+__global__ void k_normals(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? (refresh_like(c.phase) ? blocks_of_dev(w.V, kVertexThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_normals_body(wraps[wi], part, bx); });
+}
+
 // ---------------------------------------------------------------------------
 // per-vertex residuals, the data and landmark energies (FP64), and the FP32
 // residual records the assembly reads (fused_assembly.cpp:185-216, 262-280)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_residual_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (!computes_energy(c)) return;
-    if ((long)blockIdx.x * blockDim.x >= w.V) return;
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((long)bx * blockDim.x >= w.V) return;
+    const int v = bx * blockDim.x + threadIdx.x;
     const double* wt = w.weights[c.level];
     const LevelDev& L = w.levels[c.level];
     double e_p2p = 0.0, e_plane = 0.0, e_lm = 0.0;
@@ -1068,9 +1157,19 @@ __global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __re
     const double s1 = block_sum<kVertexThreads>(e_plane, scratch);
     const double s4 = block_sum<kVertexThreads>(e_lm, scratch);
     if (threadIdx.x == 0) {
-        double* p = w.partials + (long)blockIdx.x * kPartialStride;
+        double* p = w.partials + (long)bx * kPartialStride;
         p[0] = s0; p[1] = s1; p[2] = s4;
     }
+}
+
+__global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? (computes_energy(c) ? blocks_of_dev(w.V, kVertexThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_residual_body(wraps[wi], part, bx); });
 }
 
 // ---------------------------------------------------------------------------
@@ -1085,15 +1184,14 @@ __device__ inline F3 node_offset32(const WrapDev& w, const LevelDev& L, int node
     return mul3f(w.rot32 + node * 9, {(float)p.x, (float)p.y, (float)p.z});
 }
 
-__global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_node_assemble_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (!computes_energy(c)) return;
     const bool build = assembles(c);
     const LevelDev& L = w.levels[c.level];
-    if ((long)blockIdx.x * (kNodeThreads / 32) >= L.node_count) return;
-    const int node = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if ((long)bx * (kNodeThreads / 32) >= L.node_count) return;
+    const int node = (bx * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const double* wt = w.weights[c.level];
     const int buf = eval_buffer(c);
@@ -1208,7 +1306,17 @@ __global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev
     }
     __shared__ double scratch[33];
     const double total = block_sum<kNodeThreads>(e_anchor, scratch);
-    if (threadIdx.x == 0) w.node_partials[blockIdx.x] = total;
+    if (threadIdx.x == 0) w.node_partials[bx] = total;
+}
+
+__global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? (computes_energy(c) ? blocks_of_dev(w.levels[c.level].node_count * 32, kNodeThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_node_assemble_body(wraps[wi], part, bx); });
 }
 
 // Writes block k of the system twice, in row-entry order: B where the row
@@ -1225,13 +1333,12 @@ __device__ inline void store_block_pair(float* out, const LevelDev& L, int k, co
 
 // Warp per node pair: lanes stride over the vertices the two nodes share,
 // each lane keeps a 6x6 block in registers, one butterfly reduction.
-__global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (!assembles(c)) return;
     const LevelDev& L = w.levels[c.level];
-    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int p = (bx * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= L.pair_count) return;
     const int na = L.pair_nodes[p * 2], nb = L.pair_nodes[p * 2 + 1];
@@ -1280,14 +1387,23 @@ __global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev
     if (lane == 0) store_block_pair(w.offdiag[1 - c.system], L, L.edge_count + p, blk);
 }
 
-__global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps, int part) {
-    const WrapDev& w = wraps[blockIdx.y];
+__global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? (assembles(c) ? blocks_of_dev(w.levels[c.level].pair_count * 32, kNodeThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_pair_assemble_body(wraps[wi], part, bx); });
+}
+
+__device__ __forceinline__ void k_edge_assemble_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
     if (!computes_energy(c)) return;
     const LevelDev& L = w.levels[c.level];
-    if ((long)blockIdx.x * blockDim.x >= L.edge_count) return;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((long)bx * blockDim.x >= L.edge_count) return;
+    const int e = bx * blockDim.x + threadIdx.x;
     const double* wt = w.weights[c.level];
     const int buf = eval_buffer(c);
     double energy = 0.0;
@@ -1323,7 +1439,17 @@ __global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* _
     }
     __shared__ double scratch[33];
     const double total = block_sum<kEdgeThreads>(energy, scratch);
-    if (threadIdx.x == 0) w.edge_partials[blockIdx.x] = total;
+    if (threadIdx.x == 0) w.edge_partials[bx] = total;
+}
+
+__global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
+    over_virtual_blocks(
+        wraps, wrap_count,
+        [&](const WrapDev& w) {
+            const WrapControl c = *w.control;
+            return in_part(c, part) ? (computes_energy(c) ? blocks_of_dev(w.levels[c.level].edge_count, kEdgeThreads) : 0) : 0;
+        },
+        [&](int wi, int bx) { k_edge_assemble_body(wraps[wi], part, bx); });
 }
 
 // ---------------------------------------------------------------------------
@@ -1454,17 +1580,41 @@ __global__ void k_decide(const WrapDev* __restrict__ wraps, int part) {
 // ---------------------------------------------------------------------------
 // host launch of one tick
 // ---------------------------------------------------------------------------
-namespace {
-int blocks_of(long n, int threads) { return (int)((n + threads - 1) / threads); }
+// Grids of the virtual-block kernels: as many blocks as fit on the device
+// at once (occupancy of each kernel at its block size, times the SMs).
+struct VirtualGrids {
+    int prologue, c_fit, c_rhs, evaluate, normals, residual, node, pair, edge;
+};
+const VirtualGrids& virtual_grids() {
+    static const VirtualGrids grids = [] {
+        int device = 0, sms = 148;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        auto fit = [sms](auto kernel, int threads) {
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, sizeof(int) * 1025);
+            return sms * (per_sm > 0 ? per_sm : 1);
+        };
+        VirtualGrids g;
+        g.prologue = fit(k_prologue, 128);
+        g.c_fit = fit(k_c_fit, kNodeThreads);
+        g.c_rhs = fit(k_c_rhs, kNodeThreads);
+        g.evaluate = fit(k_evaluate, kVertexThreads);
+        g.normals = fit(k_normals, kVertexThreads);
+        g.residual = fit(k_residual, kVertexThreads);
+        g.node = fit(k_node_assemble, kNodeThreads);
+        g.pair = fit(k_pair_assemble, kNodeThreads);
+        g.edge = fit(k_edge_assemble, kEdgeThreads);
+        return g;
+    }();
+    return grids;
 }
 
 void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
                  KernelTimers* timers) {
     const int W = s.wraps;
-    const dim3 vertex_grid(blocks_of(s.max_vertices, kVertexThreads), W);
-    const dim3 warp_grid(blocks_of((long)s.max_nodes * 32, kNodeThreads), W);
-    const dim3 pair_grid(blocks_of((long)s.max_pairs * 32, kNodeThreads), W);
-    const dim3 edge_grid(blocks_of(s.max_edges > 0 ? s.max_edges : 1, kEdgeThreads), W);
+    const VirtualGrids& grids = virtual_grids();
+    const size_t virtual_smem = sizeof(int) * (W + 1);
     const bool timed = timers && timers->active;
     // statistics of a finished level, and every wrap's phase at the tick's start
     k_stats<<<dim3(1, W), kStatsThreads, 0, stream>>>(wraps, 0);
@@ -1480,10 +1630,10 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     cudaStream_t refresh = split ? s.side_stream : stream;
     auto assemble_and_decide = [&](int part, cudaStream_t on) {
         if (timed) cudaEventRecord(timers->assemble_begin, on);
-        k_residual<<<vertex_grid, kVertexThreads, 0, on>>>(wraps, part);
-        k_node_assemble<<<warp_grid, kNodeThreads, 0, on>>>(wraps, part);
-        if (s.max_pairs > 0) k_pair_assemble<<<pair_grid, kNodeThreads, 0, on>>>(wraps, part);
-        k_edge_assemble<<<edge_grid, kEdgeThreads, 0, on>>>(wraps, part);
+        k_residual<<<grids.residual, kVertexThreads, virtual_smem, on>>>(wraps, W, part);
+        k_node_assemble<<<grids.node, kNodeThreads, virtual_smem, on>>>(wraps, W, part);
+        if (s.max_pairs > 0) k_pair_assemble<<<grids.pair, kNodeThreads, virtual_smem, on>>>(wraps, W, part);
+        k_edge_assemble<<<grids.edge, kEdgeThreads, virtual_smem, on>>>(wraps, W, part);
         if (timed) cudaEventRecord(timers->assemble_end, on);
         k_decide<<<W, 256, 0, on>>>(wraps, part);
     };
@@ -1493,8 +1643,10 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     }
 
     // ---- the solve chain ----
-    k_c_fit<<<warp_grid, kNodeThreads, 0, stream>>>(wraps, solve_part);
-    k_c_rhs<<<warp_grid, kNodeThreads, 0, stream>>>(wraps, solve_part);
+    if (s.route_c) {
+        k_c_fit<<<grids.c_fit, kNodeThreads, virtual_smem, stream>>>(wraps, W, solve_part);
+        k_c_rhs<<<grids.c_rhs, kNodeThreads, virtual_smem, stream>>>(wraps, W, solve_part);
+    }
     if (timed) cudaEventRecord(timers->pcg_begin, stream);
     auto launch_pcg = [&](int cluster, int count, int shared, const int* index, cudaStream_t on) {
         cudaLaunchConfig_t config = {};
@@ -1528,14 +1680,14 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
     }
     if (timed) cudaEventRecord(timers->pcg_end, stream);
     if (split) {
-        k_evaluate<<<vertex_grid, kVertexThreads, 0, stream>>>(wraps, solve_part);
+        k_evaluate<<<grids.evaluate, kVertexThreads, virtual_smem, stream>>>(wraps, W, solve_part);
         assemble_and_decide(solve_part, stream);
     }
 
     // ---- the refresh chain ----
-    k_prologue<<<dim3(blocks_of(s.max_nodes, 128), W), 128, 0, refresh>>>(wraps, refresh_part);
-    k_evaluate<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps, refresh_part);
-    k_normals<<<vertex_grid, kVertexThreads, 0, refresh>>>(wraps, refresh_part);
+    k_prologue<<<grids.prologue, 128, virtual_smem, refresh>>>(wraps, W, refresh_part);
+    k_evaluate<<<grids.evaluate, kVertexThreads, virtual_smem, refresh>>>(wraps, W, refresh_part);
+    k_normals<<<grids.normals, kVertexThreads, virtual_smem, refresh>>>(wraps, W, refresh_part);
     if (timed) cudaEventRecord(timers->query_begin, refresh);
     launch_query(wraps, W, s.max_vertices, refresh, s.query_counter);
     if (timed) cudaEventRecord(timers->query_end, refresh);
@@ -1550,7 +1702,8 @@ void launch_tick(const WrapDev* wraps, const TickShape& s, cudaStream_t stream,
 int tick_kernel_launches(const TickShape& s) {
     // an untimed tick with a side stream assembles and decides in each branch
     const int per_chain = (s.max_pairs > 0 ? 5 : 4) + 1;  // residual, node, pair, edge, decide; evaluate
-    return (s.max_pairs > 0 ? 14 : 13) + (s.pcg_groups > 0 ? s.pcg_groups : 1) + (s.side_stream ? per_chain : 0);
+    return (s.max_pairs > 0 ? 14 : 13) - (s.route_c ? 0 : 2) + (s.pcg_groups > 0 ? s.pcg_groups : 1) +
+           (s.side_stream ? per_chain : 0);
 }
 
 // Cluster size of the solve for one wrap of `nodes` nodes on its own: a
