@@ -33,7 +33,12 @@ Printed (one JSON line on rank 0):
 * ``single_wrap``  the large single wrap of config 2 (25k vertices onto a
                    393k-triangle target, 2,000 nodes) one at a time.
 
-``--impl reference`` times that reference CPU route instead.  With torchrun
+``--impl reference`` times that reference CPU route instead.
+``--precision OUT.npz`` solves config 5 (100k-vertex template onto a
+2M-triangle target, 10,000 nodes) with the shipped library and with its
+variant whose solve reductions are FP32; ``--precision-compare OUT.npz`` then
+runs the reference's FP64 route A on the same problem on the CPU and reports
+max/RMS vertex error over the diagonal and the energy per level.  With torchrun
 (N > 1) every rank solves its own 64-wrap batch: replicas, no collective on
 the data path.
 """
@@ -77,6 +82,13 @@ def parse_args():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--batch-only", action="store_true",
                    help="only the batched value (for profiler captures of its launches)")
+    p.add_argument("--precision", metavar="OUT.npz",
+                   help="config 5 on the GPU with the shipped library and its FP32-reductions "
+                        "variant; writes both results to OUT.npz")
+    p.add_argument("--precision-variant", metavar="OUT.npz", help=argparse.SUPPRESS)
+    p.add_argument("--precision-compare", metavar="IN.npz",
+                   help="CPU only: the reference's FP64 route A on config 5, against the GPU "
+                        "results of --precision")
     p.add_argument("--serve-rates", default="20,80",
                    help="Poisson arrival rates (requests/s) of the serving windows")
     p.add_argument("--serve-seconds", type=float, default=6.0,
@@ -536,8 +548,102 @@ def run_ours(args, ranks):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# config 5: precision stress
+# ---------------------------------------------------------------------------
+
+def _level_energies(report: str) -> list:
+    return [lv["energy_end"] for lv in json.loads(report)["levels"]]
+
+
+def _precision_solve(seed: int) -> dict:
+    """Config 5 through solve_route_b at the reference's caps (k=4, 4-NN, so
+    that its FP64 route A can run the same problem), and at the config's own
+    k=8 for the time."""
+    from nricp_b200 import nricp_dp as dp
+    from nricp_b200 import synthetic as S
+
+    case = S.config5(seed)
+    out = {}
+    for name, opts in (("capped", reference_options(case.options)), ("k8", case.options)):
+        dp.solve_route_b(*case.args(), **opts)  # warm: library, pools
+        t0 = time.perf_counter()
+        r = dp.solve_route_b(*case.args(), **opts)
+        out[f"{name}_seconds"] = time.perf_counter() - t0
+        out[f"{name}_vertices"] = r["vertices"]
+        out[f"{name}_report"] = r["report"]
+    return out
+
+
+def run_precision(args) -> None:
+    from nricp_b200 import build as native
+
+    shipped = _precision_solve(args.seed)
+    variant_out = Path(args.precision).with_suffix(".variant.npz")
+    env = dict(os.environ, NRICP_B200_LIBRARY=str(native.FP32_REDUCTIONS_LIB))
+    subprocess.run([sys.executable, str(Path(__file__).resolve()), "--precision-variant",
+                    str(variant_out), "--seed", str(args.seed)], check=True, env=env)
+    variant = dict(np.load(variant_out, allow_pickle=False))
+    np.savez(args.precision, seed=args.seed,
+             **{f"fp64_reductions_{k}": v for k, v in shipped.items()},
+             **{f"fp32_reductions_{k}": v for k, v in variant.items()})
+    p = np.asarray(shipped["capped_vertices"])
+    q = np.asarray(variant["capped_vertices"])
+    print(json.dumps({
+        "workload": "config 5: 100k-vertex template, 2M-triangle target, 10,000 nodes, route B",
+        "fp64_reductions": {"seconds_capped": shipped["capped_seconds"], "seconds_k8": shipped["k8_seconds"],
+                            "level_energies": _level_energies(str(shipped["capped_report"]))},
+        "fp32_reductions": {"seconds_capped": float(variant["capped_seconds"]),
+                            "seconds_k8": float(variant["k8_seconds"]),
+                            "level_energies": _level_energies(str(variant["capped_report"]))},
+        "max_difference_between_them": float(np.abs(p - q).max()),
+        "written": str(args.precision)}), flush=True)
+
+
+def run_precision_variant(args) -> None:
+    out = _precision_solve(args.seed)
+    np.savez(args.precision_variant, **out)
+
+
+def run_precision_compare(args) -> None:
+    """The reference's FP64 route A (oracle/_ref) on config 5 at its caps, on
+    this host's CPU, against the GPU results in the --precision file."""
+    from nricp_b200 import synthetic as S
+    from oracle.oracle import Oracle
+
+    gpu = np.load(args.precision_compare, allow_pickle=False)
+    case = S.config5(int(gpu["seed"]))
+    t0 = time.perf_counter()
+    ref = Oracle("reference").solve(*case.args(), **reference_options(case.options))
+    seconds = time.perf_counter() - t0
+    p = case.target_points
+    diag = float(np.linalg.norm(p.max(0) - p.min(0)))
+    ref_v = ref["vertices"]
+    ref_e = json.loads(ref["report"])["energy"]["total"]
+    line = {"workload": "config 5 at the reference's caps (k=4, 4-NN): GPU route B against the "
+                        "reference's FP64 route A",
+            "route_a": {"seconds": seconds, "level_energies": _level_energies(ref["report"]),
+                        "final_energy": ref_e}}
+    for name in ("fp64_reductions", "fp32_reductions"):
+        v = gpu[f"{name}_capped_vertices"]
+        err = np.linalg.norm(v - ref_v, axis=1) / diag
+        report = str(gpu[f"{name}_capped_report"])
+        e = json.loads(report)["energy"]["total"]
+        line[name] = {"max_vertex_error_over_diag": float(err.max()),
+                      "rms_vertex_error_over_diag": float(np.sqrt(np.mean(err ** 2))),
+                      "final_energy_rel_error": abs(e - ref_e) / abs(ref_e) if ref_e else abs(e),
+                      "level_energies": _level_energies(report)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.precision_variant:
+        return run_precision_variant(args)
+    if args.precision_compare:
+        return run_precision_compare(args)
+    if args.precision:
+        return run_precision(args)
     ranks = Ranks(args.gpus)
     try:
         if args.impl == "reference":

@@ -10,7 +10,10 @@ from pathlib import Path
 from . import _abi
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "libnricp_b200.so"
+# NRICP_B200_LIBRARY may name another build of the same library (the
+# measurement variant of build.build_fp32_reductions); it is never built here.
+LIB_PATH = Path(os.environ["NRICP_B200_LIBRARY"]) if os.environ.get("NRICP_B200_LIBRARY") else \
+    _HERE / "libnricp_b200.so"
 _lib: C.CDLL | None = None
 
 
@@ -22,7 +25,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    if not LIB_PATH.exists() and build_if_missing and os.environ.get("NRICP_NO_BUILD") != "1":
+    if (not LIB_PATH.exists() and build_if_missing and os.environ.get("NRICP_NO_BUILD") != "1"
+            and not os.environ.get("NRICP_B200_LIBRARY")):
         from . import build as _build  # compiles with nvcc for sm_100a
         _build.build()
     if not LIB_PATH.exists():

@@ -36,14 +36,23 @@ def _stale() -> bool:
     return any(p.stat().st_mtime > built for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not _stale():
-        return LIB
-    build_dir = HERE / "_build"
-    build_dir.mkdir(exist_ok=True)
+# A measurement-only variant: the solve's reductions rounded to FP32
+# (NRICP_FP32_REDUCTIONS in wrap_kernels.cu), for the precision comparison of
+# `bench.py --precision`.  Loaded only when NRICP_B200_LIBRARY points at it.
+FP32_REDUCTIONS_LIB = HERE / "variants" / "fp32_reductions" / "libnricp_b200.so"
+
+
+def build(force: bool = False, verbose: bool = False, defines: tuple = (), lib: Path | None = None,
+          build_dir: Path | None = None) -> Path:
+    lib = lib or LIB
+    if not force and not defines and not _stale():
+        return lib
+    build_dir = build_dir or HERE / "_build"
+    build_dir.mkdir(parents=True, exist_ok=True)
+    lib.parent.mkdir(parents=True, exist_ok=True)
     objects = []
     common = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp"]
+              "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp", *[f"-D{d}" for d in defines]]
     for source in SOURCES:
         obj = build_dir / (Path(source).stem + ".o")
         cmd = [nvcc(), *common, "-c", str(CSRC / source), "-o", str(obj)]
@@ -53,11 +62,16 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             cmd.append("-Xptxas=-v")
         subprocess.run(cmd, check=True)
         objects.append(str(obj))
-    tmp = LIB.with_suffix(f".so.{os.getpid()}")
+    tmp = lib.with_suffix(f".so.{os.getpid()}")
     subprocess.run([nvcc(), *ARCH, "-shared", *objects, "-o", str(tmp), "-Xcompiler", "-fopenmp",
                     "-lcudart"], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
+
+
+def build_fp32_reductions() -> Path:
+    return build(force=True, defines=("NRICP_FP32_REDUCTIONS",), lib=FP32_REDUCTIONS_LIB,
+                 build_dir=HERE / "_build_fp32_reductions")
 
 
 if __name__ == "__main__":

@@ -697,6 +697,22 @@ __device__ inline void solve6(const float* l, const double* rhs, double* x) {
 // segment, never the order of any sum: a wrap's solve is bit-identical for
 // every cluster size, and with it alone and in any batch.
 constexpr int kSegNodes = 8;
+
+// The solve's reductions -- the dot products, the residual norm, the Krylov
+// scalars and the x and r vectors -- are FP64.  A build with
+// NRICP_FP32_REDUCTIONS defined rounds every one of those operations to FP32
+// instead (each FP64 result of a sum or product of FP32 values rounded to
+// FP32 is the correctly rounded FP32 result): a variant for measuring what
+// the FP64 reductions buy, never the shipped library.
+#ifdef NRICP_FP32_REDUCTIONS
+__device__ __forceinline__ double rnd(double x) { return (double)__double2float_rn(x); }
+#else
+__device__ __forceinline__ double rnd(double x) { return x; }
+#endif
+__device__ __forceinline__ double warp_sum_rnd(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = rnd(v + __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
 constexpr int kPcgWarps = kPcgThreads / 32;
 constexpr int kPcgOwnFloats = 78;  // per owned node: X, R (2 x 6 FP64) + Minv 36 + P, S, W 18
 constexpr int kPcgMaxSmemBytes = 225 * 1024;
@@ -939,13 +955,13 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
                 Wv[i] = y;
                 const double ui = (double)un[r];
                 const double ri = R[i];
-                g += ri * ui;
-                d += (double)y * ui;
-                rr += ri * ri;
+                g = rnd(g + rnd(ri * ui));
+                d = rnd(d + rnd((double)y * ui));
+                rr = rnd(rr + rnd(ri * ri));
             }
-            g = warp_sum(g);
-            d = warp_sum(d);
-            rr = warp_sum(rr);
+            g = warp_sum_rnd(g);
+            d = warp_sum_rnd(d);
+            rr = warp_sum_rnd(rr);
             if (lane < ranks) {  // lane q stores the partials in CTA q's slots
                 double* dst = cluster.map_shared_rank(slots, lane) + 3 * seg;
                 dst[0] = g;
@@ -958,19 +974,19 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
         {
             double g = 0.0, d = 0.0, rr = 0.0;
             for (int sg = threadIdx.x; sg < segs; sg += blockDim.x) {
-                g += slots[3 * sg];
-                d += slots[3 * sg + 1];
-                rr += slots[3 * sg + 2];
+                g = rnd(g + slots[3 * sg]);
+                d = rnd(d + slots[3 * sg + 1]);
+                rr = rnd(rr + slots[3 * sg + 2]);
             }
-            g = warp_sum(g);
-            d = warp_sum(d);
-            rr = warp_sum(rr);
+            g = warp_sum_rnd(g);
+            d = warp_sum_rnd(d);
+            rr = warp_sum_rnd(rr);
             if (lane == 0) { red[0][warp] = g; red[1][warp] = d; red[2][warp] = rr; }
             __syncthreads();
             if (warp == 0) {
                 for (int k = 0; k < 3; ++k) {
                     double v = lane < kPcgWarps ? red[k][lane] : 0.0;
-                    v = warp_sum(v);
+                    v = warp_sum_rnd(v);
                     if (lane == 0) tot[k] = v;
                 }
             }
@@ -978,26 +994,26 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
         }
         const double gamma = tot[0], delta = tot[1], rr_total = tot[2];
         if (it == 0) {
-            bnorm = sqrt(rr_total);
+            bnorm = rnd(sqrt(rr_total));
             if (!(bnorm > 0.0)) { converged = true; residual = 0.0; break; }
         }
-        residual = sqrt(rr_total) / bnorm;
+        residual = rnd(rnd(sqrt(rr_total)) / bnorm);
         if (residual <= tolerance) { converged = true; break; }
         if (it >= max_iterations) break;
-        const double beta = it == 0 ? 0.0 : gamma / gamma_prev;
-        const double denominator = it == 0 ? delta : delta - beta * gamma / alpha_prev;
+        const double beta = it == 0 ? 0.0 : rnd(gamma / gamma_prev);
+        const double denominator = it == 0 ? delta : rnd(delta - rnd(rnd(beta * gamma) / alpha_prev));
         if (!(fabs(denominator) > 1e-300)) break;
-        const double alpha = gamma / denominator;
+        const double alpha = rnd(gamma / denominator);
         gamma_prev = gamma;
         alpha_prev = alpha;
         // ---- p, s, x, r for the owned rows; then u = M^-1 r, shared ----
         for (int i = threadIdx.x; i < rows; i += blockDim.x) {
-            const float pn = (float)((double)U[n0 * 6 + i] + beta * (double)P[i]);
-            const float sn = (float)((double)Wv[i] + beta * (double)S[i]);
+            const float pn = (float)((double)U[n0 * 6 + i] + rnd(beta * (double)P[i]));
+            const float sn = (float)((double)Wv[i] + rnd(beta * (double)S[i]));
             P[i] = pn;
             S[i] = sn;
-            X[i] += alpha * (double)pn;
-            R[i] -= alpha * (double)sn;
+            X[i] = rnd(X[i] + rnd(alpha * (double)pn));
+            R[i] = rnd(R[i] - rnd(alpha * (double)sn));
         }
         __syncthreads();
         precondition_and_share();
