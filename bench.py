@@ -93,6 +93,8 @@ def parse_args():
                    help="Poisson arrival rates (requests/s) of the serving windows")
     p.add_argument("--serve-seconds", type=float, default=6.0,
                    help="length of each serving window (the full protocol: 60)")
+    p.add_argument("--serve-large", type=float, default=0.1,
+                   help="fraction of requests drawn from the large (100k-vertex, 2M-triangle) cases")
     return p.parse_args()
 
 
@@ -337,10 +339,12 @@ def flush_l2():
     del buf
 
 
-def serve_window(server, cases, rate: float, seconds: float, rng) -> dict:
-    """Requests drawn from `cases` arriving as a Poisson process at `rate`
-    per second for `seconds`; latency is submit to result ready."""
+def serve_window(server, cases, rate: float, seconds: float, rng, large=(), large_fraction=0.0) -> dict:
+    """Requests drawn from `cases` (a `large_fraction` of them from `large`)
+    arriving as a Poisson process at `rate` per second for `seconds`; latency
+    is submit to result ready."""
     submitted = []
+    large_count = 0
     t0 = time.perf_counter()
     t = 0.0
     while True:
@@ -350,7 +354,11 @@ def serve_window(server, cases, rate: float, seconds: float, rng) -> dict:
         delay = t0 + t - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        c = cases[int(rng.integers(len(cases)))]
+        if large and rng.random() < large_fraction:
+            c = large[int(rng.integers(len(large)))]
+            large_count += 1
+        else:
+            c = cases[int(rng.integers(len(cases)))]
         submitted.append((time.perf_counter(), server.submit(*c.args(), **c.options)))
     latencies, finished = [], []
     for ts, rid in submitted:
@@ -361,29 +369,40 @@ def serve_window(server, cases, rate: float, seconds: float, rng) -> dict:
         latencies.append(1000.0 * latency)
         finished.append(ts + latency)
     span = max(finished) - submitted[0][0] if submitted else 0.0
-    out = {"rate_per_s": rate, "seconds": seconds, "requests": len(submitted),
+    out = {"rate_per_s": rate, "seconds": seconds, "requests": len(submitted), "large_requests": large_count,
            "wraps_per_second": len(submitted) / span if span > 0 else 0.0}
     out.update({f"latency_{k}_ms": v for k, v in percentiles(latencies).items() if k != "n"})
     return out
 
 
-def run_serving(dp, cases, rates, seconds, seed) -> dict:
+def large_requests(seed: int, count: int = 2):
+    """Config 4's large requests: 100k-vertex templates onto 2M-triangle
+    targets with 10,000 nodes, generated as in config 2."""
+    from nricp_b200 import synthetic as S
+
+    return [S.config2(seed=10_000 + seed * 10 + i, vertex_count=100_000, triangle_count=2_000_000,
+                      nodes_finest=10_000, k=6, levels=4) for i in range(count)]
+
+
+def run_serving(dp, cases, rates, seconds, seed, large=(), large_fraction=0.0) -> dict:
     budget = 120 * 10**9
     with dp.WrapServer(memory_budget_bytes=budget, max_slots=64) as server:
         # warm: every template's graph cached, the launch shape captured
-        for rid in [server.submit(*c.args(), **c.options) for c in cases]:
+        for rid in [server.submit(*c.args(), **c.options) for c in list(cases) + list(large)]:
             server.result(rid, timeout=900.0)
         rng = np.random.default_rng(seed)
         windows = []
         for r in rates:
             before = server.stats()
-            windows.append(serve_window(server, cases, r, seconds, rng))
+            windows.append(serve_window(server, cases, r, seconds, rng, large, large_fraction))
             after = server.stats()
             windows[-1]["ticks"] = after["ticks"] - before["ticks"]
             windows[-1]["tick_device_s"] = after["busy_seconds"] - before["busy_seconds"]
         stats = server.stats()
-    return {"workload": "Poisson arrivals drawn from the 64 config-3 wraps, continuous batching, "
-                        "64 resident slots, 120 GB admission budget",
+    return {"workload": ("Poisson arrivals drawn from the 64 config-3 wraps" +
+                         (f" and, with probability {large_fraction:g}, from {len(large)} large requests "
+                          "(100k-vertex template, 2M-triangle target, 10,000 nodes)" if large else "") +
+                         ", continuous batching, 64 resident slots, 120 GB admission budget"),
             "windows": windows, "graph_captures": stats["captures"],
             "peak_resident_gb": stats["peak_resident_bytes"] / 1e9}
 
@@ -497,7 +516,8 @@ def run_ours(args, ranks):
     served = None
     if ranks.rank == 0 and not args.no_serve:
         rates = [float(x) for x in args.serve_rates.split(",") if x]
-        served = run_serving(dp, cases, rates, args.serve_seconds, args.seed)
+        large = large_requests(args.seed) if args.serve_large > 0 else []
+        served = run_serving(dp, cases, rates, args.serve_seconds, args.seed, large, args.serve_large)
         served["vs_plain"] = {f"{w['rate_per_s']:g}/s": w["wraps_per_second"] / plain
                               for w in served["windows"]}
 

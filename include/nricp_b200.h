@@ -292,6 +292,12 @@ typedef struct NricpServerConfig {
                                     when the running wraps would need more than three CTAs per
                                     SM; -s (1..4) latency classes always halved s times */
     int ticks_per_poll;          /* ticks launched between looks at the wraps' progress */
+    int large_face_threshold;    /* requests whose target has at least this many triangles run
+                                    in a lane of their own, with its own slots, stream and
+                                    ticks, so that they do not slow the others' ticks; 0: one
+                                    lane for all (default 1,000,000) */
+    int large_slots;             /* slots of the large lane (default 8); it gets a third of the
+                                    memory budget */
 } NricpServerConfig;
 typedef struct NricpServerStats {
     long submitted, completed, failed, waiting, running;

@@ -134,6 +134,7 @@ class ServerConfig(C.Structure):
     _fields_ = [
         ("memory_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("prep_threads", C.c_int),
         ("pcg_cluster", C.c_int), ("ticks_per_poll", C.c_int),
+        ("large_face_threshold", C.c_int), ("large_slots", C.c_int),
     ]
 
 

@@ -5,8 +5,11 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -507,9 +510,24 @@ int nricp_lbvh_export(const double* target_points, int vertex_count, const int32
 
 // ---- serving -------------------------------------------------------------
 
+// One or two lanes: a lane is a Server (own slots, stream, ticks and memory
+// pool).  Every tick of a lane runs in lockstep, so a request whose target
+// has a million triangles would slow every smaller request sharing its
+// ticks; large requests therefore get a lane of their own, whose ticks run
+// beside the other lane's on the device.  Request ids are the composite's.
 struct NricpServer {
-    explicit NricpServer(const NricpServerConfig& c) : server(c) {}
-    Server server;
+    std::vector<std::unique_ptr<Server>> lanes;  // [0] regular, [1] large (if any)
+    int large_faces = 0;
+    std::mutex mu;
+    std::map<long, std::pair<int, long>> ids;  // id -> (lane, the lane's id)
+    long next_id = 1;
+
+    std::pair<int, long> find(long id) {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = ids.find(id);
+        if (it == ids.end()) throw InvalidArgument("unknown request id " + std::to_string(id));
+        return it->second;
+    }
 };
 
 void nricp_server_default_config(NricpServerConfig* c) {
@@ -518,6 +536,8 @@ void nricp_server_default_config(NricpServerConfig* c) {
     c->prep_threads = 0;
     c->pcg_cluster = 0;
     c->ticks_per_poll = 8;
+    c->large_face_threshold = 1000000;
+    c->large_slots = 8;
 }
 
 int nricp_server_create(const NricpServerConfig* config, NricpServer** out) {
@@ -527,31 +547,86 @@ int nricp_server_create(const NricpServerConfig* config, NricpServer** out) {
         NricpServerConfig c;
         nricp_server_default_config(&c);
         if (config) c = *config;
-        *out = new NricpServer(c);
+        if (c.large_face_threshold < 0) throw InvalidArgument("large_face_threshold must be >= 0");
+        auto s = std::make_unique<NricpServer>();
+        if (c.large_face_threshold == 0) {
+            s->lanes.push_back(std::make_unique<Server>(c));
+        } else {
+            if (c.large_slots <= 0 || c.large_slots > 1024)
+                throw InvalidArgument("large_slots is " + std::to_string(c.large_slots) + "; it must be 1 to 1024");
+            size_t budget = c.memory_budget_bytes;
+            if (budget == 0) {
+                size_t free_bytes = 0, total = 0;
+                check(cudaMemGetInfo(&free_bytes, &total), "cudaMemGetInfo");
+                budget = free_bytes / 10 * 9;
+            }
+            const int cores = static_cast<int>(std::thread::hardware_concurrency());
+            NricpServerConfig regular = c, large = c;
+            regular.memory_budget_bytes = budget - budget / 3;
+            large.memory_budget_bytes = budget / 3;
+            large.max_slots = c.large_slots;
+            if (c.prep_threads <= 0) {
+                regular.prep_threads = std::max(1, cores / 2 - std::max(1, cores / 8));
+                large.prep_threads = std::max(1, cores / 8);
+            }
+            s->lanes.push_back(std::make_unique<Server>(regular));
+            s->lanes.push_back(std::make_unique<Server>(large));
+            s->large_faces = c.large_face_threshold;
+        }
+        *out = s.release();
     });
 }
 
 int nricp_server_submit(NricpServer* s, const NricpSolveDesc* desc, long* id) {
-    return guarded([&] { *id = s->server.submit(*desc); });
+    return guarded([&] {
+        const int lane = s->lanes.size() > 1 && desc && desc->target_face_count >= s->large_faces ? 1 : 0;
+        const long inner = s->lanes[lane]->submit(*desc);
+        std::lock_guard<std::mutex> lk(s->mu);
+        *id = s->next_id++;
+        s->ids[*id] = {lane, inner};
+    });
 }
 
 int nricp_server_poll(NricpServer* s, long id, int* status, double* latency_seconds) {
-    return guarded([&] { *status = s->server.poll(id, latency_seconds); });
+    return guarded([&] {
+        const auto [lane, inner] = s->find(id);
+        *status = s->lanes[lane]->poll(inner, latency_seconds);
+    });
 }
 
 int nricp_server_wait(NricpServer* s, long id, double timeout_seconds) {
     return guarded([&] {
-        if (!s->server.wait(id, timeout_seconds))
+        const auto [lane, inner] = s->find(id);
+        if (!s->lanes[lane]->wait(inner, timeout_seconds))
             throw TimeoutError("request " + std::to_string(id) + " did not finish in time");
     });
 }
 
 int nricp_server_result(NricpServer* s, long id, NricpResult* out) {
-    return guarded([&] { s->server.result(id, out); });
+    return guarded([&] {
+        const auto [lane, inner] = s->find(id);
+        double latency = 0.0;
+        const int state = s->lanes[lane]->poll(inner, &latency);
+        auto forget = [&] {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->ids.erase(id);
+        };
+        try {
+            s->lanes[lane]->result(inner, out);
+        } catch (...) {
+            if (state == NRICP_REQUEST_FAILED) forget();  // the lane has forgotten it too
+            throw;
+        }
+        forget();
+    });
 }
 
 int nricp_server_stats(NricpServer* s, NricpServerStats* out) {
-    return guarded([&] { *out = s->server.stats(); });
+    return guarded([&] {
+        std::vector<Server*> lanes;
+        for (auto& lane : s->lanes) lanes.push_back(lane.get());
+        *out = Server::merged_stats(lanes);
+    });
 }
 
 void nricp_server_destroy(NricpServer* s) { delete s; }

@@ -1913,6 +1913,42 @@ void Server::result(long id, NricpResult* out) {
     m.requests.erase(it);
 }
 
+NricpServerStats Server::merged_stats(const std::vector<Server*>& servers) {
+    if (servers.size() == 1) return servers[0]->stats();
+    NricpServerStats s{};
+    std::vector<double> latencies, queue_waits;
+    double first = -1.0, last = 0.0;
+    for (Server* server : servers) {
+        Impl& m = *server->impl_;
+        std::lock_guard<std::mutex> lk(m.mu);
+        s.submitted += m.submitted;
+        s.completed += m.completed;
+        s.failed += m.failed;
+        s.running += m.running;
+        s.waiting += static_cast<long>(m.prep_queue.size() + m.ready.size() + m.loaded.size()) + m.loading;
+        latencies.insert(latencies.end(), m.latencies.begin(), m.latencies.end());
+        queue_waits.insert(queue_waits.end(), m.queue_waits.begin(), m.queue_waits.end());
+        if (m.first_submit >= 0.0) first = first < 0.0 ? m.first_submit : std::min(first, m.first_submit);
+        last = std::max(last, m.last_done);
+        s.ticks += m.ticks;
+        s.launches += m.launches;
+        s.captures += m.captures;
+        s.busy_seconds += m.busy_seconds;
+        s.resident_bytes += m.resident;
+        s.peak_resident_bytes += m.peak;
+        s.slots_used += m.slots_used;
+    }
+    s.latency_p50_ms = 1000.0 * percentile(latencies, 0.50);
+    s.latency_p99_ms = 1000.0 * percentile(latencies, 0.99);
+    double sum = 0.0;
+    for (double x : latencies) sum += x;
+    s.latency_mean_ms = latencies.empty() ? 0.0 : 1000.0 * sum / latencies.size();
+    s.queue_p50_ms = 1000.0 * percentile(queue_waits, 0.50);
+    const double span = last - first;
+    s.wraps_per_second = first >= 0.0 && span > 0.0 ? s.completed / span : 0.0;
+    return s;
+}
+
 NricpServerStats Server::stats() {
     Impl& m = *impl_;
     std::lock_guard<std::mutex> lk(m.mu);

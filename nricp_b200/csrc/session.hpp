@@ -138,6 +138,9 @@ public:
     bool wait(long id, double timeout_seconds);
     void result(long id, NricpResult* out);
     NricpServerStats stats();
+    // Statistics of several servers as one (latency percentiles over all of
+    // their requests; peak residency is the sum of the peaks).
+    static NricpServerStats merged_stats(const std::vector<Server*>& servers);
 
     struct Impl;
 

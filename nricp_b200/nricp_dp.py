@@ -167,7 +167,8 @@ class WrapServer:
     it.  Each result is bit-identical to the same wrap solved alone."""
 
     def __init__(self, memory_budget_bytes: int = 0, max_slots: int = 64,
-                 prep_threads: int = 0, pcg_cluster: int = 0, ticks_per_poll: int = 8):
+                 prep_threads: int = 0, pcg_cluster: int = 0, ticks_per_poll: int = 8,
+                 large_face_threshold: int = 1_000_000, large_slots: int = 8):
         cfg = _abi.ServerConfig()
         load().nricp_server_default_config(C.byref(cfg))
         cfg.memory_budget_bytes = int(memory_budget_bytes)
@@ -175,6 +176,8 @@ class WrapServer:
         cfg.prep_threads = int(prep_threads)
         cfg.pcg_cluster = int(pcg_cluster)
         cfg.ticks_per_poll = int(ticks_per_poll)
+        cfg.large_face_threshold = int(large_face_threshold)
+        cfg.large_slots = int(large_slots)
         self._handle = C.c_void_p()
         check(load().nricp_server_create(C.byref(cfg), C.byref(self._handle)))
         self._plans: dict[int, tuple[int, list[int]]] = {}

@@ -60,6 +60,22 @@ def test_served_results_equal_the_wraps_solved_alone(dp, device, route, cluster)
     assert stats["latency_p99_ms"] >= stats["latency_p50_ms"] > 0.0
 
 
+def test_large_requests_run_in_their_own_lane(dp, device):
+    # a threshold that sends two of the cases to the large lane: every result
+    # is still the wrap solved alone
+    cases = _cases()
+    alone = [dp.solve_route_b(*c.args(), **c.options) for c in cases]
+    faces = sorted(len(c.target_faces) for c in cases)
+    with dp.WrapServer(max_slots=8, large_face_threshold=faces[-2], large_slots=2) as server:
+        ids = [server.submit(*c.args(), **c.options) for c in cases]
+        served = [server.result(i, timeout=120.0) for i in ids]
+        stats = server.stats()
+    for a, s in zip(alone, served):
+        _same(a, s)
+    assert stats["completed"] == len(cases) and stats["failed"] == 0
+    assert stats["latency_p99_ms"] >= stats["latency_p50_ms"] > 0.0
+
+
 def test_one_slot_serialises_the_requests(dp, device):
     cases = _cases()[:3]
     alone = [dp.solve_route_b(*c.args(), **c.options) for c in cases]
