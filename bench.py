@@ -625,17 +625,42 @@ def run_precision_variant(args) -> None:
     np.savez(args.precision_variant, **out)
 
 
-def run_precision_compare(args) -> None:
-    """The reference's FP64 route A (oracle/_ref) on config 5 at its caps, on
-    this host's CPU, against the GPU results in the --precision file."""
+def _route_a_config5(job):
+    """The reference's FP64 route A on config 5 at its caps, in a worker; with
+    `sigma` > 0 the template is first perturbed by N(0, sigma) per coordinate
+    (relative to the target's diagonal) -- the problem's own sensitivity."""
+    seed, sigma = job
+    sys.path.insert(0, str(ROOT))
     from nricp_b200 import synthetic as S
     from oracle.oracle import Oracle
 
-    gpu = np.load(args.precision_compare, allow_pickle=False)
-    case = S.config5(int(gpu["seed"]))
+    case = S.config5(seed)
+    points = case.template_points
+    if sigma > 0.0:
+        p = case.target_points
+        diag = float(np.linalg.norm(p.max(0) - p.min(0)))
+        points = points + np.random.default_rng(seed + 1).normal(0.0, sigma * diag, size=points.shape)
     t0 = time.perf_counter()
-    ref = Oracle("reference").solve(*case.args(), **reference_options(case.options))
-    seconds = time.perf_counter() - t0
+    ref = Oracle("reference").solve(points, case.template_faces, case.target_points, case.target_faces,
+                                    case.level_settings, **reference_options(case.options))
+    return time.perf_counter() - t0, ref["vertices"], ref["report"]
+
+
+def run_precision_compare(args) -> None:
+    """The reference's FP64 route A (oracle/_ref) on config 5 at its caps, on
+    this host's CPU, against the GPU results in the --precision file; and
+    route A against itself on a template perturbed by 1e-9 of the diagonal."""
+    import multiprocessing as mp
+
+    from nricp_b200 import synthetic as S
+
+    gpu = np.load(args.precision_compare, allow_pickle=False)
+    seed = int(gpu["seed"])
+    case = S.config5(seed)
+    with mp.get_context("spawn").Pool(2) as pool:
+        (seconds, ref_vertices, ref_report), (_, pert_vertices, pert_report) = pool.map(
+            _route_a_config5, [(seed, 0.0), (seed, 1e-9)])
+    ref = {"vertices": ref_vertices, "report": ref_report}
     p = case.target_points
     diag = float(np.linalg.norm(p.max(0) - p.min(0)))
     ref_v = ref["vertices"]
@@ -644,6 +669,12 @@ def run_precision_compare(args) -> None:
                         "reference's FP64 route A",
             "route_a": {"seconds": seconds, "level_energies": _level_energies(ref["report"]),
                         "final_energy": ref_e}}
+    pert_err = np.linalg.norm(pert_vertices - ref_v, axis=1) / diag
+    pert_e = json.loads(pert_report)["energy"]["total"]
+    line["route_a_perturbed_1e-9"] = {"max_vertex_error_over_diag": float(pert_err.max()),
+                                      "rms_vertex_error_over_diag": float(np.sqrt(np.mean(pert_err ** 2))),
+                                      "final_energy_rel_error": abs(pert_e - ref_e) / abs(ref_e),
+                                      "level_energies": _level_energies(pert_report)}
     for name in ("fp64_reductions", "fp32_reductions"):
         v = gpu[f"{name}_capped_vertices"]
         err = np.linalg.norm(v - ref_v, axis=1) / diag

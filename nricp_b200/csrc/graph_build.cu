@@ -8,14 +8,19 @@
 // bindings, (distance, index) for the edges.  Only the scan orders differ,
 // and none of the rules depends on them.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <vector>
+
+#include <cooperative_groups.h>
 
 #include "graph_build.hpp"
 #include "session.hpp"
 #include "staging.hpp"
 
 namespace nricp_b200 {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -34,16 +39,17 @@ __device__ inline void arg_max(double& v, int& i, double ov, int oi) {
     if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
 }
 
-// One block per template: seeds[0] = 0, then repeatedly the point farthest
-// from all seeds so far (sampling.cpp:47-88).
+// One block per template (templates[blockIdx.x]): seeds[0] = 0, then
+// repeatedly the point farthest from all seeds so far (sampling.cpp:47-88).
 __global__ void __launch_bounds__(kFpsThreads) k_fps(const double* __restrict__ points,
                                                      const long* __restrict__ point_offset,
                                                      const int* __restrict__ point_count,
                                                      const int* __restrict__ seed_count,
                                                      const long* __restrict__ seed_offset,
+                                                     const int* __restrict__ templates,
                                                      double* __restrict__ nearest_all,
                                                      int* __restrict__ seeds_all) {
-    const int t = blockIdx.x;
+    const int t = templates[blockIdx.x];
     const int n = point_count[t];
     const int count = min(seed_count[t], n);
     if (n <= 0 || count <= 0) return;
@@ -100,6 +106,105 @@ __global__ void __launch_bounds__(kFpsThreads) k_fps(const double* __restrict__ 
         }
         best = block_arg_max(bv, bi);
     }
+}
+
+// The same seeds from one thread-block cluster per template
+// (templates[blockIdx.y]), for templates of at most kFpsClusterPoints
+// points: the points are split in contiguous chunks over the cluster's CTAs,
+// and every thread keeps up to four points and their distances to the
+// nearest seed in registers.  Per seed: the thread's, the warp's and the
+// CTA's farthest point, then every CTA writes its candidate into every CTA's
+// shared slots (distributed shared memory, two sets used in turn), one
+// cluster barrier, and every CTA takes the same winner in rank order.  The
+// arithmetic and the tie rule (the larger distance, then the lower index) are
+// k_fps's, so the winner and the seeds are the same for any split.
+constexpr int kFpsClusterThreads = 1024;
+constexpr int kFpsPerThread = 4;
+constexpr int kFpsClusterPoints = 16 * kFpsClusterThreads * kFpsPerThread;  // 65,536
+
+struct FpsCandidate {
+    double v, x, y, z;
+    int i, pad;
+};
+
+__device__ inline void better(FpsCandidate& a, const FpsCandidate& b) {
+    if (b.v > a.v || (b.v == a.v && b.i < a.i)) a = b;
+}
+
+__device__ inline FpsCandidate shuffle(const FpsCandidate& c, int lane_mask) {
+    FpsCandidate o;
+    o.v = __shfl_xor_sync(0xffffffffu, c.v, lane_mask);
+    o.x = __shfl_xor_sync(0xffffffffu, c.x, lane_mask);
+    o.y = __shfl_xor_sync(0xffffffffu, c.y, lane_mask);
+    o.z = __shfl_xor_sync(0xffffffffu, c.z, lane_mask);
+    o.i = __shfl_xor_sync(0xffffffffu, c.i, lane_mask);
+    o.pad = 0;
+    return o;
+}
+
+__global__ void __launch_bounds__(kFpsClusterThreads) k_fps_cluster(const double* __restrict__ points,
+                                                                   const long* __restrict__ point_offset,
+                                                                   const int* __restrict__ point_count,
+                                                                   const int* __restrict__ seed_count,
+                                                                   const long* __restrict__ seed_offset,
+                                                                   const int* __restrict__ templates,
+                                                                   int* __restrict__ seeds_all) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int t = templates[blockIdx.y];
+    const int n = point_count[t];
+    const int count = min(seed_count[t], n);
+    if (n <= 0 || count <= 0) return;  // the same for the whole cluster
+    const int rank = (int)cluster.block_rank(), ranks = (int)cluster.num_blocks();
+    const int chunk = (n + ranks - 1) / ranks;  // <= kFpsClusterThreads * kFpsPerThread
+    const int c0 = rank * chunk, c1 = min(n, c0 + chunk);
+    const double* p = points + point_offset[t] * 3;
+    int* seeds = seeds_all + seed_offset[t];
+    __shared__ FpsCandidate slots[2][16];
+    __shared__ FpsCandidate warp_best[kFpsClusterThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double px[kFpsPerThread], py[kFpsPerThread], pz[kFpsPerThread], near[kFpsPerThread];
+    int idx[kFpsPerThread];
+    for (int k = 0; k < kFpsPerThread; ++k) {
+        const int i = c0 + threadIdx.x + k * kFpsClusterThreads;
+        idx[k] = i < c1 ? i : -1;
+        px[k] = py[k] = pz[k] = near[k] = 0.0;
+        if (idx[k] >= 0) {
+            px[k] = p[(long)i * 3];
+            py[k] = p[(long)i * 3 + 1];
+            pz[k] = p[(long)i * 3 + 2];
+        }
+    }
+    if (rank == 0 && threadIdx.x == 0) seeds[0] = 0;
+    double c[3] = {p[0], p[1], p[2]};
+    for (int s = 0;; ++s) {
+        FpsCandidate best{-1.0, 0.0, 0.0, 0.0, INT_MAX, 0};
+        for (int k = 0; k < kFpsPerThread; ++k) {
+            if (idx[k] < 0) continue;
+            const double q[3] = {px[k], py[k], pz[k]};
+            const double d = sq_rn(q, c);
+            const double m = s == 0 ? d : (near[k] < d ? near[k] : d);
+            near[k] = m;
+            better(best, FpsCandidate{m, px[k], py[k], pz[k], idx[k], 0});
+        }
+        if (s + 1 >= count) break;
+        for (int o = 16; o > 0; o >>= 1) better(best, shuffle(best, o));
+        if (lane == 0) warp_best[warp] = best;
+        __syncthreads();
+        if (warp == 0) {
+            best = warp_best[lane];  // 32 warps
+            for (int o = 16; o > 0; o >>= 1) better(best, shuffle(best, o));
+            if (lane < ranks) *cluster.map_shared_rank(&slots[s & 1][rank], lane) = best;
+        }
+        cluster.sync();
+        FpsCandidate win = slots[s & 1][0];
+        for (int r = 1; r < ranks; ++r) better(win, slots[s & 1][r]);
+        if (rank == 0 && threadIdx.x == 0) seeds[s + 1] = win.i;
+        c[0] = win.x;
+        c[1] = win.y;
+        c[2] = win.z;
+    }
+    // no CTA leaves while another may still write into its shared memory
+    cluster.sync();
 }
 
 // (sq, idx) kept sorted ascending, at most `capacity` entries, entries offered
@@ -324,8 +429,52 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
     };
     int* host_neigh = reinterpret_cast<int*>(lease.data() + seed_bytes + level_bytes * max_levels);
 
-    k_fps<<<W, kFpsThreads, 0, stream>>>(d_points, d_point_offset, d_point_count, d_seed_count,
-                                         d_seed_offset, d_nearest, d_seeds);
+    // seeds: a cluster of 1-16 CTAs per template (4,096 points per CTA), one
+    // launch per cluster size; a single block for templates beyond 65,536
+    // points
+    {
+        std::vector<std::vector<int>> by_size(5);
+        std::vector<int> single;
+        for (int t = 0; t < W; ++t) {
+            if (point_count[t] > kFpsClusterPoints) {
+                single.push_back(t);
+                continue;
+            }
+            int g = 0;
+            while ((1 << g) * kFpsClusterThreads * kFpsPerThread < point_count[t]) ++g;
+            by_size[g].push_back(t);
+        }
+        static const bool enabled = [] {
+            cudaFuncSetAttribute(k_fps_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            return true;
+        }();
+        (void)enabled;
+        for (int g = 0; g < 5; ++g) {
+            if (by_size[g].empty()) continue;
+            const int* d_templates = to_device(by_size[g], owned, stream);
+            cudaLaunchConfig_t config = {};
+            config.gridDim = dim3(1 << g, static_cast<unsigned>(by_size[g].size()));
+            config.blockDim = dim3(kFpsClusterThreads);
+            config.stream = stream;
+            cudaLaunchAttribute attribute[1];
+            attribute[0].id = cudaLaunchAttributeClusterDimension;
+            attribute[0].val.clusterDim.x = 1 << g;
+            attribute[0].val.clusterDim.y = 1;
+            attribute[0].val.clusterDim.z = 1;
+            config.attrs = attribute;
+            config.numAttrs = 1;
+            check(cudaLaunchKernelEx(&config, k_fps_cluster, (const double*)d_points, (const long*)d_point_offset,
+                                     (const int*)d_point_count, (const int*)d_seed_count,
+                                     (const long*)d_seed_offset, d_templates, d_seeds),
+                  "farthest-point seeds");
+        }
+        if (!single.empty()) {
+            const int* d_templates = to_device(single, owned, stream);
+            k_fps<<<static_cast<int>(single.size()), kFpsThreads, 0, stream>>>(
+                d_points, d_point_offset, d_point_count, d_seed_count, d_seed_offset, d_templates, d_nearest,
+                d_seeds);
+        }
+    }
     check(cudaGetLastError(), "farthest-point seeds");
     check(cudaMemcpyAsync(seeds, d_seeds, sizeof(int) * std::max<long>(1, total_seeds), cudaMemcpyDeviceToHost,
                           stream), "download seeds");

@@ -689,14 +689,16 @@ __device__ inline void solve6(const float* l, const double* rhs, double* x) {
 
 // ---- the solve's partition and shared-memory layout ------------------------
 //
-// Rows are grouped into segments of kSegNodes nodes (48 rows).  A segment is
+// Rows are grouped into segments of kSegNodes nodes (24 rows: one pass of a
+// warp; 4-node segments balance the warps better than 8-node ones, 0.90 s
+// against 0.93 s per 64-wrap batch, and 16-node ones are slower).  A segment is
 // the unit of ownership and of reduction: one warp forms the segment's FP64
 // partial dot products in a fixed lane order, and the cluster sums the
 // segments' partials in a fixed order.  A CTA owns a contiguous run of
 // segments, so the cluster size only decides which CTA computes which
 // segment, never the order of any sum: a wrap's solve is bit-identical for
 // every cluster size, and with it alone and in any batch.
-constexpr int kSegNodes = 8;
+constexpr int kSegNodes = 4;
 
 // The solve's reductions -- the dot products, the residual norm, the Krylov
 // scalars and the x and r vectors -- are FP64.  A build with
@@ -898,7 +900,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
 
     // u = M^-1 r for the owned rows into this CTA's copy, then the slice into
     // every other CTA's copy (16-byte stores; the slice starts on a segment,
-    // so at a multiple of 192 bytes)
+    // so at a multiple of 96 bytes)
     auto precondition_and_share = [&]() {
         for (int i = threadIdx.x; i < rows; i += blockDim.x) {
             const int m = i / 6, r = i - m * 6;
@@ -910,7 +912,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(const WrapDev* __restrict__
         if (place.u_shared && ranks > 1) {
             __syncthreads();
             const float4* src = reinterpret_cast<const float4*>(U + n0 * 6);
-            const int vec = rows / 4;  // rows = 6 * own, own a multiple of 8 except at the end
+            const int vec = rows / 4;  // rows = 6 * own, own a multiple of 4 except at the end
             for (int q = 1; q < ranks; ++q) {
                 const int dst_rank = (rank + q) % ranks;
                 float4* dst = reinterpret_cast<float4*>(cluster.map_shared_rank(U, dst_rank) + n0 * 6);
@@ -1723,7 +1725,7 @@ int tick_kernel_launches(const TickShape& s) {
 }
 
 // Cluster size of the solve for one wrap of `nodes` nodes on its own: a
-// power of two with about 128 nodes (16 segments, one per warp) per CTA, at
+// power of two with about 128 nodes (32 segments, two per warp) per CTA, at
 // most 16 CTAs (the non-portable maximum, enabled here).
 int pcg_latency_cluster(int nodes) {
     int ranks = 1;
