@@ -343,6 +343,15 @@ int nricp_template_graph_level(const double* points, int count, int levels,
                                int32_t* edges, int edge_capacity, int* edge_count,
                                int use_device);
 
+/* fit_rigid(source_points, target_points, weights) (bindings.cpp:857-883,
+ * src/core/deformation.cpp:86-139), on the device: the weighted rigid
+ * transform (reflections excluded) that best maps `count` source points onto
+ * their targets; weights below zero count as zero.  rotation: 9 doubles,
+ * row-major; translation: 3.  With no points or no positive weight, the
+ * identity and zero, as the reference.  Host pointers. */
+int nricp_fit_rigid(const double* source_points, const double* target_points, const double* weights,
+                    int count, double* rotation, double* translation);
+
 /* closest_points(...) (bindings.cpp:1004-1044 -> src/cuda/lbvh.cu:439-533):
  * nearest target point, interpolated normal, distance and triangle per query,
  * through the device hierarchy. */

@@ -395,6 +395,40 @@ int nricp_template_graph_level(const double* points, int count, int levels, int 
     });
 }
 
+int nricp_fit_rigid(const double* source_points, const double* target_points, const double* weights,
+                    int count, double* rotation, double* translation) {
+    return guarded([&] {
+        if (count < 0) throw InvalidArgument("fit_rigid expects (n, 3) point pairs and (n,) weights");
+        require_device();
+        const size_t n = static_cast<size_t>(count);
+        const size_t bytes = sizeof(double) * (7 * std::max<size_t>(1, n) + 12);
+        char* base = nullptr;
+        check(cudaMalloc(&base, bytes), "cudaMalloc(rigid fit)");
+        std::unique_ptr<char, void (*)(char*)> guard(base, [](char* p) { cudaFree(p); });
+        double* src = reinterpret_cast<double*>(base);
+        double* dst = src + 3 * std::max<size_t>(1, n);
+        double* w = dst + 3 * std::max<size_t>(1, n);
+        double* out = w + std::max<size_t>(1, n);
+        cudaStream_t stream;
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        std::unique_ptr<CUstream_st, void (*)(cudaStream_t)> stream_guard(stream, [](cudaStream_t s) {
+            cudaStreamDestroy(s);
+        });
+        if (n > 0) {
+            check(cudaMemcpyAsync(src, source_points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, stream), "upload");
+            check(cudaMemcpyAsync(dst, target_points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, stream), "upload");
+            check(cudaMemcpyAsync(w, weights, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload");
+        }
+        launch_fit_rigid(src, dst, w, count, out, stream);
+        check(cudaGetLastError(), "rigid fit");
+        double host[12];
+        check(cudaMemcpyAsync(host, out, sizeof host, cudaMemcpyDeviceToHost, stream), "download");
+        check(cudaStreamSynchronize(stream), "rigid fit");
+        std::memcpy(rotation, host, sizeof(double) * 9);
+        std::memcpy(translation, host + 9, sizeof(double) * 3);
+    });
+}
+
 int nricp_closest_points(const double* target_points, int vertex_count, const int32_t* faces,
                          int face_count, const double* queries, int query_count,
                          double* out_points, double* out_normals, double* out_distances,

@@ -74,6 +74,10 @@ int pcg_latency_cluster(int nodes);
 int pcg_cluster_size(int max_nodes, int wraps, int sm_count);
 int pcg_shared_bytes(const int* max_nodes, int wraps, int cluster);
 int pcg_max_nodes();
+// The weighted rigid fit of n point pairs (device arrays); out = R (row-major
+// 3x3), t.
+void launch_fit_rigid(const double* src, const double* dst, const double* weights, int n, double* out,
+                      cudaStream_t stream);
 void launch_evaluate_state(const WrapDev* wraps, const TickShape& shape, cudaStream_t stream);
 
 }  // namespace nricp_b200

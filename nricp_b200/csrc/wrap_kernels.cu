@@ -501,6 +501,52 @@ __device__ inline void horn_rotation(const double* S, double* R) {
 
 constexpr double kRotationRelaxation = 0.2;  // local_global.cu:18
 
+// The weighted rigid fit of point pairs (fit_rigid, deformation.cpp:86-139):
+// weights clamped at zero, weighted centroids, the covariance
+// sum w (p - cp)(q - cq)^T, the proper rotation that best maps the sources
+// onto the targets, and t = cq - R cp.  The reference takes the rotation
+// from an SVD with the reflection corrected; Horn's quaternion (the top
+// eigenvector of the 4x4 matrix built from the covariance, Jacobi in FP64)
+// is the same rotation.  One block, FP64 sums in a fixed order.
+constexpr int kRigidThreads = 1024;
+__global__ void __launch_bounds__(kRigidThreads) k_fit_rigid(const double* __restrict__ src,
+                                                            const double* __restrict__ dst,
+                                                            const double* __restrict__ weights, int n,
+                                                            double* __restrict__ out) {
+    __shared__ double scratch[33];
+    double sums[7] = {0, 0, 0, 0, 0, 0, 0};  // w, w p, w q
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double w = fmax(0.0, weights[i]);
+        sums[0] += w;
+        for (int k = 0; k < 3; ++k) {
+            sums[1 + k] += src[i * 3 + k] * w;
+            sums[4 + k] += dst[i * 3 + k] * w;
+        }
+    }
+    for (int k = 0; k < 7; ++k) sums[k] = block_sum<kRigidThreads>(sums[k], scratch);
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (!(sums[0] > 0.0)) {
+        if (threadIdx.x == 0)
+            for (int k = 0; k < 12; ++k) out[k] = k < 9 ? R[k] : 0.0;
+        return;
+    }
+    const double cp[3] = {sums[1] / sums[0], sums[2] / sums[0], sums[3] / sums[0]};
+    const double cq[3] = {sums[4] / sums[0], sums[5] / sums[0], sums[6] / sums[0]};
+    double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double w = fmax(0.0, weights[i]);
+        if (w == 0.0) continue;
+        for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q) S[r * 3 + q] += w * (src[i * 3 + r] - cp[r]) * (dst[i * 3 + q] - cq[q]);
+    }
+    for (int k = 0; k < 9; ++k) S[k] = block_sum<kRigidThreads>(S[k], scratch);
+    if (threadIdx.x == 0) {
+        horn_rotation(S, R);
+        for (int k = 0; k < 9; ++k) out[k] = R[k];
+        for (int r = 0; r < 3; ++r) out[9 + r] = cq[r] - (R[r * 3] * cp[0] + R[r * 3 + 1] * cp[1] + R[r * 3 + 2] * cp[2]);
+    }
+}
+
 // Warp per node: the correlation of the influences that mention the node
 // (bound vertices' data and landmark rows, edges it is the first endpoint of),
 // Horn's rotation, and the under-relaxed update into the candidate buffer.
@@ -1762,5 +1808,10 @@ int pcg_shared_bytes(const int* max_nodes, int wraps, int cluster) {
 }
 
 int pcg_max_nodes() { return 32768; }
+
+void launch_fit_rigid(const double* src, const double* dst, const double* weights, int n, double* out,
+                      cudaStream_t stream) {
+    k_fit_rigid<<<1, kRigidThreads, 0, stream>>>(src, dst, weights, n, out);
+}
 
 }  // namespace nricp_b200

@@ -459,5 +459,21 @@ def closest_points(target_points, target_faces, query_points) -> dict:
     return out
 
 
+def fit_rigid(source_points, target_points, weights) -> dict:
+    """Weighted rigid fit (reflection excluded) between point pairs, on the
+    device (bindings.cpp:857-883, deformation.cpp:86-139): the rotation (1, 3,
+    3) and translation (1, 3) that best map the sources onto the targets."""
+    s = np.ascontiguousarray(source_points, dtype=np.float64)
+    t = np.ascontiguousarray(target_points, dtype=np.float64)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    if (s.ndim != 2 or s.shape[1:] != (3,) or t.shape != s.shape or w.ndim != 1
+            or w.shape[0] != s.shape[0]):
+        raise ValueError("fit_rigid expects (n, 3) point pairs and (n,) weights")
+    rotation, translation = np.zeros((1, 3, 3)), np.zeros((1, 3))
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    check(load().nricp_fit_rigid(P(s), P(t), P(w), len(s), P(rotation), P(translation)))
+    return {"rotation": rotation, "translation": translation}
+
+
 def serialize_report(report: str) -> dict:
     return json.loads(report)

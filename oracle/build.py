@@ -103,6 +103,52 @@ def build_reference(force: bool = False) -> Path | None:
     return REF_LIB
 
 
+REF_GPU_LIB = REF_DIR / "libnricp_ref_gpu.so"
+_REF_CUDA_SOURCES = ["assemble.cu", "deform_ops.cu", "gpu_level.cu", "gpu_solver.cu", "graph_build.cu",
+                     "host_staging.cu", "lbvh.cu", "level_layout.cu", "local_global.cu", "pcg_solver.cu",
+                     "session.cu"]
+
+
+def build_reference_gpu(force: bool = False) -> Path | None:
+    """The reference's own GPU route B (src/cuda, compiled for sm_100a with
+    nvcc, as its CMake does with --extended-lambda) beside its host sources,
+    with this driver's ref_solve_route_b; None when the checkout is absent.
+    A timed comparison only, never a checker."""
+    src = reference_dir() / "src"
+    if not (src / "cuda" / "gpu_solver.cu").exists():
+        return REF_GPU_LIB if REF_GPU_LIB.exists() else None
+    REF_DIR.mkdir(exist_ok=True)
+    cuda_sources = [src / "cuda" / s for s in _REF_CUDA_SOURCES]
+    host_sources = [src / s for s in _REF_SOURCES]
+    own = [HERE / "ref" / "ref_driver.cpp", HERE / "ref" / "solve_direct.cpp", HERE / "block_cholesky.c"]
+    deps = cuda_sources + host_sources + own
+    if not (force or _stale(REF_GPU_LIB, deps)):
+        return REF_GPU_LIB
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    arch = ["-gencode", "arch=compute_100a,code=sm_100a"]
+    objects = []
+    for source in cuda_sources + host_sources + own:
+        obj = REF_DIR / ("gpu_" + source.parent.name + "_" + source.stem + ".o")
+        if source.suffix == ".c":
+            cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-std=gnu11", "-c", str(source), "-o", str(obj)]
+        elif source.suffix == ".cu":
+            cmd = [nvcc, *arch, "-O2", "-std=c++20", "--extended-lambda", "-Xcompiler", "-fPIC",
+                   f"-I{src}", "-c", str(source), "-o", str(obj)]
+        else:
+            cmd = ["g++", "-O2", "-ffp-contract=off", "-fPIC", "-std=c++20", "-DNRICP_REF_GPU", f"-I{src}",
+                   f"-I{HERE / 'ref' / 'eigen_shim'}", f"-I{HERE}", "-I/usr/local/cuda/include",
+                   "-c", str(source), "-o", str(obj)]
+        subprocess.run(cmd, check=True)
+        objects.append(str(obj))
+    tmp = REF_GPU_LIB.with_suffix(f".so.{os.getpid()}")
+    subprocess.run([nvcc, *arch, "-shared", *objects, "-o", str(tmp), "-lcudart"], check=True)
+    os.replace(tmp, REF_GPU_LIB)
+    for obj in objects:
+        Path(obj).unlink()
+    return REF_GPU_LIB
+
+
 if __name__ == "__main__":
     print(build_oracle(force=True))
     print(build_reference(force=True))
+    print(build_reference_gpu(force=True))

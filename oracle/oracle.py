@@ -45,6 +45,11 @@ def _load(kind: str) -> C.CDLL:
             if built is None:
                 raise FileNotFoundError("the reference's route A is not built here")
         prefix = "ref_"
+    elif kind == "reference_gpu":  # the reference's own GPU route B: a timed comparison, not a checker
+        path = build.REF_GPU_LIB
+        if not path.exists():
+            raise FileNotFoundError("the reference's GPU route B is not built here")
+        prefix = "ref_"
     else:
         raise ValueError(kind)
     lib = C.CDLL(str(path))
@@ -90,10 +95,11 @@ class Oracle:
         desc = _abi.Desc(template_points, template_faces, target_points, target_faces,
                          level_settings, route=0, **kwargs)
         out = _abi.ResultBuffers(desc.template_points.shape[0], desc.level_node_counts())
-        if self.kind == "reference":
+        if self.kind in ("reference", "reference_gpu"):
             if route != ROUTE_A:
                 raise ValueError("the reference has no CPU route C")
-            fn = self.lib.ref_solve_route_a
+            # the GPU build runs the reference's route B on the device instead
+            fn = self.lib.ref_solve_route_b if self.kind == "reference_gpu" else self.lib.ref_solve_route_a
             fn.argtypes = [C.POINTER(_abi.SolveDesc), C.POINTER(_abi.Result)]
             status = fn(C.byref(desc.struct), C.byref(out.struct))
             if status:

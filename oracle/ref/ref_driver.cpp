@@ -25,6 +25,9 @@
 #include "geometry/closest_point.h"
 #include "solver/fused_assembly.h"
 #include "solver/route_a.h"
+#ifdef NRICP_REF_GPU
+#include "cuda/gpu_solver.cuh"
+#endif
 
 #include "nricp_oracle.h"
 
@@ -57,11 +60,12 @@ void raise_if_invalid(const nricp::ValidationIssues& issues, const char* what) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-const char* ref_last_error(void) { return g_error.c_str(); }
-
-int ref_solve_route_a(const NricpSolveDesc* desc, NricpResult* out) {
+// prepare_solve (src/python/bindings.cpp:584-672) around one of the
+// reference's route functions, and route_result_to_dict's outputs.
+template <typename Route>
+int solve_with(const NricpSolveDesc* desc, NricpResult* out, Route route) {
     try {
         nricp::Mesh template_mesh{points_of(desc->template_points, desc->template_vertex_count),
                                   faces_of(desc->template_faces, desc->template_face_count)};
@@ -126,10 +130,11 @@ int ref_solve_route_a(const NricpSolveDesc* desc, NricpResult* out) {
         raise_if_invalid(nricp::validate_landmarks(
                              landmarks, static_cast<int>(normalized_template.vertices.size())),
                          "invalid landmarks");
-        const nricp::TargetQueries queries(normalized_target);
-        const nricp::RouteResult solved = nricp::solve_route_a(
-            normalized_template, queries, graph, settings,
-            mask.active.empty() ? nullptr : &mask, landmarks);
+        settings.pcg_tolerance = static_cast<float>(desc->pcg_tolerance);
+        settings.pcg_max_iterations = desc->pcg_max_iterations;
+        const nricp::RouteResult solved =
+            route(normalized_template, normalized_target, graph, settings,
+                  mask.active.empty() ? nullptr : &mask, landmarks);
 
         nricp::Mesh restored;
         restored.vertices = solved.vertices;
@@ -173,6 +178,33 @@ int ref_solve_route_a(const NricpSolveDesc* desc, NricpResult* out) {
         return NRICP_ERR_CUDA;
     }
 }
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+int ref_solve_route_a(const NricpSolveDesc* desc, NricpResult* out) {
+    return solve_with(desc, out, [](const nricp::Mesh& tpl, const nricp::Mesh& tgt, const nricp::TemplateGraph& graph,
+                                    const nricp::RouteSettings& settings, const nricp::VertexMask* mask,
+                                    const std::vector<nricp::Landmark>& landmarks) {
+        const nricp::TargetQueries queries(tgt);
+        return nricp::solve_route_a(tpl, queries, graph, settings, mask, landmarks);
+    });
+}
+
+#ifdef NRICP_REF_GPU
+// The reference's own GPU route B (src/cuda/gpu_solver.cu), in the GPU build
+// of this driver only.
+int ref_solve_route_b(const NricpSolveDesc* desc, NricpResult* out) {
+    return solve_with(desc, out, [](const nricp::Mesh& tpl, const nricp::Mesh& tgt, const nricp::TemplateGraph& graph,
+                                    const nricp::RouteSettings& settings, const nricp::VertexMask* mask,
+                                    const std::vector<nricp::Landmark>& landmarks) {
+        return nricp::solve_route_b(tpl, tgt, graph, settings, mask, landmarks);
+    });
+}
+#endif
 
 int ref_farthest_point_seeds(const double* points, int count, int seeds, int first,
                              int32_t* out) {
