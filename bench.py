@@ -204,6 +204,48 @@ def _reference_wrap(args):
     return seconds, result["vertices"], json.loads(result["report"])["energy"]["total"]
 
 
+def reference_gpu_sample(dp, cases, idx, route_a_vertices):
+    """The reference's own GPU route B (its src/cuda, compiled for sm_100a in
+    oracle/_ref) one wrap at a time on the CPU sample's wraps, beside this
+    engine on the same wraps and settings (the reference's caps), one at a
+    time and as one batch -- each through its public call from host arrays --
+    with both routes' errors against route A."""
+    from oracle.oracle import Oracle
+
+    try:
+        ref = Oracle("reference_gpu")
+    except (FileNotFoundError, OSError) as error:
+        return {"unavailable": str(error)}
+    same = [(*cases[i].args(), reference_options(cases[i].options)) for i in idx]
+    ref.solve(*same[0][:5], **same[0][5])  # warm: the reference's device set-up
+    t0 = time.perf_counter()
+    theirs = [ref.solve(*c[:5], **c[5]) for c in same]
+    ref_s = time.perf_counter() - t0
+    dp.solve_route_b(*same[0][:5], **same[0][5])
+    t0 = time.perf_counter()
+    ours_one = [dp.solve_route_b(*c[:5], **c[5]) for c in same]
+    ours_one_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    dp.solve_batch(same)
+    ours_batch_s = time.perf_counter() - t0
+
+    def worst(results):
+        out = 0.0
+        for i, r, a in zip(idx, results, route_a_vertices):
+            p = cases[i].target_points
+            out = max(out, float(np.abs(r["vertices"] - a).max()) / float(np.linalg.norm(p.max(0) - p.min(0))))
+        return out
+
+    n = len(same)
+    return {"sample": f"the CPU sample's {n} wraps, the reference's caps (k=4, 4-NN), host arrays in and out",
+            "reference_route_b_one_at_a_time": n / ref_s,
+            "ours_one_at_a_time": n / ours_one_s,
+            "ours_batched": n / ours_batch_s,
+            "unit": METRIC,
+            "max_vertex_error_over_diag_vs_route_a": {"reference_route_b": worst(theirs),
+                                                      "ours": worst(ours_one)}}
+
+
 def cpu_reference_sample(seed: int, cores: int) -> dict:
     """The sample's wraps, one per process (route A is single-threaded by
     construction), all at once: wraps/s of the host on that sample."""
@@ -489,7 +531,7 @@ def run_ours(args, ranks):
         roof, detail = roofline(batch, measured_peak())
 
     # ---- CPU reference sample and the fit against it ----
-    cpu, fit = None, None
+    cpu, fit, reference_gpu = None, None, None
     if ranks.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(args.seed, host_cores())
         idx = cpu.pop("indices")
@@ -511,6 +553,7 @@ def run_ours(args, ranks):
                "median_vertex_error_over_diag": errors[order[len(order) // 2]],
                "max_final_energy_rel_error": max(energy_errors),
                "wraps_within_1e-4": sum(1 for e in errors if e <= 1e-4)}
+        reference_gpu = reference_gpu_sample(dp, cases, idx, ref_vertices)
 
     # ---- serving: continuous batching under Poisson arrivals ----
     served = None
@@ -561,6 +604,7 @@ def run_ours(args, ranks):
         "kernels": detail,
         "served": served,
         "fit": fit,
+        "reference_gpu": reference_gpu,
         "cpu_baseline": cpu,
         "single_wrap": single,
     }
