@@ -86,6 +86,9 @@ def parse_args():
                    help="config 5 on the GPU with the shipped library and its FP32-reductions "
                         "variant; writes both results to OUT.npz")
     p.add_argument("--precision-variant", metavar="OUT.npz", help=argparse.SUPPRESS)
+    p.add_argument("--capture-steps", type=int, default=0,
+                   help="profiler captures: the config-2 wrap through RouteBSession for this many "
+                        "ticks, eager launches, nothing timed")
     p.add_argument("--precision-compare", metavar="IN.npz",
                    help="CPU only: the reference's FP64 route A on config 5, against the GPU "
                         "results of --precision")
@@ -731,8 +734,29 @@ def run_precision_compare(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_capture(args) -> None:
+    """A few hundred eager launches (one config-2 wrap, a few ticks) for
+    ncu: the tick graphs of the timed runs make every launch slow under a
+    profiler."""
+    import torch
+
+    from nricp_b200 import nricp_dp as dp
+    from nricp_b200 import synthetic as S
+
+    case = S.config2(args.seed)
+    session = dp.RouteBSession(*case.args(), **case.options)
+    for _ in range(args.capture_steps):
+        if session.finished():
+            break
+        session.step()
+    torch.cuda.synchronize()
+    print(json.dumps({"capture_steps": args.capture_steps, "ticks": session.ticks()[0]}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.capture_steps:
+        return run_capture(args)
     if args.precision_variant:
         return run_precision_variant(args)
     if args.precision_compare:
