@@ -48,8 +48,10 @@ __device__ inline int blocks_of_dev(long n, int threads) { return (int)((n + thr
 // the same reductions and the same partial slots, as that block of the full
 // grid, so results do not change.  need(w) gives the virtual blocks of wrap w
 // (0: none this tick); body(wrap index, x) runs one.  The launch gives
-// (wrap_count + 1) ints of dynamic shared memory.
-template <typename Need, typename Body>
+// (wrap_count + 1) ints of dynamic shared memory.  kShared: the body uses
+// shared memory, so the block meets at a barrier between virtual blocks;
+// bodies without it let each warp go on to the next virtual block at once.
+template <bool kShared, typename Need, typename Body>
 __device__ __forceinline__ void over_virtual_blocks(const WrapDev* __restrict__ wraps, int wrap_count, Need need,
                                                     Body body) {
     extern __shared__ int first[];  // each wrap's first virtual block
@@ -78,7 +80,7 @@ __device__ __forceinline__ void over_virtual_blocks(const WrapDev* __restrict__ 
             if (first[mid] <= vb) lo = mid; else hi = mid - 1;
         }
         body(lo, vb - first[lo]);
-        __syncthreads();  // shared memory of one virtual block before the next
+        if (kShared) __syncthreads();  // shared memory of one virtual block before the next
     }
 }
 
@@ -430,7 +432,7 @@ __device__ __forceinline__ void k_prologue_body(const WrapDev& w, int part, int 
 }
 
 __global__ void k_prologue(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -613,7 +615,7 @@ __device__ __forceinline__ void k_c_fit_body(const WrapDev& w, int part, int bx)
 }
 
 __global__ void k_c_fit(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -690,7 +692,7 @@ __device__ __forceinline__ void k_c_rhs_body(const WrapDev& w, int part, int bx)
 }
 
 __global__ void k_c_rhs(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1129,7 +1131,7 @@ __device__ __forceinline__ void k_evaluate_body(const WrapDev& w, int part, int 
 }
 
 __global__ void k_evaluate(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1159,7 +1161,7 @@ __device__ __forceinline__ void k_normals_body(const WrapDev& w, int part, int b
 }
 
 __global__ void k_normals(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1227,7 +1229,7 @@ __device__ __forceinline__ void k_residual_body(const WrapDev& w, int part, int 
 }
 
 __global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<true>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1374,7 +1376,7 @@ __device__ __forceinline__ void k_node_assemble_body(const WrapDev& w, int part,
 }
 
 __global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<true>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1452,7 +1454,7 @@ __device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part,
 }
 
 __global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1507,7 +1509,7 @@ __device__ __forceinline__ void k_edge_assemble_body(const WrapDev& w, int part,
 }
 
 __global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks(
+    over_virtual_blocks<true>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
