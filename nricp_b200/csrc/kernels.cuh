@@ -69,7 +69,9 @@ struct KernelTimers {
 
 void launch_tick(const WrapDev* wraps, const TickShape& shape, cudaStream_t stream,
                  KernelTimers* timers);
-int tick_kernel_launches(const TickShape& shape);
+// Kernels one tick launches (a timed tick runs its branches one after the
+// other, with one assembly).
+int tick_kernel_launches(const TickShape& shape, bool timed = false);
 int pcg_latency_cluster(int nodes);
 int pcg_cluster_size(int max_nodes, int wraps, int sm_count);
 int pcg_shared_bytes(const int* max_nodes, int wraps, int cluster);

@@ -757,7 +757,7 @@ void Batch::tick(KernelTimers* timers) {
     launch_tick(dev_wraps_, shape_, stream_, timers);
     check(cudaGetLastError(), "tick launch");
     ticks_ += 1;
-    launches_ += tick_kernel_launches(shape_);
+    launches_ += tick_kernel_launches(shape_, timers && timers->active);
 }
 
 void Batch::pull_controls() {
