@@ -216,7 +216,10 @@ def _faces(array, name: str) -> np.ndarray:
     out = np.asarray(array)
     if out.ndim != 2 or out.shape[1] != 3:
         raise ValueError(f"{name} must have shape (n, 3)")
-    return np.ascontiguousarray(out.astype(np.int64).astype(np.int32))
+    if out.dtype == np.int32:  # as the cast below would give, without copies
+        return np.ascontiguousarray(out)
+    # any other type through int64 (the reference's forcecast), then narrowed
+    return np.ascontiguousarray(np.asarray(out, dtype=np.int64).astype(np.int32))
 
 
 def _ptr(array: np.ndarray | None, ctype):

@@ -23,6 +23,7 @@ from __future__ import annotations
 import ctypes as C
 import json
 import math
+import os
 
 import numpy as np
 
@@ -68,12 +69,26 @@ def solve_route_c(template_points, template_faces, target_points, target_faces,
                   level_settings, **kwargs)
 
 
+def _descs(cases, route: str) -> list:
+    """The cases' descriptors; the array conversions (numpy copies, which
+    release the GIL) run on a few threads when there are many cases."""
+    def one(case):
+        return _abi.Desc(*case[:5], route=_ROUTES[route], **(case[5] if len(case) > 5 else {}))
+
+    cases = list(cases)
+    if len(cases) < 8:
+        return [one(c) for c in cases]
+    import concurrent.futures as cf
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
+        return list(pool.map(one, cases))
+
+
 def solve_batch(cases, route: str = "route_b") -> list[dict]:
     """Many wraps at once: every case is ``(template_points, template_faces,
     target_points, target_faces, level_settings, kwargs)``.  The wraps may
     differ in every size; they share the device launches."""
-    descs = [_abi.Desc(*case[:5], route=_ROUTES[route], **(case[5] if len(case) > 5 else {}))
-             for case in cases]
+    descs = _descs(cases, route)
     outs = [_abi.ResultBuffers(d.template_points.shape[0], _plan(d)) for d in descs]
     array = (_abi.SolveDesc * len(descs))(*[d.struct for d in descs])
     results = (_abi.Result * len(outs))(*[o.struct for o in outs])
@@ -87,8 +102,7 @@ class WrapBatch:
     call).  `cases` as for solve_batch."""
 
     def __init__(self, cases, route: str = "route_b"):
-        self._descs = [_abi.Desc(*case[:5], route=_ROUTES[route],
-                                 **(case[5] if len(case) > 5 else {})) for case in cases]
+        self._descs = _descs(cases, route)
         self._plans = [_plan(d) for d in self._descs]
         array = (_abi.SolveDesc * len(self._descs))(*[d.struct for d in self._descs])
         self._handle = C.c_void_p()
