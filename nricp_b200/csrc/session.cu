@@ -560,9 +560,14 @@ Batch::~Batch() {
     if (stream_) cudaStreamSynchronize(stream_);
     if (pool_) {  // back to the pool in stream order, without a device-wide wait
         for (auto& w : wraps_) w->arena.release_async(stream_);
-        if (lbvh_scratch_) cudaFreeAsync(lbvh_scratch_, stream_);
-        lbvh_scratch_ = nullptr;
+        for (int k = 0; k < kBuildStreams; ++k)
+            if (build_scratch_[k]) cudaFreeAsync(build_scratch_[k], stream_);
     }
+    for (int k = 0; k < kBuildStreams; ++k) {
+        if (build_streams_[k]) cudaStreamDestroy(build_streams_[k]);
+        if (build_done_[k]) cudaEventDestroy(build_done_[k]);
+    }
+    if (build_fork_) cudaEventDestroy(build_fork_);
     wraps_.clear();
     if (query_counter_) cudaFree(query_counter_);
     if (side_stream_) cudaStreamDestroy(side_stream_);
@@ -570,7 +575,6 @@ Batch::~Batch() {
     if (side_join_) cudaEventDestroy(side_join_);
     if (dev_wraps_) cudaFree(dev_wraps_);
     if (dev_controls_) cudaFree(dev_controls_);
-    if (lbvh_scratch_) cudaFree(lbvh_scratch_);
     if (pcg_index_) cudaFree(pcg_index_);
     for (int g = 0; g < 5; ++g) {
         if (pcg_streams_[g]) cudaStreamDestroy(pcg_streams_[g]);
@@ -683,7 +687,13 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
     check(cudaMallocHost(&host_controls_, sizeof(WrapControl) * W), "cudaMallocHost(controls)");
     size_t scratch_bytes = 0;
     for (const auto& w : wraps_) scratch_bytes = std::max(scratch_bytes, lbvh_scratch_bytes(w->F));
-    check(cudaMallocFromPoolAsync(&lbvh_scratch_, scratch_bytes, pool_, stream_), "cudaMallocFromPoolAsync(scratch)");
+    for (int k = 0; k < kBuildStreams; ++k) {
+        check(cudaMallocFromPoolAsync(&build_scratch_[k], scratch_bytes, pool_, stream_),
+              "cudaMallocFromPoolAsync(scratch)");
+        check(cudaStreamCreateWithFlags(&build_streams_[k], cudaStreamNonBlocking), "stream");
+        check(cudaEventCreateWithFlags(&build_done_[k], cudaEventDisableTiming), "event");
+    }
+    check(cudaEventCreateWithFlags(&build_fork_, cudaEventDisableTiming), "event");
     // every wrap's input prefix, staged side by side in page-locked memory
     // on the host's cores, then one copy per wrap
     std::vector<size_t> offset(W + 1, 0);
@@ -715,12 +725,10 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
     shape_.side_stream = side_stream_;
     shape_.side_fork = side_fork_;
     shape_.side_join = side_join_;
+    reset_all(staging.data(), &offset, lbvh_out);
     for (int i = 0; i < W; ++i) {
         Wrap& w = *wraps_[i];
-        check(cudaMemcpyAsync(w.arena.base(), staging.data() + offset[i], w.input_bytes, cudaMemcpyHostToDevice,
-                              stream_), "upload inputs");
         g_transfers.h2d += w.input_bytes;
-        reset_device(w, stream_, lbvh_scratch_, i == 0 ? lbvh_out : nullptr);
         shape_.max_vertices = std::max(shape_.max_vertices, w.V);
         shape_.max_nodes = std::max(shape_.max_nodes, w.max_nodes);
         shape_.max_edges = std::max(shape_.max_edges, w.max_edges);
@@ -741,12 +749,27 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
     }
 }
 
+void Batch::reset_all(const char* staging, const std::vector<size_t>* offset, LbvhExport* lbvh_out) {
+    check(cudaEventRecord(build_fork_, stream_), "event");
+    for (int k = 0; k < kBuildStreams; ++k) check(cudaStreamWaitEvent(build_streams_[k], build_fork_, 0), "wait");
+    for (size_t i = 0; i < wraps_.size(); ++i) {
+        Wrap& w = *wraps_[i];
+        const int k = static_cast<int>(i % kBuildStreams);
+        if (staging)
+            check(cudaMemcpyAsync(w.arena.base(), staging + (*offset)[i], w.input_bytes, cudaMemcpyHostToDevice,
+                                  build_streams_[k]), "upload inputs");
+        reset_device(w, build_streams_[k], build_scratch_[k], i == 0 ? lbvh_out : nullptr);
+    }
+    for (int k = 0; k < kBuildStreams; ++k) {
+        check(cudaEventRecord(build_done_[k], build_streams_[k]), "event");
+        check(cudaStreamWaitEvent(stream_, build_done_[k], 0), "wait");
+    }
+}
+
 void Batch::reset() {
     check(cudaStreamSynchronize(stream_), "reset");
-    for (auto& w : wraps_) {
-        reset_device(*w, stream_, lbvh_scratch_, nullptr);
-        w->solve_seconds = 0.0;
-    }
+    reset_all(nullptr, nullptr, nullptr);
+    for (auto& w : wraps_) w->solve_seconds = 0.0;
     ticks_ = 0;
     launches_ = 0;
     const double t = now_seconds();
@@ -912,7 +935,7 @@ double Batch::timed_step() {
     check(cudaEventCreate(&end), "event");
     check(cudaStreamSynchronize(stream_), "step");
     check(cudaEventRecord(begin, stream_), "event");
-    for (auto& w : wraps_) reset_device(*w, stream_, lbvh_scratch_, nullptr);
+    reset_all(nullptr, nullptr, nullptr);
     ticks_ = 0;
     launches_ = 0;
     for (auto& w : wraps_) launches_ += lbvh_build_launches(w->F);

@@ -101,7 +101,14 @@ private:
     cudaStream_t stream_ = nullptr;
     WrapDev* dev_wraps_ = nullptr;
     WrapControl* dev_controls_ = nullptr;
-    void* lbvh_scratch_ = nullptr;  // hierarchy build scratch, shared by the wraps' builds
+    // Start states and target hierarchies are built on kBuildStreams side
+    // streams, each with its own hierarchy scratch (sized for the largest
+    // target), forked from and joined back into stream_.
+    static constexpr int kBuildStreams = 4;
+    void reset_all(const char* staging, const std::vector<size_t>* offset, LbvhExport* lbvh_out);
+    cudaStream_t build_streams_[kBuildStreams] = {};
+    cudaEvent_t build_fork_ = nullptr, build_done_[kBuildStreams] = {};
+    void* build_scratch_[kBuildStreams] = {};
     cudaMemPool_t pool_ = nullptr;  // the arenas' and the scratch's (batch_pool)
     int* query_counter_ = nullptr;  // the query queue's next item
     cudaStream_t side_stream_ = nullptr;  // the tick's refresh branch
