@@ -515,7 +515,8 @@ def run_ours(args, ranks):
                     for i in range(len(cases)))
 
     # ---- e2e: the public API from host arrays ----
-    dp.solve_batch(tuples)  # warm-up: the process's page-locked staging and device pool
+    for _ in range(2):  # warm-up: the process's page-locked staging, device pool and host heap
+        dp.solve_batch(tuples)
     dp.transfer_counters(reset=True)
     ranks.barrier()
     e2e_steps = 3
@@ -536,8 +537,8 @@ def run_ours(args, ranks):
            "call_seconds": [round(x, 3) for x in call_s],
            "preparation_seconds": [round(x, 3) for x in prep_s],
            "solve_seconds": [round(x, 3) for x in solve_s],
-           "how": "nricp_dp.solve_batch on the 64 wraps from host arrays, three calls after one untimed "
-                  "call; preparation = input checks, graphs, layouts, uploads and hierarchies (the "
+           "how": "nricp_dp.solve_batch on the 64 wraps from host arrays, three calls after two untimed "
+                  "calls; preparation = input checks, graphs, layouts, uploads and hierarchies (the "
                   "reports' setup_seconds summed), solve = the device schedule"}
 
     # ---- roofline of the dominant kernel over the batch ----
