@@ -129,16 +129,19 @@ void compute_normalization(const double* p, int n, double center[3], double* sca
     *scale = diagonal > 0.0 ? 1.0 / diagonal : 1.0;
 }
 
-std::vector<double> normalized(const double* p, int n, const double center[3], double scale) {
-    std::vector<double> out(static_cast<size_t>(n) * 3);  // mesh.cpp:183-187
-    for (int i = 0; i < n; ++i)
+void normalized_into(const double* p, int n, const double center[3], double scale, double* out) {
+    for (int i = 0; i < n; ++i)  // mesh.cpp:183-187
         for (int k = 0; k < 3; ++k) out[i * 3 + k] = (p[i * 3 + k] - center[k]) * scale;
+}
+
+std::vector<double> normalized(const double* p, int n, const double center[3], double scale) {
+    std::vector<double> out(static_cast<size_t>(n) * 3);
+    normalized_into(p, n, center, scale, out.data());
     return out;
 }
 
-std::vector<double> vertex_normals(const std::vector<double>& p, const int32_t* f, int m) {
-    const size_t n = p.size() / 3;  // mesh.cpp:71-88
-    std::vector<double> out(n * 3, 0.0);
+void vertex_normals_into(const double* p, int n, const int32_t* f, int m, double* out) {
+    std::fill(out, out + static_cast<size_t>(n) * 3, 0.0);  // mesh.cpp:71-88
     for (int i = 0; i < m; ++i) {
         const double* a = &p[f[i * 3] * 3];
         const double* b = &p[f[i * 3 + 1] * 3];
@@ -154,7 +157,7 @@ std::vector<double> vertex_normals(const std::vector<double>& p, const int32_t* 
             t[2] = t[2] + w[2];
         }
     }
-    for (size_t i = 0; i < n; ++i) {
+    for (int i = 0; i < n; ++i) {
         double* v = &out[i * 3];
         const double length = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         if (length > 0.0) {
@@ -163,6 +166,11 @@ std::vector<double> vertex_normals(const std::vector<double>& p, const int32_t* 
             v[0] = v[1] = v[2] = 0.0;
         }
     }
+}
+
+std::vector<double> vertex_normals(const std::vector<double>& p, const int32_t* f, int m) {
+    std::vector<double> out(p.size());
+    vertex_normals_into(p.data(), static_cast<int>(p.size() / 3), f, m, out.data());
     return out;
 }
 

@@ -59,6 +59,9 @@ void validate_mesh(const double* points, int count, const int32_t* faces, int fa
 void validate_settings(const NricpSolveDesc& desc);
 
 void compute_normalization(const double* points, int count, double center[3], double* scale);
+// The same two, written into caller memory (count x 3 doubles).
+void normalized_into(const double* points, int count, const double center[3], double scale, double* out);
+void vertex_normals_into(const double* points, int count, const int32_t* faces, int face_count, double* out);
 std::vector<double> normalized(const double* points, int count, const double center[3],
                                double scale);
 std::vector<double> vertex_normals(const std::vector<double>& points, const int32_t* faces,

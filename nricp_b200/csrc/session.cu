@@ -85,9 +85,9 @@ private:
 // target's diagonal: far above the rounding of FP32 boxes and queries.
 constexpr double kRankWindow = 4e-6;
 
-double target_diagonal(const std::vector<double>& p) {
+double target_diagonal(const double* p, size_t n) {
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    for (size_t i = 0; i < p.size() / 3; ++i)
+    for (size_t i = 0; i < n; ++i)
         for (int k = 0; k < 3; ++k) {
             lo[k] = i ? std::min(lo[k], p[i * 3 + k]) : p[k];
             hi[k] = i ? std::max(hi[k], p[i * 3 + k]) : p[k];
@@ -397,9 +397,24 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.pcg_tolerance = d.pcg_tolerance;
 
     // template and target, normalised with the template's frame
-    const std::vector<double> tpl = normalized(w.template_in.data(), V, w.graph.center, w.graph.scale);
-    const std::vector<double> tgt = normalized(w.target_in.data(), w.Vt, w.graph.center, w.graph.scale);
-    const std::vector<double> tgt_normals = vertex_normals(tgt, w.target_faces.data(), w.F);
+    // (written straight into the staging area when there is one)
+    std::vector<double> tpl_v, tgt_v, normals_v;
+    double *tpl, *tgt, *tgt_normals;
+    if (staging) {
+        tpl = reinterpret_cast<double*>(staging + o_tpl);
+        tgt = reinterpret_cast<double*>(staging + o_tgt);
+        tgt_normals = reinterpret_cast<double*>(staging + o_tgt_normals);
+    } else {
+        tpl_v.resize(static_cast<size_t>(V) * 3);
+        tgt_v.resize(static_cast<size_t>(w.Vt) * 3);
+        normals_v.resize(static_cast<size_t>(w.Vt) * 3);
+        tpl = tpl_v.data();
+        tgt = tgt_v.data();
+        tgt_normals = normals_v.data();
+    }
+    normalized_into(w.template_in.data(), V, w.graph.center, w.graph.scale, tpl);
+    normalized_into(w.target_in.data(), w.Vt, w.graph.center, w.graph.scale, tgt);
+    vertex_normals_into(tgt, w.Vt, w.target_faces.data(), w.F, tgt_normals);
     std::vector<double> lm_target(static_cast<size_t>(V) * 3, 0.0);
     std::vector<uint8_t> lm_flag(V, 0);
     for (int i = 0; i < w.L; ++i) {
@@ -421,8 +436,8 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.tgt_faces = a.at<int32_t>(o_tgt_faces);
     D.bvh_nodes = a.at<float4>(o_bvh_nodes);
     D.bvh_leaves = a.at<float4>(o_bvh_leaves);
-    D.rank_window = static_cast<float>(kRankWindow * target_diagonal(tgt));
-    in.put(const_cast<double*>(D.tpl), tpl);
+    D.rank_window = static_cast<float>(kRankWindow * target_diagonal(tgt, static_cast<size_t>(w.Vt)));
+    if (!staging) in.put(const_cast<double*>(D.tpl), tpl_v);
     in.put(const_cast<int32_t*>(D.tpl_faces), w.template_faces);
     in.put(const_cast<int32_t*>(D.vf_begin), vf_begin);
     in.put(const_cast<int32_t*>(D.vf_faces), vf_list);
@@ -430,8 +445,10 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     in.put(const_cast<double*>(D.lm_target), lm_target);
     in.put(const_cast<uint8_t*>(D.lm_flag), lm_flag);
     in.put(const_cast<int32_t*>(D.lm_vertices), w.landmark_indices);
-    in.put(const_cast<double*>(D.tgt_points), tgt);
-    in.put(const_cast<double*>(D.tgt_normals), tgt_normals);
+    if (!staging) {
+        in.put(const_cast<double*>(D.tgt_points), tgt_v);
+        in.put(const_cast<double*>(D.tgt_normals), normals_v);
+    }
     in.put(const_cast<int32_t*>(D.tgt_faces), w.target_faces);
 
     for (int l = 0; l < w.levels; ++l) {
@@ -664,7 +681,12 @@ void Batch::add_all(const NricpSolveDesc* descs, int count) {
         }
         for (size_t k = 0; k < tasks.size(); ++k)
             if (!failure[k].empty()) throw std::runtime_error(failure[k]);
-        for (auto& w : prepared) envelope(*w);
+        for (auto& w : prepared) {
+            envelope(*w);
+            // the layouts hold all the solve needs; the graph's per-vertex
+            // bindings (about 100 bytes per vertex and level) go now
+            std::vector<GraphLevel>().swap(w->graph.levels);
+        }
     } else {
 #pragma omp parallel for schedule(dynamic, 1) if (count > 1)
         for (int i = 0; i < count; ++i) guarded_step(i, [&] { prepare_host(*prepared[i]); });
