@@ -751,15 +751,14 @@ void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaSt
         k_query<<<grid, 128, 0, stream>>>(wraps);
         return;
     }
-    static int resident = 0;  // blocks of the queue that fit on the device at once
-    if (resident == 0) {
+    static const int resident = [] {  // blocks of the queue that fit on the device at once
         int device = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_queue, 128, sizeof(int) * 1025);
-        resident = sms * (per_sm > 0 ? per_sm : 1);
-        if (resident <= 0) resident = 1;
-    }
+        const int blocks = sms * (per_sm > 0 ? per_sm : 1);
+        return blocks > 0 ? blocks : 1;
+    }();
     cudaMemsetAsync(counter, 0, sizeof(int), stream);
     k_query_queue<<<resident, 128, sizeof(int) * (wrap_count + 1), stream>>>(wraps, wrap_count, counter);
 }

@@ -1782,12 +1782,12 @@ int pcg_latency_cluster(int nodes) {
 }
 
 void pcg_enable() {
-    static bool enabled = false;
-    if (!enabled) {
+    static const bool enabled = [] {  // once per process, thread-safe
         cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         cudaFuncSetAttribute(k_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, kPcgMaxSmemBytes);
-        enabled = true;
-    }
+        return true;
+    }();
+    (void)enabled;
 }
 
 // Default cluster size for a batch: one wrap takes its latency cluster; many
