@@ -343,6 +343,24 @@ int nricp_template_graph_level(const double* points, int count, int levels,
                                int32_t* edges, int edge_capacity, int* edge_count,
                                int use_device);
 
+/* farthest_point_seeds(points, count, first_index) (bindings.cpp:796-804,
+ * src/core/sampling.cpp:47-88): deterministic farthest-point sampling, ties
+ * to the lower index; first_index is clamped into range.  Writes
+ * min(count, point_count) indices (none when either is <= 0) and their
+ * number to *written.  Host code, the graph build's own. */
+int nricp_farthest_point_seeds(const double* points, int point_count, int count, int first_index,
+                               int32_t* out, int* written);
+/* bind_vertices(points, nodes, max_nodes) (bindings.cpp:806-815,
+ * sampling.cpp:90-143): each point's nearest max_nodes (1..8) nodes with the
+ * reference's distance-ratio weights.  out_nodes / out_weights: point_count x
+ * NRICP_MAX_SLOTS (-1 / 0 past the count); out_counts: point_count. */
+int nricp_bind_vertices(const double* points, int point_count, const double* nodes, int node_count,
+                        int max_nodes, int32_t* out_nodes, double* out_weights, int32_t* out_counts);
+/* vertex_normals(points, faces) (bindings.cpp:1014-1024, mesh.cpp:71-88):
+ * area-weighted vertex normals, zero where a vertex has no area. */
+int nricp_vertex_normals(const double* points, int point_count, const int32_t* faces, int face_count,
+                         double* out);
+
 /* fit_rigid(source_points, target_points, weights) (bindings.cpp:857-883,
  * src/core/deformation.cpp:86-139), on the device: the weighted rigid
  * transform (reflections excluded) that best maps `count` source points onto

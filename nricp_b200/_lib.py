@@ -75,6 +75,9 @@ def _declare(lib: C.CDLL) -> None:
                                                  i32p, C.c_int, P(C.c_int), C.c_int]),
         "nricp_closest_points": (C.c_int, [dp, C.c_int, i32p, C.c_int, dp, C.c_int, dp, dp, dp, i32p]),
         "nricp_fit_rigid": (C.c_int, [dp, dp, dp, C.c_int, dp, dp]),
+        "nricp_farthest_point_seeds": (C.c_int, [dp, C.c_int, C.c_int, C.c_int, i32p, P(C.c_int)]),
+        "nricp_bind_vertices": (C.c_int, [dp, C.c_int, dp, C.c_int, C.c_int, i32p, dp, i32p]),
+        "nricp_vertex_normals": (C.c_int, [dp, C.c_int, i32p, C.c_int, dp]),
         "nricp_lbvh_export": (C.c_int, [dp, C.c_int, i32p, C.c_int, u32p, u32p, i32p, i32p, fp]),
         "nricp_lbvh_export_static": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

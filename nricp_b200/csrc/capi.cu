@@ -395,6 +395,46 @@ int nricp_template_graph_level(const double* points, int count, int levels, int 
     });
 }
 
+int nricp_farthest_point_seeds(const double* points, int point_count, int count, int first_index,
+                               int32_t* out, int* written) {
+    return guarded([&] {
+        if (point_count < 0) throw InvalidArgument("points must have shape (n, 3)");
+        const std::vector<double> p(points, points + static_cast<size_t>(point_count) * 3);
+        const std::vector<int> seeds = farthest_point_seeds(p, count, first_index);
+        for (size_t i = 0; i < seeds.size(); ++i) out[i] = seeds[i];
+        *written = static_cast<int>(seeds.size());
+    });
+}
+
+int nricp_bind_vertices(const double* points, int point_count, const double* nodes, int node_count,
+                        int max_nodes, int32_t* out_nodes, double* out_weights, int32_t* out_counts) {
+    return guarded([&] {
+        if (point_count < 0 || node_count < 0) throw InvalidArgument("points and nodes must have shape (n, 3)");
+        if (max_nodes > NRICP_MAX_SLOTS) throw InvalidArgument("max_nodes_per_vertex exceeds 8");
+        const std::vector<double> p(points, points + static_cast<size_t>(point_count) * 3);
+        const std::vector<double> q(nodes, nodes + static_cast<size_t>(node_count) * 3);
+        const std::vector<Binding> b = bind_vertices(p, q, max_nodes, NRICP_MAX_SLOTS);
+        for (int v = 0; v < point_count; ++v) {
+            for (int s = 0; s < NRICP_MAX_SLOTS; ++s) {
+                out_nodes[static_cast<size_t>(v) * NRICP_MAX_SLOTS + s] = b[v].nodes[s];
+                out_weights[static_cast<size_t>(v) * NRICP_MAX_SLOTS + s] = b[v].weights[s];
+            }
+            out_counts[v] = b[v].count;
+        }
+    });
+}
+
+int nricp_vertex_normals(const double* points, int point_count, const int32_t* faces, int face_count,
+                         double* out) {
+    return guarded([&] {
+        if (point_count < 0 || face_count < 0) throw InvalidArgument("points and faces must have shape (n, 3)");
+        for (long i = 0; i < static_cast<long>(face_count) * 3; ++i)
+            if (faces[i] < 0 || faces[i] >= point_count)
+                throw InvalidArgument("face " + std::to_string(i / 3) + " references a missing vertex");
+        vertex_normals_into(points, point_count, faces, face_count, out);
+    });
+}
+
 int nricp_fit_rigid(const double* source_points, const double* target_points, const double* weights,
                     int count, double* rotation, double* translation) {
     return guarded([&] {

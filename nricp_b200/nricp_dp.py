@@ -473,6 +473,48 @@ def closest_points(target_points, target_faces, query_points) -> dict:
     return out
 
 
+def farthest_point_seeds(points, count: int, first_index: int = 0) -> np.ndarray:
+    """Deterministic farthest-point sampling; ties break to the lower index
+    (bindings.cpp:796-804, sampling.cpp:47-88)."""
+    p = _points(points, "points")
+    out = np.zeros(max(0, min(int(count), len(p))), dtype=np.int32)
+    written = C.c_int()
+    check(load().nricp_farthest_point_seeds(p.ctypes.data_as(C.POINTER(C.c_double)), len(p), int(count),
+                                            int(first_index),
+                                            (out if len(out) else np.zeros(1, np.int32)).ctypes.data_as(
+                                                C.POINTER(C.c_int32)), C.byref(written)))
+    return out[:written.value].astype(np.int64)
+
+
+def bind_vertices(points, nodes, max_nodes: int = 4) -> dict:
+    """Bind every vertex to its nearest nodes with distance-ratio weights
+    (bindings.cpp:806-815, sampling.cpp:90-143): nodes (n, 4) -- (n, 8) when
+    max_nodes > 4 -- with -1 past the count, weights likewise, counts (n,)."""
+    p, q = _points(points, "points"), _points(nodes, "nodes")
+    n = len(p)
+    nodes_out = np.full((max(1, n), 8), -1, dtype=np.int32)
+    weights_out = np.zeros((max(1, n), 8))
+    counts_out = np.zeros(max(1, n), dtype=np.int32)
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    check(load().nricp_bind_vertices(P(p, C.c_double), n, P(q, C.c_double), len(q), int(max_nodes),
+                                     P(nodes_out, C.c_int32), P(weights_out, C.c_double),
+                                     P(counts_out, C.c_int32)))
+    width = 4 if int(max_nodes) <= 4 else 8
+    return {"nodes": nodes_out[:n, :width].astype(np.int64), "weights": weights_out[:n, :width].copy(),
+            "counts": counts_out[:n].astype(np.int64)}
+
+
+def vertex_normals(points, faces) -> np.ndarray:
+    """Area-weighted vertex normals (bindings.cpp:1014-1024, mesh.cpp:71-88)."""
+    p, f = _points(points, "points"), _faces(faces, "faces")
+    out = np.zeros((len(p), 3))
+    P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    check(load().nricp_vertex_normals(P(p, C.c_double) if len(p) else P(np.zeros(3), C.c_double), len(p),
+                                      P(f, C.c_int32) if len(f) else P(np.zeros(3, np.int32), C.c_int32),
+                                      len(f), P(out, C.c_double) if len(p) else P(np.zeros(3), C.c_double)))
+    return out
+
+
 def fit_rigid(source_points, target_points, weights) -> dict:
     """Weighted rigid fit (reflection excluded) between point pairs, on the
     device (bindings.cpp:857-883, deformation.cpp:86-139): the rotation (1, 3,
