@@ -409,6 +409,44 @@ def validate_mesh(points, faces) -> dict:
     return {"ok": not problems, "problems": problems}
 
 
+def validate_mask(mask, template_vertex_count: int) -> int:
+    """Validate a participation mask and return how many vertices stay active
+    (bindings.cpp:955-973, src/core/constraints.cpp:33-58).  Entries are
+    read as true or false, so only the length and an all-false mask can fail."""
+    m = np.asarray(mask).reshape(-1) != 0
+    if m.size == 0:
+        return 0  # no mask (every vertex takes part); the reference counts none (constraints.cpp:60-63)
+    if m.size != int(template_vertex_count):
+        raise ValueError(f"invalid mask: mask has {m.size} entries but the template has "
+                         f"{int(template_vertex_count)} vertices")
+    active = int(m.sum())
+    if active == 0:
+        raise ValueError("invalid mask: mask excludes every vertex; the fit would be unconstrained")
+    return active
+
+
+def validate_landmarks(indices, targets, template_vertex_count: int) -> None:
+    """Raise with a descriptive message when landmarks are unusable
+    (bindings.cpp:926-953, src/core/constraints.cpp:8-31)."""
+    idx, tgt = np.asarray(indices), np.asarray(targets, dtype=np.float64)
+    if idx.ndim != 1:
+        raise ValueError("landmark indices must have shape (n,)")
+    if tgt.ndim != 2 or tgt.shape[1] != 3 or tgt.shape[0] != idx.shape[0]:
+        raise ValueError("landmark targets must have shape (n, 3), matching indices")
+    problems, seen, n = [], set(), int(template_vertex_count)
+    for i, (v, t) in enumerate(zip(idx.astype(np.int64).astype(np.int32).tolist(), tgt)):
+        if v < 0 or v >= n:
+            problems.append(f"landmark {i} points at template vertex {v} but the template has {n} vertices")
+            continue
+        if not np.isfinite(t).all():
+            problems.append(f"landmark {i} has a non-finite target")
+        if v in seen:
+            problems.append(f"landmark {i} marks template vertex {v} twice")
+        seen.add(v)
+    if problems:
+        raise ValueError("invalid landmarks: " + "; ".join(problems))
+
+
 def build_template_graph(points, faces, levels: int = 4, nodes_initial: int = 100,
                          growth: int = 2, max_nodes_per_vertex: int = 4,
                          use_device: bool = False, edge_neighbours: int = 4) -> dict:

@@ -60,3 +60,21 @@ def test_descriptors_built_on_threads_equal_the_serial_ones():
         # the struct points into the descriptor's own arrays
         assert C.addressof(a.target_faces.ctypes.data_as(C.POINTER(C.c_int32)).contents) == \
             C.addressof(a.struct.target_faces.contents)
+
+
+def test_mask_and_landmark_validation_follow_the_reference():
+    from nricp_b200 import nricp_dp as dp
+
+    assert dp.validate_mask([1, 0, 2, 0], 4) == 2
+    assert dp.validate_mask([], 7) == 0
+    with pytest.raises(ValueError, match="invalid mask: mask has 3 entries but the template has 4 vertices"):
+        dp.validate_mask([1, 1, 1], 4)
+    with pytest.raises(ValueError, match="mask excludes every vertex"):
+        dp.validate_mask([0, 0], 2)
+    dp.validate_landmarks([0, 3], [[0, 0, 0], [1, 1, 1]], 4)
+    with pytest.raises(ValueError, match=r"invalid landmarks: landmark 1 points at template vertex 9 but the "
+                                         r"template has 4 vertices; landmark 2 has a non-finite target; "
+                                         r"landmark 3 marks template vertex 0 twice"):
+        dp.validate_landmarks([0, 9, 1, 0], [[0, 0, 0], [1, 1, 1], [np.nan, 0, 0], [2, 2, 2]], 4)
+    with pytest.raises(ValueError, match="landmark targets must have shape"):
+        dp.validate_landmarks([0, 1], [[0, 0, 0]], 4)
