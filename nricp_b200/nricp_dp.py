@@ -409,6 +409,242 @@ def validate_mesh(points, faces) -> dict:
     return {"ok": not problems, "problems": problems}
 
 
+# ---- deformation helpers on the host (the reference's component functions) ----
+
+def _matrices(array, name: str) -> np.ndarray:
+    m = np.asarray(array, dtype=np.float64)
+    if m.ndim != 3 or m.shape[1:] != (3, 3):
+        raise ValueError(f"{name} must have shape (n, 3, 3)")
+    return m
+
+
+def _deformation(rotations, translations, node_positions=None):
+    r = _matrices(rotations, "rotations")
+    t = np.asarray(translations, dtype=np.float64)
+    if t.ndim != 2 or t.shape[1:] != (3,) or t.shape[0] != r.shape[0]:
+        raise ValueError("translations must have shape (n, 3)")
+    if node_positions is not None:
+        g = np.asarray(node_positions, dtype=np.float64)
+        if g.ndim != 2 or g.shape[1:] != (3,) or g.shape[0] != r.shape[0]:
+            raise ValueError("node_positions must have shape (n, 3)")
+        return r, t, g
+    return r, t, None
+
+
+def _libm(fn, *args) -> np.ndarray:
+    """fn applied elementwise through the C library's own function (Python's
+    math module), which the reference's std:: calls resolve to; numpy's
+    vectorised transcendentals can round the last bit differently."""
+    return np.frompyfunc(fn, len(args), 1)(*args).astype(np.float64)
+
+
+def _mat_vec(m: np.ndarray, v: np.ndarray) -> np.ndarray:
+    """m v per row, each dot summed left to right (mat3.h:17-22)."""
+    return np.stack([m[:, i, 0] * v[:, 0] + m[:, i, 1] * v[:, 1] + m[:, i, 2] * v[:, 2] for i in range(3)], 1)
+
+
+def _mat_mat(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """a b per pair of matrices, each entry summed left to right (mat3.h:24-36)."""
+    out = np.empty((max(len(a), len(b)), 3, 3))
+    for i in range(3):
+        for j in range(3):
+            out[:, i, j] = a[:, i, 0] * b[:, 0, j] + a[:, i, 1] * b[:, 1, j] + a[:, i, 2] * b[:, 2, j]
+    return out
+
+
+def _exp_so3(omega: np.ndarray) -> np.ndarray:
+    """Rodrigues: R = I + (a [w] + b [w]^2), a = sin(th)/th,
+    b = (1 - cos(th))/th^2, and the second-order series below th^2 = 1e-24
+    (rotation.h:28-46)."""
+    w = np.asarray(omega, dtype=np.float64).reshape(-1, 3)
+    hat = np.zeros((len(w), 3, 3))
+    hat[:, 0, 1], hat[:, 0, 2], hat[:, 1, 2] = -w[:, 2], w[:, 1], -w[:, 0]
+    hat[:, 1, 0], hat[:, 2, 0], hat[:, 2, 1] = w[:, 2], -w[:, 1], w[:, 0]
+    hat2 = _mat_mat(hat, hat)
+    th2 = w[:, 0] * w[:, 0] + w[:, 1] * w[:, 1] + w[:, 2] * w[:, 2]
+    small = th2 < 1e-24
+    th = np.sqrt(np.where(small, 1.0, th2))
+    a = np.where(small, 1.0, _libm(math.sin, th) / th)
+    b = np.where(small, 0.5, (1.0 - _libm(math.cos, th)) / np.where(small, 1.0, th2))
+    return np.eye(3) + (a[:, None, None] * hat + b[:, None, None] * hat2)
+
+
+def _quaternions(m: np.ndarray) -> np.ndarray:
+    """(w, x, y, z) of each rotation matrix by Shepperd's branches, unnormalised
+    (quaternion.h:48-75)."""
+    q = np.empty((len(m), 4))
+    d0, d1, d2 = m[:, 0, 0], m[:, 1, 1], m[:, 2, 2]
+    trace = d0 + d1 + d2
+    b0 = trace > 0.0
+    b1 = ~b0 & (d0 > d1) & (d0 > d2)
+    b2 = ~b0 & ~b1 & (d1 > d2)
+    b3 = ~(b0 | b1 | b2)
+    r = lambda sel, i, j: m[sel, i, j]  # noqa: E731
+    s = np.sqrt(trace[b0] + 1.0) * 2.0
+    q[b0] = np.stack([0.25 * s, (r(b0, 2, 1) - r(b0, 1, 2)) / s, (r(b0, 0, 2) - r(b0, 2, 0)) / s,
+                      (r(b0, 1, 0) - r(b0, 0, 1)) / s], 1)
+    s = np.sqrt(1.0 + d0[b1] - d1[b1] - d2[b1]) * 2.0
+    q[b1] = np.stack([(r(b1, 2, 1) - r(b1, 1, 2)) / s, 0.25 * s, (r(b1, 0, 1) + r(b1, 1, 0)) / s,
+                      (r(b1, 0, 2) + r(b1, 2, 0)) / s], 1)
+    s = np.sqrt(1.0 + d1[b2] - d0[b2] - d2[b2]) * 2.0
+    q[b2] = np.stack([(r(b2, 0, 2) - r(b2, 2, 0)) / s, (r(b2, 0, 1) + r(b2, 1, 0)) / s, 0.25 * s,
+                      (r(b2, 1, 2) + r(b2, 2, 1)) / s], 1)
+    s = np.sqrt(1.0 + d2[b3] - d0[b3] - d1[b3]) * 2.0
+    q[b3] = np.stack([(r(b3, 1, 0) - r(b3, 0, 1)) / s, (r(b3, 0, 2) + r(b3, 2, 0)) / s,
+                      (r(b3, 1, 2) + r(b3, 2, 1)) / s, 0.25 * s], 1)
+    return q
+
+
+def _qdot(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    return a[:, 0] * b[:, 0] + a[:, 1] * b[:, 1] + a[:, 2] * b[:, 2] + a[:, 3] * b[:, 3]
+
+
+def _unit(q: np.ndarray) -> np.ndarray:
+    """q / |q|, the identity for a zero quaternion (quaternion.h:38-44)."""
+    length = np.sqrt(_qdot(q, q))
+    zero = length <= 0.0
+    out = q / np.where(zero, 1.0, length)[:, None]
+    out[zero] = (1.0, 0.0, 0.0, 0.0)
+    return out
+
+
+def _matrices_of(q: np.ndarray) -> np.ndarray:
+    """Rotation matrix of each unit quaternion (quaternion.h:77-93)."""
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    return np.stack([1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+                     2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+                     2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)],
+                    1).reshape(-1, 3, 3)
+
+
+def _log_so3(rotations: np.ndarray) -> np.ndarray:
+    """The rotation vector of each matrix, through its unit quaternion (w >= 0)
+    so that it stays accurate up to a half turn (rotation.h:48-62)."""
+    q = _unit(_quaternions(rotations))
+    q[q[:, 0] < 0.0] *= -1.0
+    v = q[:, 1:]
+    length = np.sqrt(v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2])
+    tiny = length < 1e-12
+    safe = np.where(tiny, 1.0, length)
+    out = v * ((2.0 * _libm(math.atan2, length, q[:, 0])) / safe)[:, None]
+    out[tiny] = 0.0
+    return out
+
+
+def _applied(r: np.ndarray, t: np.ndarray, g: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """R (p - g) + g + t for node transforms and points paired row by row
+    (deformation.h:39-43)."""
+    return _mat_vec(r, p - g) + g + t
+
+
+def robust_weights(kernel: str, squared_residuals, threshold: float) -> np.ndarray:
+    """IRLS weights of a robust kernel, 'none', 'huber' or 'geman_mcclure'
+    (bindings.cpp:1077-1092, src/energy/robust.cpp:7-58); negative squared
+    residuals count as zero."""
+    r = np.maximum(np.asarray(squared_residuals, dtype=np.float64).reshape(-1), 0.0)
+    t = float(threshold)
+    if kernel in ("huber", "Huber"):
+        if t <= 0.0:
+            return np.ones_like(r)
+        return np.where(r <= t * t, 1.0, t / np.sqrt(np.where(r > 0.0, r, 1.0)))
+    if kernel in ("geman_mcclure", "geman-mcclure", "GemanMcClure"):
+        if t <= 0.0:
+            return np.ones_like(r)
+        d = 1.0 + r / (t * t)
+        return 1.0 / (d * d)
+    return np.ones_like(r)
+
+
+def evaluate_deformation(points, binding_nodes, binding_weights, binding_counts, rotations, translations,
+                         node_positions) -> np.ndarray:
+    """The embedded deformation at the points: sum over a point's bound nodes
+    of w (R (p - g) + g + t), skipping node indices out of range
+    (bindings.cpp:817-838, 338-367, deformation.cpp:55-85)."""
+    r, t, g = _deformation(rotations, translations, node_positions)
+    n_idx = np.asarray(binding_nodes)
+    w = np.asarray(binding_weights, dtype=np.float64)
+    c = np.asarray(binding_counts)
+    if n_idx.ndim != 2 or n_idx.shape[1] != 4:
+        raise ValueError("binding nodes must have shape (n, 4)")
+    if w.ndim != 2 or w.shape != n_idx.shape:
+        raise ValueError("binding weights must have shape (n, 4)")
+    if c.ndim != 1 or c.shape[0] != n_idx.shape[0]:
+        raise ValueError("binding counts must have shape (n,)")
+    bad = np.nonzero((c < 1) | (c > 4))[0]
+    if len(bad):
+        raise ValueError(f"binding count out of range at vertex {bad[0]}")
+    p = _points(points, "points")
+    if len(p) != len(n_idx):
+        raise ValueError(f"points and bindings must have the same length ({len(p)} vs {len(n_idx)})")
+    out = np.zeros_like(p)
+    for s in range(4):
+        j = n_idx[:, s]
+        ok = (s < c) & (j >= 0) & (j < len(r))
+        jj = np.where(ok, j, 0)
+        out += np.where(ok[:, None], _applied(r[jj], t[jj], g[jj], p) * w[:, s:s + 1], 0.0)
+    return out
+
+
+def retract_deformation(rotations, translations, node_positions, delta) -> dict:
+    """R <- exp([w]) R, t <- t + dt per node, delta = (w, dt) per node
+    (bindings.cpp:1026-1049, deformation.cpp:19-32)."""
+    r, t, _ = _deformation(rotations, translations, node_positions)
+    d = np.asarray(delta, dtype=np.float64)
+    if d.ndim != 1 or d.shape[0] != 6 * len(r):
+        raise ValueError("delta must have shape (6 * node_count,): rotation increment then translation "
+                         "increment per node")
+    d = d.reshape(-1, 6)
+    return {"rotations": _mat_mat(_exp_so3(d[:, :3]), r), "translations": t + d[:, 3:]}
+
+
+def tangent_difference(rotations_from, translations_from, rotations_to, translations_to) -> np.ndarray:
+    """The tangent increment taking one deformation to the other:
+    w = log(R_to R_from^T), dt = t_to - t_from, per node
+    (bindings.cpp:1051-1075, deformation.cpp:34-54)."""
+    ra, ta, _ = _deformation(rotations_from, translations_from)
+    rb, tb, _ = _deformation(rotations_to, translations_to)
+    n = min(len(ra), len(rb))
+    w = _log_so3(_mat_mat(rb[:n], np.transpose(ra[:n], (0, 2, 1))))
+    return np.concatenate([w, tb[:n] - ta[:n]], axis=1).reshape(-1)
+
+
+def transfer_level(from_nodes, rotations, translations, to_nodes, max_nodes: int = 4) -> dict:
+    """Sample a deformation at new node positions (bindings.cpp:840-856,
+    deformation.cpp:141-203): each new node binds to its nearest source nodes
+    (support clamped to 4 slots, as the reference's binding has), blends their
+    rotations as quaternions with signs aligned to the heaviest contributor --
+    falling back to that contributor's rotation when the blend is shorter than
+    1e-8 -- and takes the field's own value at its rest position."""
+    src = _points(from_nodes, "from_nodes")
+    r, t, g = _deformation(rotations, translations, src)
+    dst = _points(to_nodes, "to_nodes")
+    n = len(dst)
+    rot = np.broadcast_to(np.eye(3), (n, 3, 3)).copy()
+    shift = np.zeros((n, 3))
+    if len(src) == 0 or n == 0:
+        return {"rotations": rot, "translations": shift}
+    b = bind_vertices(dst, src, min(int(max_nodes), 4))
+    nodes, w, c = b["nodes"], b["weights"], b["counts"]
+    q_src = _quaternions(r)
+    heaviest, heavy_w = nodes[:, 0].copy(), w[:, 0].copy()
+    for s in range(1, 4):
+        take = (s < c) & (w[:, s] > heavy_w)
+        heaviest[take], heavy_w[take] = nodes[take, s], w[take, s]
+    q_ref = q_src[heaviest]
+    blended = np.zeros((n, 4))
+    position = np.zeros((n, 3))
+    for s in range(4):
+        ok = (s < c)[:, None]
+        j = np.where(s < c, nodes[:, s], 0)
+        q = q_src[j]
+        q = np.where((_qdot(q, q_ref) < 0.0)[:, None], q * -1.0, q)
+        blended += np.where(ok, q * w[:, s:s + 1], 0.0)
+        position += np.where(ok, _applied(r[j], t[j], g[j], dst) * w[:, s:s + 1], 0.0)
+    spread = np.sqrt(_qdot(blended, blended)) > 1e-8
+    rot = _matrices_of(np.where(spread[:, None], _unit(blended), q_ref))
+    return {"rotations": rot, "translations": position - dst}
+
+
 def validate_mask(mask, template_vertex_count: int) -> int:
     """Validate a participation mask and return how many vertices stay active
     (bindings.cpp:955-973, src/core/constraints.cpp:33-58).  Entries are

@@ -276,3 +276,49 @@ class Oracle:
         out = np.zeros(9)
         lib.oracle_horn_rotation(_p(c), _p(out))
         return out.reshape(3, 3)
+
+    # ---- deformation pieces (the reference's own functions only) ----------
+    def _reference_only(self, what: str):
+        if self.kind not in ("reference", "reference_gpu"):
+            raise NotImplementedError(f"{what} is pinned to the reference's own function only")
+
+    def retract(self, rotations, translations, delta) -> tuple[np.ndarray, np.ndarray]:
+        self._reference_only("retract")
+        r, t, d = _f64(rotations).copy(), _f64(translations).copy(), _f64(delta)
+        self.lib.ref_retract(C.c_int(len(r)), _p(r), _p(t), _p(d))
+        return r, t
+
+    def tangent_difference(self, rotations_from, translations_from, rotations_to, translations_to):
+        self._reference_only("tangent_difference")
+        ra, ta, rb, tb = map(_f64, (rotations_from, translations_from, rotations_to, translations_to))
+        out = np.zeros(len(ra) * 6)
+        self.lib.ref_tangent_difference(C.c_int(len(ra)), _p(ra), _p(ta), _p(rb), _p(tb), _p(out))
+        return out
+
+    def evaluate_deformation(self, points, binding_nodes, binding_weights, binding_counts,
+                             rotations, translations, node_positions) -> np.ndarray:
+        self._reference_only("evaluate_deformation")
+        pts = _f64(points)
+        n, w, c = _i32(binding_nodes), _f64(binding_weights), _i32(binding_counts)
+        r, t, g = _f64(rotations), _f64(translations), _f64(node_positions)
+        out = np.zeros_like(pts)
+        self.lib.ref_evaluate_deformation(_p(pts), C.c_int(len(pts)), _p(n, C.c_int32), _p(w),
+                                          _p(c, C.c_int32), C.c_int(len(r)), _p(r), _p(t), _p(g),
+                                          _p(out))
+        return out
+
+    def robust_weights(self, kernel: str, squared_residuals, threshold: float) -> np.ndarray:
+        self._reference_only("robust_weights")
+        r = _f64(squared_residuals)
+        out = np.zeros(len(r))
+        self.lib.ref_robust_weights(kernel.encode(), _p(r), C.c_int(len(r)), C.c_double(threshold),
+                                    _p(out))
+        return out
+
+    def transfer_level(self, from_nodes, rotations, translations, to_nodes, max_nodes: int = 4):
+        self._reference_only("transfer_level")
+        src, r, t, dst = _f64(from_nodes), _f64(rotations), _f64(translations), _f64(to_nodes)
+        out_r, out_t = np.zeros((len(dst), 3, 3)), np.zeros((len(dst), 3))
+        self.lib.ref_transfer_level(C.c_int(len(src)), _p(src), _p(r), _p(t), C.c_int(len(dst)), _p(dst),
+                                    C.c_int(max_nodes), _p(out_r), _p(out_t))
+        return out_r, out_t

@@ -394,3 +394,92 @@ int ref_fused_system(const OracleSystemInputs* in, double* diagonal, double* rhs
 }
 
 }  // extern "C"
+
+namespace {
+
+nricp::Deformation deformation_of(int node_count, const double* rotations, const double* translations,
+                                  const double* node_positions) {
+    nricp::Deformation deformation;
+    deformation.nodes.resize(static_cast<std::size_t>(node_count));
+    deformation.node_rest_positions.resize(static_cast<std::size_t>(node_count));
+    for (int n = 0; n < node_count; ++n) {
+        std::memcpy(deformation.nodes[n].rotation.m, rotations + n * 9, sizeof(double) * 9);
+        deformation.nodes[n].translation = {translations[n * 3], translations[n * 3 + 1],
+                                            translations[n * 3 + 2]};
+        if (node_positions != nullptr) {
+            deformation.node_rest_positions[n] = {node_positions[n * 3], node_positions[n * 3 + 1],
+                                                  node_positions[n * 3 + 2]};
+        }
+    }
+    return deformation;
+}
+
+void store_deformation(const nricp::Deformation& deformation, double* rotations, double* translations) {
+    for (std::size_t n = 0; n < deformation.nodes.size(); ++n) {
+        std::memcpy(rotations + n * 9, deformation.nodes[n].rotation.m, sizeof(double) * 9);
+        translations[n * 3] = deformation.nodes[n].translation.x;
+        translations[n * 3 + 1] = deformation.nodes[n].translation.y;
+        translations[n * 3 + 2] = deformation.nodes[n].translation.z;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- the deformation pieces of the Python module, one reference call each
+// (src/python/bindings.cpp:817-856, 1026-1092).  Rotations are n x 9 row-major
+// doubles, bindings n x 4 with a count per vertex.
+
+void ref_retract(int node_count, double* rotations, double* translations, const double* delta) {
+    nricp::Deformation deformation = deformation_of(node_count, rotations, translations, nullptr);
+    nricp::retract(deformation, std::vector<double>(delta, delta + node_count * 6));
+    store_deformation(deformation, rotations, translations);
+}
+
+void ref_tangent_difference(int node_count, const double* rotations_from, const double* translations_from,
+                            const double* rotations_to, const double* translations_to, double* out) {
+    const std::vector<double> delta = nricp::tangent_difference(
+        deformation_of(node_count, rotations_from, translations_from, nullptr),
+        deformation_of(node_count, rotations_to, translations_to, nullptr));
+    std::memcpy(out, delta.data(), sizeof(double) * delta.size());
+}
+
+void ref_evaluate_deformation(const double* points, int point_count, const int32_t* binding_nodes,
+                              const double* binding_weights, const int32_t* binding_counts,
+                              int node_count, const double* rotations, const double* translations,
+                              const double* node_positions, double* out) {
+    std::vector<nricp::VertexBinding> bindings(static_cast<std::size_t>(point_count));
+    for (int v = 0; v < point_count; ++v) {
+        bindings[v].count = binding_counts[v];
+        for (int s = 0; s < nricp::VertexBinding::kMaxNodes; ++s) {
+            bindings[v].nodes[s] = binding_nodes[v * 4 + s];
+            bindings[v].weights[s] = binding_weights[v * 4 + s];
+        }
+    }
+    const auto result = nricp::evaluate(points_of(points, point_count), bindings,
+                                        deformation_of(node_count, rotations, translations,
+                                                       node_positions));
+    for (int v = 0; v < point_count; ++v) {
+        out[v * 3] = result[v].x;
+        out[v * 3 + 1] = result[v].y;
+        out[v * 3 + 2] = result[v].z;
+    }
+}
+
+void ref_transfer_level(int from_count, const double* from_nodes, const double* rotations,
+                        const double* translations, int to_count, const double* to_nodes, int max_nodes,
+                        double* out_rotations, double* out_translations) {
+    const nricp::Deformation transferred = nricp::transfer_level(
+        points_of(from_nodes, from_count), deformation_of(from_count, rotations, translations, from_nodes),
+        points_of(to_nodes, to_count), max_nodes);
+    store_deformation(transferred, out_rotations, out_translations);
+}
+
+void ref_robust_weights(const char* kernel, const double* squared_residuals, int count,
+                        double threshold, double* out) {
+    const nricp::RobustKernel selected = nricp::robust_kernel_from_string(kernel);
+    for (int i = 0; i < count; ++i) out[i] = nricp::robust_weight(selected, squared_residuals[i], threshold);
+}
+
+}  // extern "C"
