@@ -390,50 +390,77 @@ LevelLayout build_layout(const TemplateGraph& graph, int level, int V) {
         }
     }
     // node pairs sharing a vertex (the interactions_ map of
-    // fused_assembly.cpp:68-79), grouped by (a, b)
-    struct PairEntry { int a, b, code; };
-    std::vector<PairEntry> entries;
+    // fused_assembly.cpp:68-79), grouped by (a, b) with a < b, and within a
+    // group in the order the vertices' slot pairs (x < y) come.  The entry
+    // code is v * 64 + (slot of a) * 8 + (slot of b).  Node a's entries come
+    // from its gather list (vertex order); where a holds one slot of a vertex,
+    // the slot pairs' order is the other slot's order.
     {
         size_t most = 0;
         for (int v = 0; v < V; ++v) most += static_cast<size_t>(L.bind_counts[v]) * (L.bind_counts[v] - 1) / 2;
-        entries.reserve(most);
-    }
-    for (int v = 0; v < V; ++v) {
-        const int c = L.bind_counts[v];
-        for (int x = 0; x < c; ++x)
-            for (int y = x + 1; y < c; ++y) {
-                const int nx = L.bind_nodes[v * NRICP_MAX_SLOTS + x];
-                const int ny = L.bind_nodes[v * NRICP_MAX_SLOTS + y];
-                if (nx == ny) continue;
-                const bool xf = nx < ny;
-                entries.push_back({xf ? nx : ny, xf ? ny : nx,
-                                   v * 64 + (xf ? x : y) * 8 + (xf ? y : x)});
+        L.pair_entry.reserve(most);
+        struct Tail { int32_t b, code; };
+        struct Keyed { int key; Tail tail; };
+        std::vector<Tail> run;               // node a's entries, in order
+        std::vector<Keyed> several;
+        std::vector<int32_t> at(N, 0);       // per b: entries, then the next place
+        std::vector<int32_t> group_b;
+        for (int a = 0; a < N; ++a) {
+            const int32_t begin = L.gather_begin[a], end = L.gather_begin[a + 1];
+            // a vertex adds at most its slot count: a bound for the run
+            if (run.size() < static_cast<size_t>(end - begin) * NRICP_MAX_SLOTS)
+                run.resize(static_cast<size_t>(end - begin) * NRICP_MAX_SLOTS);
+            size_t n = 0;
+            for (int32_t i = begin; i < end;) {
+                const int v = L.gather_entry[i] / NRICP_MAX_SLOTS;
+                int32_t j = i + 1;
+                while (j < end && L.gather_entry[j] / NRICP_MAX_SLOTS == v) ++j;
+                const int32_t* nodes = &L.bind_nodes[static_cast<size_t>(v) * NRICP_MAX_SLOTS];
+                const int c = L.bind_counts[v];
+                if (j == i + 1) {
+                    // every slot written, the partners above a kept (no branch
+                    // on the comparison: it goes either way at random)
+                    const int sa = L.gather_entry[i] % NRICP_MAX_SLOTS;
+                    for (int so = 0; so < c; ++so) {
+                        run[n] = {nodes[so], v * 64 + sa * 8 + so};
+                        n += nodes[so] > a;
+                    }
+                } else {  // a in several slots of v: order by the slot pair itself
+                    several.clear();
+                    for (int32_t k = i; k < j; ++k) {
+                        const int sa = L.gather_entry[k] % NRICP_MAX_SLOTS;
+                        for (int so = 0; so < c; ++so)
+                            if (nodes[so] > a)
+                                several.push_back({std::min(sa, so) * 8 + std::max(sa, so),
+                                                   {nodes[so], v * 64 + sa * 8 + so}});
+                    }
+                    std::sort(several.begin(), several.end(),
+                              [](const Keyed& x, const Keyed& y) { return x.key < y.key; });
+                    for (const Keyed& e : several) run[n++] = e.tail;
+                }
+                i = j;
             }
-    }
-    // stable order by (a, b): two stable counting passes, by b then by a
-    {
-        std::vector<PairEntry> by_b(entries.size());
-        std::vector<int64_t> start(N + 1, 0);
-        for (const PairEntry& e : entries) start[e.b + 1]++;
-        for (int n = 0; n < N; ++n) start[n + 1] += start[n];
-        for (const PairEntry& e : entries) by_b[start[e.b]++] = e;
-        std::fill(start.begin(), start.end(), 0);
-        for (const PairEntry& e : by_b) start[e.a + 1]++;
-        for (int n = 0; n < N; ++n) start[n + 1] += start[n];
-        for (const PairEntry& e : by_b) entries[start[e.a]++] = e;
-    }
-    L.pair_begin.push_back(0);
-    for (size_t i = 0; i < entries.size(); ++i) {
-        if (i == 0 || entries[i].a != entries[i - 1].a || entries[i].b != entries[i - 1].b) {
-            if (i > 0) L.pair_begin.push_back(static_cast<int32_t>(i));
-            L.pair_nodes.push_back(entries[i].a);
-            L.pair_nodes.push_back(entries[i].b);
+            // stable grouping of the run by b, groups in ascending b
+            group_b.clear();
+            for (size_t k = 0; k < n; ++k)
+                if (at[run[k].b]++ == 0) group_b.push_back(run[k].b);
+            std::sort(group_b.begin(), group_b.end());
+            int32_t place = static_cast<int32_t>(L.pair_entry.size());
+            for (int32_t b : group_b) {
+                L.pair_begin.push_back(place);
+                L.pair_nodes.push_back(a);
+                L.pair_nodes.push_back(b);
+                const int32_t count = at[b];
+                at[b] = place;
+                place += count;
+            }
+            L.pair_entry.resize(place);
+            for (size_t k = 0; k < n; ++k) L.pair_entry[at[run[k].b]++] = run[k].code;
+            for (int32_t b : group_b) at[b] = 0;
         }
-        L.pair_entry.push_back(entries[i].code);
+        L.pair_count = static_cast<int>(L.pair_nodes.size() / 2);
+        L.pair_begin.push_back(static_cast<int32_t>(L.pair_entry.size()));
     }
-    L.pair_count = static_cast<int>(L.pair_nodes.size() / 2);
-    L.pair_begin.resize(L.pair_count + 1);
-    L.pair_begin[L.pair_count] = static_cast<int32_t>(entries.size());
     // off-diagonal blocks: smoothness edges, then pair groups
     L.offdiag_nodes = L.edges;
     L.offdiag_nodes.insert(L.offdiag_nodes.end(), L.pair_nodes.begin(), L.pair_nodes.end());
