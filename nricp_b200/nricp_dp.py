@@ -355,9 +355,14 @@ def device_info() -> dict:
 
 
 def build_info() -> dict:
+    """The reference's keys (bindings.cpp:723-737); pybind11_version names the
+    binding layer, here ctypes over the C ABI."""
+    import platform
+
     return {"version": __version__, "build_type": "Release", "cxx_compiler": "GNU (via nvcc)",
             "cuda_toolkit": "12.9", "cuda_architectures": "100a",
-            "accelerated_precision": "float"}
+            "accelerated_precision": "float", "python_version": platform.python_version(),
+            "pybind11_version": "none (ctypes over the C ABI)"}
 
 
 def _points(a, name):
@@ -805,5 +810,60 @@ def fit_rigid(source_points, target_points, weights) -> dict:
     return {"rotation": rotation, "translation": translation}
 
 
-def serialize_report(report: str) -> dict:
-    return json.loads(report)
+def _escape(text: str) -> str:
+    return text.replace("\\", "\\\\").replace('"', '\\"').replace("\n", "\\n").replace("\t", "\\t")
+
+
+def _number(value) -> str:
+    """%.17g, or null for a non-finite value (report.cpp:35-42)."""
+    value = float(value)
+    return "%.17g" % value if math.isfinite(value) else "null"
+
+
+def serialize_report(route: str, precision: str, setup_seconds: float, solve_seconds: float, energy: dict,
+                     correspondence: dict, levels: list, settings: dict) -> str:
+    """A run report as JSON, carrying this artifact's version, in the
+    reference's exact text (bindings.cpp:1253-1312, report.cpp:44-106): the
+    energy total is the five terms summed in order, non-finite numbers are
+    null, settings keep their order."""
+    e = [float(energy[k]) for k in ("point_to_point", "point_to_plane", "smoothness", "anchor", "landmark")]
+    c = correspondence
+    out = ["{\n",
+           f'  "version": "{_escape(__version__)}",\n',
+           f'  "route": "{_escape(route)}",\n',
+           f'  "precision": "{_escape(precision)}",\n',
+           f'  "setup_seconds": {_number(setup_seconds)},\n',
+           f'  "solve_seconds": {_number(solve_seconds)},\n',
+           '  "energy": {\n',
+           f'    "point_to_point": {_number(e[0])},\n',
+           f'    "point_to_plane": {_number(e[1])},\n',
+           f'    "smoothness": {_number(e[2])},\n',
+           f'    "anchor": {_number(e[3])},\n',
+           f'    "landmark": {_number(e[4])},\n',
+           f'    "total": {_number(e[0] + e[1] + e[2] + e[3] + e[4])}\n',
+           "  },\n",
+           '  "correspondence": {\n']
+    for key in ("total", "accepted", "rejected_distance", "rejected_normal", "rejected_slope", "rejected_masked"):
+        out.append(f'    "{key}": {int(c[key])},\n')
+    out += [f'    "distance_mean": {_number(c["distance_mean"])},\n',
+            f'    "distance_p95": {_number(c["distance_p95"])},\n',
+            f'    "distance_max": {_number(c["distance_max"])}\n',
+            "  },\n",
+            '  "levels": [']
+    for i, level in enumerate(levels):
+        out.append("\n" if i == 0 else ",\n")
+        out.append(f'    {{"level": {int(level["level"])}, "nodes": {int(level["nodes"])}, '
+                   f'"outer_iterations": {int(level["outer_iterations"])}, '
+                   f'"inner_iterations": {int(level["inner_iterations"])}, '
+                   f'"energy_start": {_number(level["energy_start"])}, '
+                   f'"energy_end": {_number(level["energy_end"])}, '
+                   f'"correspondence_mean": {_number(level["correspondence_mean"])}, '
+                   f'"converged": {"true" if level["converged"] else "false"}}}')
+    out.append("],\n" if not levels else "\n  ],\n")
+    out.append('  "settings": {')
+    for i, (name, value) in enumerate(settings.items()):
+        out.append("\n" if i == 0 else ",\n")
+        out.append(f'    "{_escape(str(name))}": {_number(value)}')
+    out.append("}\n" if not settings else "\n  }\n")
+    out.append("}\n")
+    return "".join(out)

@@ -147,9 +147,32 @@ def test_plan_follows_the_reference_level_sizes(dp):
     assert dp._plan(desc) == [min(40, v), min(80, v), min(160, v)]
 
 
-def test_report_serialisation_round_trip(dp):
-    report = '{"version":"0.1.0","energy":{"total":null},"levels":[]}'
-    assert dp.serialize_report(report)["energy"]["total"] is None
+def test_report_serialisation_is_the_references_text(dp):
+    """The reference's own report of a route-A run (tests/golden), written
+    again from its parsed values, comes out byte for byte (report.cpp:44-106)."""
+    import json
+    from pathlib import Path
+
+    text = str(np.load(Path(__file__).parent / "golden" / "route_a_small.npz")["out_report"])
+    r = json.loads(text)
+    nan = lambda d: {k: (float("nan") if v is None else v) for k, v in d.items()}  # noqa: E731
+    again = dp.serialize_report(r["route"], r["precision"], r["setup_seconds"], r["solve_seconds"],
+                                nan(r["energy"]), nan(r["correspondence"]), [nan(x) for x in r["levels"]],
+                                nan(r["settings"]))
+    assert again == text
+
+
+def test_report_non_finite_values_are_null(dp):
+    import json
+
+    zero = {k: 0 for k in ("total", "accepted", "rejected_distance", "rejected_normal", "rejected_slope",
+                           "rejected_masked", "distance_mean", "distance_p95", "distance_max")}
+    text = dp.serialize_report("route_b", "float", 0.0, 0.0,
+                               {"point_to_point": float("nan"), "point_to_plane": 0.0, "smoothness": 0.0,
+                                "anchor": 0.0, "landmark": float("inf")}, zero, [], {})
+    report = json.loads(text)
+    assert report["energy"]["point_to_point"] is None and report["energy"]["total"] is None
+    assert report["levels"] == [] and report["settings"] == {} and '"levels": [],' in text
 
 
 def test_device_info_without_a_device(dp):
