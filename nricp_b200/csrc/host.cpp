@@ -9,6 +9,7 @@
 #include <cmath>
 #include <iomanip>
 #include <limits>
+#include <memory>
 #include <numeric>
 #include <sstream>
 #include <unordered_set>
@@ -43,6 +44,108 @@ void keep_nearest(double* sq, int* idx, int& held, int capacity, double value, i
     sq[at] = value;
     idx[at] = entry;
 }
+
+// A uniform grid over a point set for exact nearest-point searches.  The
+// searches below keep the k smallest (key, index) pairs under a strict total
+// order, so their result does not depend on the order candidates arrive in:
+// offering every point that could enter the k smallest gives exactly what a
+// scan of all points gives.  A search visits cells in shells of growing
+// Chebyshev radius around the query's cell and stops once every cell not yet
+// visited lies farther than its k-th key.  That bound takes a margin of a
+// millionth of a cell and a relative 1e-12 on squares, far above the few
+// ulps by which a rounded distance can fall below the exact one.
+class PointGrid {
+public:
+    PointGrid(const double* pts, int n) {
+        double hi[3];
+        for (int a = 0; a < 3; ++a) lo_[a] = hi[a] = n > 0 ? pts[a] : 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int a = 0; a < 3; ++a) {
+                lo_[a] = std::min(lo_[a], pts[i * 3 + a]);
+                hi[a] = std::max(hi[a], pts[i * 3 + a]);
+            }
+        double widest = 0.0;
+        for (int a = 0; a < 3; ++a) widest = std::max(widest, hi[a] - lo_[a]);
+        // cells of about one point each for a solid cloud: a few per occupied
+        // cell for points on a surface; flat extents count as a thousandth
+        double volume = 1.0;
+        for (int a = 0; a < 3; ++a) volume *= std::max(hi[a] - lo_[a], widest * 1e-3);
+        h_ = widest > 0.0 ? std::cbrt(volume / std::max(1, n)) : 1.0;
+        long cells = 1;
+        for (;;) {
+            cells = 1;
+            for (int a = 0; a < 3; ++a) {
+                dim_[a] = static_cast<int>(std::floor((hi[a] - lo_[a]) / h_)) + 1;
+                cells *= dim_[a];
+            }
+            if (cells <= 8L * n + 64) break;
+            h_ *= 1.25;
+        }
+        begin_.assign(cells + 1, 0);
+        std::vector<int32_t> cell_of(static_cast<size_t>(n));
+        for (int i = 0; i < n; ++i) {
+            long c = 0;
+            for (int a = 2; a >= 0; --a)
+                c = c * dim_[a] + std::clamp(coord(pts[i * 3 + a], a), 0, dim_[a] - 1);
+            cell_of[i] = static_cast<int32_t>(c);
+            begin_[c + 1]++;
+        }
+        for (long c = 0; c < cells; ++c) begin_[c + 1] += begin_[c];
+        items_.resize(static_cast<size_t>(n));
+        std::vector<int32_t> cursor(begin_.begin(), begin_.end() - 1);
+        for (int i = 0; i < n; ++i) items_[cursor[cell_of[i]]++] = i;
+    }
+
+    // Calls offer(point index) for every point of the cells in shell after
+    // shell around p, until done(gap) -- gap a lower bound on the distance
+    // from p to any point not yet offered -- returns true, or every cell has
+    // been offered.
+    template <class Offer, class Done>
+    void search(const double* p, Offer&& offer, Done&& done) const {
+        int c[3];
+        for (int a = 0; a < 3; ++a) c[a] = coord(p[a], a);
+        for (int r = 0;; ++r) {
+            const int x0 = std::max(c[0] - r, 0), x1 = std::min(c[0] + r, dim_[0] - 1);
+            const int y0 = std::max(c[1] - r, 0), y1 = std::min(c[1] + r, dim_[1] - 1);
+            const int z0 = std::max(c[2] - r, 0), z1 = std::min(c[2] + r, dim_[2] - 1);
+            auto visit = [&](int x, int y, int z) {
+                const long cell = (static_cast<long>(z) * dim_[1] + y) * dim_[0] + x;
+                for (int32_t k = begin_[cell]; k < begin_[cell + 1]; ++k) offer(items_[k]);
+            };
+            for (int z = z0; z <= z1; ++z)
+                for (int y = y0; y <= y1; ++y) {
+                    if (z == c[2] - r || z == c[2] + r || y == c[1] - r || y == c[1] + r) {
+                        for (int x = x0; x <= x1; ++x) visit(x, y, z);  // a face row: all of it
+                    } else {                                            // else its two ends
+                        if (c[0] - r >= 0 && c[0] - r < dim_[0]) visit(c[0] - r, y, z);
+                        if (r > 0 && c[0] + r >= 0 && c[0] + r < dim_[0]) visit(c[0] + r, y, z);
+                    }
+                }
+            bool covered = true;
+            double gap = std::numeric_limits<double>::infinity();
+            for (int a = 0; a < 3; ++a) {
+                covered = covered && c[a] - r <= 0 && c[a] + r >= dim_[a] - 1;
+                if (c[a] - r > 0) gap = std::min(gap, p[a] - (lo_[a] + (c[a] - r) * h_));
+                if (c[a] + r < dim_[a] - 1) gap = std::min(gap, lo_[a] + (c[a] + r + 1) * h_ - p[a]);
+            }
+            if (covered) return;
+            if (done(std::max(0.0, gap - h_ * 1e-6))) return;
+        }
+    }
+
+private:
+    int coord(double x, int a) const {
+        const double t = std::floor((x - lo_[a]) / h_);
+        return static_cast<int>(std::clamp(t, -1e9, 1e9));
+    }
+
+    double lo_[3], h_;
+    int dim_[3];
+    std::vector<int32_t> begin_, items_;
+};
+
+// Below this many (query, point) pairs a plain scan is as fast.
+constexpr long kGridPairs = 1L << 20;
 
 }  // namespace
 
@@ -247,13 +350,22 @@ std::vector<Binding> bind_vertices(const std::vector<double>& vertices,
     }
     if (nc <= 0) return out;
     const int support = std::max(1, std::min({max_nodes, nc, slot_cap}));
+    // the same k nearest by (squared distance, index) as a scan of all nodes
+    std::unique_ptr<PointGrid> grid;
+    if (static_cast<long>(vc) * nc > kGridPairs && nc > 64) grid = std::make_unique<PointGrid>(nodes.data(), nc);
 #pragma omp parallel for schedule(static) if (static_cast<long>(vc) * nc > 2000000)
     for (int v = 0; v < vc; ++v) {
         double best_sq[NRICP_MAX_SLOTS];
         int best_idx[NRICP_MAX_SLOTS];
         int held = 0;
         const double* p = &vertices[v * 3];
-        for (int n = 0; n < nc; ++n) keep_nearest(best_sq, best_idx, held, support, sqdist(p, &nodes[n * 3]), n);
+        if (grid) {
+            grid->search(
+                p, [&](int n) { keep_nearest(best_sq, best_idx, held, support, sqdist(p, &nodes[n * 3]), n); },
+                [&](double gap) { return held == support && best_sq[support - 1] < gap * gap * (1.0 - 1e-12); });
+        } else {
+            for (int n = 0; n < nc; ++n) keep_nearest(best_sq, best_idx, held, support, sqdist(p, &nodes[n * 3]), n);
+        }
         Binding b;
         for (int s = 0; s < NRICP_MAX_SLOTS; ++s) { b.nodes[s] = -1; b.weights[s] = 0.0; }
         b.count = support;
@@ -279,19 +391,32 @@ std::vector<int32_t> node_edges(const std::vector<double>& nodes, int neighbours
     if (n <= 1 || neighbours <= 0) return {};
     const int taken = std::min(neighbours, n - 1);
     std::vector<std::pair<int, int>> pairs(static_cast<size_t>(n) * taken);
+    // the k nearest by (distance, index), as the reference's partial sort
+    // over all other nodes orders them; through a grid when n is large
+    std::unique_ptr<PointGrid> grid;
+    if (static_cast<long>(n) * n > kGridPairs && n > 64) grid = std::make_unique<PointGrid>(nodes.data(), n);
 #pragma omp parallel for schedule(static) if (n > 512)
     for (int i = 0; i < n; ++i) {
-        std::vector<std::pair<double, int>> d;
-        d.reserve(n - 1);
-        for (int o = 0; o < n; ++o) {
-            if (o == i) continue;
+        auto distance = [&](int o) {
             const double x = nodes[i * 3] - nodes[o * 3], y = nodes[i * 3 + 1] - nodes[o * 3 + 1],
                          z = nodes[i * 3 + 2] - nodes[o * 3 + 2];
-            d.push_back({std::sqrt(x * x + y * y + z * z), o});
+            return std::sqrt(x * x + y * y + z * z);
+        };
+        std::vector<double> best_d(taken);
+        std::vector<int> best_o(taken);
+        int held = 0;
+        auto offer = [&](int o) {
+            if (o != i) keep_nearest(best_d.data(), best_o.data(), held, taken, distance(o), o);
+        };
+        if (grid) {
+            grid->search(&nodes[i * 3], offer, [&](double gap) {
+                return held == taken && best_d[taken - 1] < gap * (1.0 - 1e-12);
+            });
+        } else {
+            for (int o = 0; o < n; ++o) offer(o);
         }
-        std::partial_sort(d.begin(), d.begin() + taken, d.end());
         for (int k = 0; k < taken; ++k) {
-            const int o = d[k].second;
+            const int o = best_o[k];
             pairs[static_cast<size_t>(i) * taken + k] = {std::min(i, o), std::max(i, o)};
         }
     }

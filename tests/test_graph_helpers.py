@@ -62,3 +62,50 @@ def test_vertex_normals_are_the_references(oracle):
         assert np.array_equal(mine, checker.vertex_normals(case.target_points, case.target_faces))
     with pytest.raises(ValueError, match="missing vertex"):
         dp.vertex_normals(case.target_points[:3], case.target_faces)
+
+
+# Above a million (query, node) pairs the library searches a uniform grid over
+# the nodes instead of scanning them all; the k nearest it keeps must be the
+# scan's, ties and all.
+@pytest.mark.parametrize("shape", ["cloud", "plane", "far"])
+def test_bindings_through_the_grid_are_the_references(oracle, shape):
+    rng = np.random.default_rng(11)
+    p = rng.uniform(-1.0, 1.0, size=(20_000, 3))
+    if shape == "plane":
+        p[:, 2] = 0.0
+    p[-2000:] = p[:2000]                       # duplicates: equal distances
+    nodes = p[dp.farthest_point_seeds(p, 500)]
+    if shape == "far":                         # queries well outside the nodes' box
+        p = p * 7.0 + np.array([30.0, -5.0, 2.0])
+    mine = dp.bind_vertices(p, nodes, 4)
+    for checker in _checkers(oracle):
+        n, w, c = checker.bind_vertices(p, nodes, 4)
+        assert np.array_equal(mine["counts"], c)
+        assert np.array_equal(mine["nodes"], n[:, :4])
+        assert np.array_equal(mine["weights"], w[:, :4])
+    # eight slots (beyond the reference's four): the nearest eight by
+    # (squared distance, index), from every distance, rounded as the library does
+    eight = dp.bind_vertices(p, nodes, 8)["nodes"]
+    for rows in np.array_split(np.arange(len(p)), 10):
+        d = p[rows, None, :] - nodes[None, :, :]
+        sq = d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1] + d[..., 2] * d[..., 2]
+        order = np.lexsort((np.broadcast_to(np.arange(len(nodes)), sq.shape), sq), axis=1)[:, :8]
+        assert np.array_equal(eight[rows], order)
+
+
+def test_graph_levels_through_the_grid_are_the_references(oracle):
+    points, faces = S.latlong_ellipsoid(120, 220, (1.0, 0.8, 1.2))[:2]
+    graph = dp.build_template_graph(points, faces, levels=2, nodes_initial=1100, growth=2,
+                                    max_nodes_per_vertex=4, edge_neighbours=6)
+    center, scale = oracle.normalization(points)
+    normalized = (points - center) * scale
+    for level in graph["levels"]:
+        nodes = np.asarray(level["node_positions"])
+        assert len(nodes) > 1024               # edges: more than a million node pairs
+        for checker in _checkers(oracle):
+            assert np.array_equal(np.asarray(level["edges"]), checker.node_edges(nodes, 6))
+            n, w, c = checker.bind_vertices(normalized, nodes, 4)
+            b = level["bindings"]
+            assert np.array_equal(np.asarray(b["counts"]), c)
+            assert np.array_equal(np.asarray(b["nodes"])[:, :4], n[:, :4])
+            assert np.array_equal(np.asarray(b["weights"])[:, :4], w[:, :4])
