@@ -102,6 +102,14 @@ public:
     // been offered.
     template <class Offer, class Done>
     void search(const double* p, Offer&& offer, Done&& done) const {
+        search_cells(
+            p, [&](long cell) { for (int32_t k = begin_[cell]; k < begin_[cell + 1]; ++k) offer(items_[k]); },
+            done);
+    }
+
+    // The same walk, a cell at a time.
+    template <class Visit, class Done>
+    void search_cells(const double* p, Visit&& visit_cell, Done&& done) const {
         int c[3];
         for (int a = 0; a < 3; ++a) c[a] = coord(p[a], a);
         for (int r = 0;; ++r) {
@@ -110,7 +118,7 @@ public:
             const int z0 = std::max(c[2] - r, 0), z1 = std::min(c[2] + r, dim_[2] - 1);
             auto visit = [&](int x, int y, int z) {
                 const long cell = (static_cast<long>(z) * dim_[1] + y) * dim_[0] + x;
-                for (int32_t k = begin_[cell]; k < begin_[cell + 1]; ++k) offer(items_[k]);
+                if (begin_[cell] < begin_[cell + 1]) visit_cell(cell);
             };
             for (int z = z0; z <= z1; ++z)
                 for (int y = y0; y <= y1; ++y) {
@@ -132,6 +140,11 @@ public:
             if (done(std::max(0.0, gap - h_ * 1e-6))) return;
         }
     }
+
+    long cells() const { return static_cast<long>(begin_.size()) - 1; }
+    int32_t begin(long cell) const { return begin_[cell]; }
+    int32_t end(long cell) const { return begin_[cell + 1]; }
+    int32_t item(int32_t k) const { return items_[k]; }  // in ascending index within a cell
 
 private:
     int coord(double x, int a) const {
@@ -279,6 +292,74 @@ std::vector<double> vertex_normals(const std::vector<double>& p, const int32_t* 
 
 // sampling.cpp:47-88.  Ties go to the lowest index; a parallel sweep keeps
 // that rule by combining per-thread maxima in thread order.
+namespace {
+
+// The rest of the greedy sampling below, given the first seed, every point's
+// squared distance to it and the first point farthest from it.  A new seed s
+// can only lower the distances of points closer to it than the current
+// maximum M, so each step walks the grid's cells until the gap exceeds sqrt(M)
+// and updates those alone.  Every non-empty cell keeps its largest distance
+// and the first point holding it, and a tournament over the cells -- larger
+// distance first, then smaller index -- names the next seed: the same first
+// maximum the scan over all points finds.
+std::vector<int> seeds_through_grid(const std::vector<double>& pts, int count, std::vector<int> seeds,
+                                    std::vector<double> nearest) {
+    const int n = static_cast<int>(pts.size() / 3);
+    const PointGrid grid(pts.data(), n);
+    std::vector<int32_t> slot(grid.cells(), -1);
+    std::vector<long> cell_of_slot;
+    for (long c = 0; c < grid.cells(); ++c)
+        if (grid.begin(c) < grid.end(c)) {
+            slot[c] = static_cast<int32_t>(cell_of_slot.size());
+            cell_of_slot.push_back(c);
+        }
+    int leaves = 1;
+    while (leaves < static_cast<int>(cell_of_slot.size())) leaves *= 2;
+    std::vector<double> value(2 * leaves, -2.0);   // below any distance
+    std::vector<int> index(2 * leaves, n);
+    auto wins = [&](int a, int b) {
+        return value[a] > value[b] || (value[a] == value[b] && index[a] < index[b]);
+    };
+    auto settle = [&](long cell) {  // the cell's first maximum, then up the tree
+        int at = leaves + slot[cell];
+        double bs = -1.0;
+        int bi = n;
+        for (int32_t k = grid.begin(cell); k < grid.end(cell); ++k) {
+            const int i = grid.item(k);
+            if (nearest[i] > bs) { bs = nearest[i]; bi = i; }
+        }
+        value[at] = bs;
+        index[at] = bi;
+        for (at /= 2; at >= 1; at /= 2) {
+            const int w = wins(2 * at, 2 * at + 1) ? 2 * at : 2 * at + 1;
+            value[at] = value[w];
+            index[at] = index[w];
+        }
+    };
+    for (long c : cell_of_slot) settle(c);
+    while (static_cast<int>(seeds.size()) < count) {
+        const int s = index[1];
+        const double reach = value[1];  // no distance is larger
+        seeds.push_back(s);
+        const double* chosen = &pts[s * 3];
+        grid.search_cells(
+            chosen,
+            [&](long cell) {
+                bool lowered = false;
+                for (int32_t k = grid.begin(cell); k < grid.end(cell); ++k) {
+                    const int i = grid.item(k);
+                    const double d = sqdist(&pts[i * 3], chosen);
+                    if (d < nearest[i]) { nearest[i] = d; lowered = true; }
+                }
+                if (lowered) settle(cell);
+            },
+            [&](double gap) { return gap * gap * (1.0 - 1e-12) >= reach; });
+    }
+    return seeds;
+}
+
+}  // namespace
+
 std::vector<int> farthest_point_seeds(const std::vector<double>& pts, int count, int first) {
     const int n = static_cast<int>(pts.size() / 3);
     std::vector<int> seeds;
@@ -301,6 +382,8 @@ std::vector<int> farthest_point_seeds(const std::vector<double>& pts, int count,
     // The ranges are strided over whatever team runs the region: inside an
     // enclosing parallel region (a batch preparing wraps side by side) that
     // team is a single thread.
+    if (static_cast<long>(n) * count > kGridPairs && n > 1024 && count > 16)
+        return seeds_through_grid(pts, count, std::move(seeds), std::move(nearest));
 #ifdef _OPENMP
     const int chunks = n >= 20000 ? std::min(omp_get_max_threads(), 16) : 1;
 #else
@@ -355,9 +438,9 @@ std::vector<Binding> bind_vertices(const std::vector<double>& vertices,
     if (static_cast<long>(vc) * nc > kGridPairs && nc > 64) grid = std::make_unique<PointGrid>(nodes.data(), nc);
 #pragma omp parallel for schedule(static) if (static_cast<long>(vc) * nc > 2000000)
     for (int v = 0; v < vc; ++v) {
-        double best_sq[NRICP_MAX_SLOTS];
-        int best_idx[NRICP_MAX_SLOTS];
-        int held = 0;
+        double best_sq[NRICP_MAX_SLOTS] = {};
+        int best_idx[NRICP_MAX_SLOTS] = {};
+        int held = 0;  // reaches support: a search ends with every node offered, or its k nearest held
         const double* p = &vertices[v * 3];
         if (grid) {
             grid->search(

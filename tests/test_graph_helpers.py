@@ -109,3 +109,20 @@ def test_graph_levels_through_the_grid_are_the_references(oracle):
             assert np.array_equal(np.asarray(b["counts"]), c)
             assert np.array_equal(np.asarray(b["nodes"])[:, :4], n[:, :4])
             assert np.array_equal(np.asarray(b["weights"])[:, :4], w[:, :4])
+
+
+@pytest.mark.parametrize("shape", ["cloud", "plane", "lattice"])
+def test_seeds_through_the_grid_are_the_references(oracle, shape):
+    """Farthest-point sampling of more than a million (point, seed) pairs
+    updates only the grid cells a new seed can reach; ties (duplicates, a
+    lattice's equal distances) must still go to the first point."""
+    rng = np.random.default_rng(12)
+    p = rng.uniform(-1.0, 1.0, size=(20_000, 3))
+    if shape == "plane":
+        p[:, 2] = 0.0
+    if shape == "lattice":
+        p = np.round(p * 6.0) / 6.0
+    p[-3000:] = p[:3000]
+    mine = dp.farthest_point_seeds(p, 700, 5)
+    for checker in _checkers(oracle):
+        assert np.array_equal(mine, checker.farthest_point_seeds(p, 700, 5))
