@@ -8,14 +8,20 @@ device routes:
 * ``RouteBSession`` with ``step``, ``finished``, ``vertices``, ``report``,
   ``result`` (bindings.cpp:1510-1612)
 * ``device_info``, ``build_info``, ``build_template_graph``, ``closest_points``,
-  ``normalization``, ``bounding_box_diagonal``, ``validate_mesh``
+  ``fit_rigid``, ``normalization``, ``bounding_box_diagonal``, ``validate_*``,
+  ``clean_mesh``, ``farthest_point_seeds``, ``bind_vertices``,
+  ``vertex_normals``, ``evaluate_deformation``, ``transfer_level``,
+  ``retract_deformation``, ``tangent_difference``, ``robust_weights``,
+  ``serialize_report``
 
 plus, beyond the reference, ``solve_batch`` (many uneven wraps advanced by the
 same kernel launches) and the keyword extensions ``max_nodes_per_vertex``
 (k <= 8 bindings) and ``edge_neighbours`` (k-NN graph edges).
 
-Everything below is argument marshalling; the work happens in the CUDA
-library through its C ABI.  The FP64 route A lives only in the test oracle.
+The solves, the graph build, the closest-point query and the rigid fit run
+in the CUDA library through its C ABI; the small host helpers (deformation
+algebra, cleaning, report text) are numpy restatements, bit-exact with the
+reference's own functions.  The FP64 route A lives only in the test oracle.
 """
 
 from __future__ import annotations
@@ -380,8 +386,13 @@ def _faces(a, name):
 
 
 def bounding_box_diagonal(points) -> float:
+    """|max - min| of the bounding box, summed as the reference sums it
+    (mesh.cpp:48-69, vec3.h:62-72)."""
     p = _points(points, "points")
-    return float(np.linalg.norm(p.max(0) - p.min(0))) if len(p) else 0.0
+    if not len(p):
+        return 0.0
+    d = p.max(0) - p.min(0)
+    return math.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
 
 
 def normalization(points) -> dict:
@@ -412,6 +423,39 @@ def validate_mesh(points, faces) -> dict:
         for i, k in zip(*np.nonzero(bad)):
             problems.append(f"face {i} corner {k} index {f[i, k]} is out of range")
     return {"ok": not problems, "problems": problems}
+
+
+def clean_mesh(points, faces) -> dict:
+    """Drops degenerate faces -- a repeated corner, or a squared cross product
+    of at most 1e-12 of the squared bounding-box diagonal -- then faces whose
+    three corners repeat an earlier face's in any order (the first is kept,
+    winding and all), then the vertices no face uses, renumbering the rest in
+    order (bindings.cpp:762-778, mesh.cpp:118-173)."""
+    p = _points(points, "points")
+    f = np.asarray(faces)
+    if f.ndim != 2 or f.shape[1] != 3:
+        raise ValueError("faces must have shape (n, 3)")
+    f = np.ascontiguousarray(f.astype(np.int64))
+    check = validate_mesh(p, f)
+    if not check["ok"]:
+        raise ValueError("invalid mesh: " + "; ".join(check["problems"]))
+    diagonal = bounding_box_diagonal(p)
+    floor = 1e-12 * max(diagonal * diagonal, 1e-300)
+    a, b, c = f[:, 0], f[:, 1], f[:, 2]
+    u, v = p[b] - p[a], p[c] - p[a]
+    x = u[:, 1] * v[:, 2] - u[:, 2] * v[:, 1]
+    y = u[:, 2] * v[:, 0] - u[:, 0] * v[:, 2]
+    z = u[:, 0] * v[:, 1] - u[:, 1] * v[:, 0]
+    degenerate = (a == b) | (b == c) | (a == c) | (x * x + y * y + z * z <= floor)
+    candidates = np.nonzero(~degenerate)[0]
+    first = np.unique(np.sort(f[candidates], axis=1), axis=0, return_index=True)[1] if len(candidates) else []
+    kept = candidates[np.sort(np.asarray(first, dtype=np.int64))]
+    used = np.zeros(len(p), dtype=bool)
+    used[f[kept].reshape(-1)] = True
+    renumber = np.cumsum(used) - 1
+    return {"points": p[used], "faces": renumber[f[kept]].astype(np.int64).reshape(-1, 3),
+            "duplicate_faces": int(len(candidates) - len(kept)), "degenerate_faces": int(degenerate.sum()),
+            "isolated_vertices": int(len(p) - used.sum())}
 
 
 # ---- deformation helpers on the host (the reference's component functions) ----

@@ -322,3 +322,14 @@ class Oracle:
         self.lib.ref_transfer_level(C.c_int(len(src)), _p(src), _p(r), _p(t), C.c_int(len(dst)), _p(dst),
                                     C.c_int(max_nodes), _p(out_r), _p(out_t))
         return out_r, out_t
+
+    def clean_mesh(self, points, faces) -> dict:
+        self._reference_only("clean_mesh")
+        pts, fcs = _f64(points), _i32(faces)
+        out_p, out_f = np.zeros_like(pts), np.zeros_like(fcs)
+        counts = np.zeros(4, dtype=np.int32)
+        kept = self.lib.ref_clean_mesh(_p(pts), C.c_int(len(pts)), _p(fcs, C.c_int32), C.c_int(len(fcs)),
+                                       _p(out_p), _p(out_f, C.c_int32), _p(counts, C.c_int32))
+        return {"points": out_p[:kept], "faces": out_f[:counts[3]].astype(np.int64),
+                "duplicate_faces": int(counts[0]), "degenerate_faces": int(counts[1]),
+                "isolated_vertices": int(counts[2])}

@@ -476,6 +476,29 @@ void ref_transfer_level(int from_count, const double* from_nodes, const double* 
     store_deformation(transferred, out_rotations, out_translations);
 }
 
+// mesh.cpp:118-173 through the Python binding's steps (bindings.cpp:762-778);
+// returns the kept vertex count, faces in out_faces[0..out_counts[3]).
+int ref_clean_mesh(const double* points, int point_count, const int32_t* faces, int face_count,
+                   double* out_points, int32_t* out_faces, int* out_counts) {
+    nricp::Mesh mesh{points_of(points, point_count), faces_of(faces, face_count)};
+    const nricp::CleanReport report = nricp::clean(mesh);
+    for (std::size_t i = 0; i < mesh.vertices.size(); ++i) {
+        out_points[i * 3] = mesh.vertices[i].x;
+        out_points[i * 3 + 1] = mesh.vertices[i].y;
+        out_points[i * 3 + 2] = mesh.vertices[i].z;
+    }
+    for (std::size_t i = 0; i < mesh.faces.size(); ++i) {
+        out_faces[i * 3] = mesh.faces[i].v0;
+        out_faces[i * 3 + 1] = mesh.faces[i].v1;
+        out_faces[i * 3 + 2] = mesh.faces[i].v2;
+    }
+    out_counts[0] = report.duplicate_faces;
+    out_counts[1] = report.degenerate_faces;
+    out_counts[2] = report.isolated_vertices;
+    out_counts[3] = static_cast<int>(mesh.faces.size());
+    return static_cast<int>(mesh.vertices.size());
+}
+
 void ref_robust_weights(const char* kernel, const double* squared_residuals, int count,
                         double threshold, double* out) {
     const nricp::RobustKernel selected = nricp::robust_kernel_from_string(kernel);
