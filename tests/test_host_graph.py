@@ -1,8 +1,10 @@
-"""The library's host graph build on large templates: farthest-point sampling
-runs in parallel from 20,000 vertices up, and its seeds must not depend on the
-thread count (a batch prepares its wraps side by side, leaving each wrap's
-sampling one thread).  Checked in subprocesses with different OpenMP thread
-counts against the oracle's sequential scan (src/core/sampling.cpp)."""
+"""The library's host graph build on large templates: above a million
+(point, seed) pairs farthest-point sampling walks a grid of the points, below
+it scans them in parallel chunks from 20,000 vertices up; the bindings run in
+parallel over vertices.  The graph must not depend on the thread count (a
+batch prepares its wraps side by side, leaving each wrap one thread).
+Checked in subprocesses with different OpenMP thread counts against the
+oracle's sequential scan (src/core/sampling.cpp)."""
 
 from __future__ import annotations
 
