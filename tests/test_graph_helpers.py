@@ -126,3 +126,15 @@ def test_seeds_through_the_grid_are_the_references(oracle, shape):
     mine = dp.farthest_point_seeds(p, 700, 5)
     for checker in _checkers(oracle):
         assert np.array_equal(mine, checker.farthest_point_seeds(p, 700, 5))
+
+
+def test_seeds_of_the_chunked_scan_are_the_references(oracle):
+    """From 20,000 points up to a million (point, seed) pairs the sampling
+    scans the points in parallel chunks, each keeping its first maximum."""
+    rng = np.random.default_rng(13)
+    p = rng.normal(size=(25_000, 3))
+    p[-500:] = p[:500]
+    mine = dp.farthest_point_seeds(p, 36, 17)
+    assert len(p) * len(mine) <= 1 << 20
+    for checker in _checkers(oracle):
+        assert np.array_equal(mine, checker.farthest_point_seeds(p, 36, 17))
