@@ -102,17 +102,27 @@ public:
     // been offered.
     template <class Offer, class Done>
     void search(const double* p, Offer&& offer, Done&& done) const {
-        search_cells(
+        const bool walked = search_cells(
             p, [&](long cell) { for (int32_t k = begin_[cell]; k < begin_[cell + 1]; ++k) offer(items_[k]); },
             done);
+        if (!walked)  // every point, in index order: a scan's own order
+            for (int32_t i = 0; i < static_cast<int32_t>(items_.size()); ++i) offer(i);
     }
 
-    // The same walk, a cell at a time.
+    // The same walk, a cell at a time.  Returns false, having visited
+    // nothing, for a query beyond twice the grid's extent or not finite.
     template <class Visit, class Done>
-    void search_cells(const double* p, Visit&& visit_cell, Done&& done) const {
+    bool search_cells(const double* p, Visit&& visit_cell, Done&& done) const {
         int c[3];
         for (int a = 0; a < 3; ++a) c[a] = coord(p[a], a);
-        for (int r = 0;; ++r) {
+        // shells nearer than the grid hold nothing
+        int first = 0, widest = 1;
+        for (int a = 0; a < 3; ++a) {
+            first = std::max({first, -c[a], c[a] - (dim_[a] - 1)});
+            widest = std::max(widest, dim_[a]);
+        }
+        if (first > 2 * widest || !std::isfinite(p[0] + p[1] + p[2])) return false;
+        for (int r = first;; ++r) {
             const int x0 = std::max(c[0] - r, 0), x1 = std::min(c[0] + r, dim_[0] - 1);
             const int y0 = std::max(c[1] - r, 0), y1 = std::min(c[1] + r, dim_[1] - 1);
             const int z0 = std::max(c[2] - r, 0), z1 = std::min(c[2] + r, dim_[2] - 1);
@@ -136,8 +146,8 @@ public:
                 if (c[a] - r > 0) gap = std::min(gap, p[a] - (lo_[a] + (c[a] - r) * h_));
                 if (c[a] + r < dim_[a] - 1) gap = std::min(gap, lo_[a] + (c[a] + r + 1) * h_ - p[a]);
             }
-            if (covered) return;
-            if (done(std::max(0.0, gap - h_ * 1e-6))) return;
+            if (covered) return true;
+            if (done(std::max(0.0, gap - h_ * 1e-6))) return true;
         }
     }
 
@@ -149,7 +159,7 @@ public:
 private:
     int coord(double x, int a) const {
         const double t = std::floor((x - lo_[a]) / h_);
-        return static_cast<int>(std::clamp(t, -1e9, 1e9));
+        return t == t ? static_cast<int>(std::clamp(t, -1e9, 1e9)) : 1000000000;  // NaN: far away
     }
 
     double lo_[3], h_;
@@ -159,6 +169,14 @@ private:
 
 // Below this many (query, point) pairs a plain scan is as fast.
 constexpr long kGridPairs = 1L << 20;
+
+// The grid holds finite points only: with a NaN among them the keys are no
+// longer totally ordered and only the scan's own order gives its result.
+bool all_finite(const std::vector<double>& v) {
+    for (double x : v)
+        if (!std::isfinite(x)) return false;
+    return true;
+}
 
 }  // namespace
 
@@ -342,7 +360,7 @@ std::vector<int> seeds_through_grid(const std::vector<double>& pts, int count, s
         const double reach = value[1];  // no distance is larger
         seeds.push_back(s);
         const double* chosen = &pts[s * 3];
-        grid.search_cells(
+        grid.search_cells(  // a point of the grid itself: always walked
             chosen,
             [&](long cell) {
                 bool lowered = false;
@@ -382,7 +400,7 @@ std::vector<int> farthest_point_seeds(const std::vector<double>& pts, int count,
     // The ranges are strided over whatever team runs the region: inside an
     // enclosing parallel region (a batch preparing wraps side by side) that
     // team is a single thread.
-    if (static_cast<long>(n) * count > kGridPairs && n > 1024 && count > 16)
+    if (static_cast<long>(n) * count > kGridPairs && n > 1024 && count > 16 && all_finite(pts))
         return seeds_through_grid(pts, count, std::move(seeds), std::move(nearest));
 #ifdef _OPENMP
     const int chunks = n >= 20000 ? std::min(omp_get_max_threads(), 16) : 1;
@@ -435,7 +453,8 @@ std::vector<Binding> bind_vertices(const std::vector<double>& vertices,
     const int support = std::max(1, std::min({max_nodes, nc, slot_cap}));
     // the same k nearest by (squared distance, index) as a scan of all nodes
     std::unique_ptr<PointGrid> grid;
-    if (static_cast<long>(vc) * nc > kGridPairs && nc > 64) grid = std::make_unique<PointGrid>(nodes.data(), nc);
+    if (static_cast<long>(vc) * nc > kGridPairs && nc > 64 && all_finite(nodes))
+        grid = std::make_unique<PointGrid>(nodes.data(), nc);
 #pragma omp parallel for schedule(static) if (static_cast<long>(vc) * nc > 2000000)
     for (int v = 0; v < vc; ++v) {
         double best_sq[NRICP_MAX_SLOTS] = {};
@@ -477,7 +496,8 @@ std::vector<int32_t> node_edges(const std::vector<double>& nodes, int neighbours
     // the k nearest by (distance, index), as the reference's partial sort
     // over all other nodes orders them; through a grid when n is large
     std::unique_ptr<PointGrid> grid;
-    if (static_cast<long>(n) * n > kGridPairs && n > 64) grid = std::make_unique<PointGrid>(nodes.data(), n);
+    if (static_cast<long>(n) * n > kGridPairs && n > 64 && all_finite(nodes))
+        grid = std::make_unique<PointGrid>(nodes.data(), n);
 #pragma omp parallel for schedule(static) if (n > 512)
     for (int i = 0; i < n; ++i) {
         auto distance = [&](int o) {
@@ -485,18 +505,23 @@ std::vector<int32_t> node_edges(const std::vector<double>& nodes, int neighbours
                          z = nodes[i * 3 + 2] - nodes[o * 3 + 2];
             return std::sqrt(x * x + y * y + z * z);
         };
-        std::vector<double> best_d(taken);
         std::vector<int> best_o(taken);
-        int held = 0;
-        auto offer = [&](int o) {
-            if (o != i) keep_nearest(best_d.data(), best_o.data(), held, taken, distance(o), o);
-        };
-        if (grid) {
-            grid->search(&nodes[i * 3], offer, [&](double gap) {
-                return held == taken && best_d[taken - 1] < gap * (1.0 - 1e-12);
-            });
-        } else {
-            for (int o = 0; o < n; ++o) offer(o);
+        if (grid) {  // finite nodes: (distance, index) is a strict total order
+            std::vector<double> best_d(taken);
+            int held = 0;
+            grid->search(
+                &nodes[i * 3],
+                [&](int o) {
+                    if (o != i) keep_nearest(best_d.data(), best_o.data(), held, taken, distance(o), o);
+                },
+                [&](double gap) { return held == taken && best_d[taken - 1] < gap * (1.0 - 1e-12); });
+        } else {      // the reference's partial sort over every other node
+            std::vector<std::pair<double, int>> d;
+            d.reserve(n - 1);
+            for (int o = 0; o < n; ++o)
+                if (o != i) d.push_back({distance(o), o});
+            std::partial_sort(d.begin(), d.begin() + taken, d.end());
+            for (int k = 0; k < taken; ++k) best_o[k] = d[k].second;
         }
         for (int k = 0; k < taken; ++k) {
             const int o = best_o[k];
