@@ -67,7 +67,7 @@ def test_vertex_normals_are_the_references(oracle):
 # Above a million (query, node) pairs the library searches a uniform grid over
 # the nodes instead of scanning them all; the k nearest it keeps must be the
 # scan's, ties and all.
-@pytest.mark.parametrize("shape", ["cloud", "plane", "far"])
+@pytest.mark.parametrize("shape", ["cloud", "plane", "outside", "far"])
 def test_bindings_through_the_grid_are_the_references(oracle, shape):
     rng = np.random.default_rng(11)
     p = rng.uniform(-1.0, 1.0, size=(20_000, 3))
@@ -75,7 +75,9 @@ def test_bindings_through_the_grid_are_the_references(oracle, shape):
         p[:, 2] = 0.0
     p[-2000:] = p[:2000]                       # duplicates: equal distances
     nodes = p[dp.farthest_point_seeds(p, 500)]
-    if shape == "far":                         # queries well outside the nodes' box
+    if shape == "outside":                     # a few cells beyond the nodes' box
+        p = p + np.array([2.5, -1.0, 0.0])
+    if shape == "far":                         # beyond twice the box: the plain scan
         p = p * 7.0 + np.array([30.0, -5.0, 2.0])
     mine = dp.bind_vertices(p, nodes, 4)
     for checker in _checkers(oracle):
