@@ -8,7 +8,7 @@ device routes:
 * ``RouteBSession`` with ``step``, ``finished``, ``vertices``, ``report``,
   ``result`` (bindings.cpp:1510-1612)
 * ``device_info``, ``build_info``, ``build_template_graph``, ``closest_points``,
-  ``fit_rigid``, ``normalization``, ``bounding_box_diagonal``, ``validate_*``,
+  ``find_correspondences``, ``fit_rigid``, ``normalization``, ``bounding_box_diagonal``, ``validate_*``,
   ``clean_mesh``, ``farthest_point_seeds``, ``bind_vertices``,
   ``vertex_normals``, ``evaluate_deformation``, ``transfer_level``,
   ``retract_deformation``, ``tangent_difference``, ``robust_weights``,
@@ -794,6 +794,73 @@ def closest_points(target_points, target_faces, query_points) -> dict:
                                       P(out["triangles"], C.c_int32)))
     out["triangles"] = out["triangles"].astype(np.int64)
     return out
+
+
+def find_correspondences(target_points, target_faces, query_points, query_normals,
+                         distance_threshold: float = math.inf, min_normal_cosine: float = -1.0,
+                         min_slope: float = 0.0, mask=None) -> dict:
+    """Closest-point correspondences with the reference's filters and
+    rejection breakdown (bindings.cpp:1187-1251, correspondence.cpp:18-97).
+    The closest points come from the device query (``closest_points``); a
+    query is then, in this order, masked (mask 0, or beyond a non-empty
+    mask), rejected for distance, for its normal against the surface's
+    (queries past the end of ``query_normals`` skip this test) or for slope
+    (|n . (q - p)| / distance below ``min_slope``), else accepted.  Rejection
+    codes: 0 accepted, 1 distance, 2 normal, 3 slope, 4 masked."""
+    tp, q = _points(target_points, "target_points"), _points(query_points, "query_points")
+    tf = np.asarray(target_faces)
+    if tf.ndim != 2 or tf.shape[1] != 3:
+        raise ValueError("target_faces must have shape (n, 3)")
+    check_target = validate_mesh(tp, tf)
+    if not check_target["ok"]:
+        raise ValueError("invalid target mesh: " + "; ".join(check_target["problems"]))
+    qn = _points(query_normals, "query_normals")
+    active = np.ones(len(q), dtype=bool)
+    if mask is not None:
+        m = np.asarray(mask)
+        if m.ndim != 1:
+            raise ValueError("mask must have shape (n,)")
+        if len(m):
+            active = np.zeros(len(q), dtype=bool)
+            k = min(len(m), len(q))
+            active[:k] = m[:k].astype(np.int64) != 0
+    n = len(q)
+    points, normals, distances = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+    triangles = np.full(n, -1, dtype=np.int64)
+    rejection = np.full(n, 4, dtype=np.int64)
+    idx = np.nonzero(active)[0]
+    if len(idx):
+        found = closest_points(tp, tf, q[idx])
+        points[idx], normals[idx] = found["points"], found["normals"]
+        distances[idx], triangles[idx] = found["distances"], found["triangles"]
+        p, cn, d = points[idx], normals[idx], distances[idx]
+        code = np.zeros(len(idx), dtype=np.int64)
+        far = d > float(distance_threshold)
+        code[far] = 1
+        has_normal = idx < len(qn)
+        qni = qn[np.minimum(idx, max(len(qn) - 1, 0))] if len(qn) else np.zeros((len(idx), 3))
+        cos = qni[:, 0] * cn[:, 0] + qni[:, 1] * cn[:, 1] + qni[:, 2] * cn[:, 2]
+        turned = ~far & has_normal & (cos < float(min_normal_cosine))
+        code[turned] = 2
+        off = q[idx] - p
+        along = np.abs(cn[:, 0] * off[:, 0] + cn[:, 1] * off[:, 1] + cn[:, 2] * off[:, 2])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            slope = along / d
+        sliding = ~far & ~turned & (d > 0.0) & (slope < float(min_slope))
+        code[sliding] = 3
+        rejection[idx] = code
+    accepted = rejection == 0
+    counts = {"total": n, "accepted": int(accepted.sum()),
+              "rejected_distance": int((rejection == 1).sum()), "rejected_normal": int((rejection == 2).sum()),
+              "rejected_slope": int((rejection == 3).sum()), "rejected_masked": int((rejection == 4).sum()),
+              "distance_mean": 0.0, "distance_p95": 0.0, "distance_max": 0.0}
+    if accepted.any():
+        kept = np.sort(distances[accepted])
+        counts["distance_mean"] = float(np.cumsum(kept)[-1] / len(kept))  # summed in sorted order
+        counts["distance_p95"] = float(kept[int(min(len(kept) - 1, 0.95 * (len(kept) - 1)))])
+        counts["distance_max"] = float(kept[-1])
+    return {"points": points, "normals": normals, "distances": distances, "triangles": triangles,
+            "rejection": rejection, "accepted": accepted.astype(np.int64), "counts": counts}
 
 
 def farthest_point_seeds(points, count: int, first_index: int = 0) -> np.ndarray:

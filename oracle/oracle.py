@@ -333,3 +333,23 @@ class Oracle:
         return {"points": out_p[:kept], "faces": out_f[:counts[3]].astype(np.int64),
                 "duplicate_faces": int(counts[0]), "degenerate_faces": int(counts[1]),
                 "isolated_vertices": int(counts[2])}
+
+    def find_correspondences(self, target_points, target_faces, query_points, query_normals,
+                             distance_threshold=np.inf, min_normal_cosine=-1.0, min_slope=0.0, mask=None):
+        self._reference_only("find_correspondences")
+        tp, tf, q, qn = _f64(target_points), _i32(target_faces), _f64(query_points), _f64(query_normals)
+        m = np.zeros(0, dtype=np.uint8) if mask is None else (np.asarray(mask) != 0).astype(np.uint8)
+        n = len(q)
+        out = dict(points=np.zeros((n, 3)), normals=np.zeros((n, 3)), distances=np.zeros(n),
+                   triangles=np.zeros(n, dtype=np.int32), rejection=np.zeros(n, dtype=np.int32))
+        ints, stats = np.zeros(6, dtype=np.int32), np.zeros(3)
+        self.lib.ref_find_correspondences(
+            _p(tp), C.c_int(len(tp)), _p(tf, C.c_int32), C.c_int(len(tf)), _p(q), C.c_int(n), _p(qn),
+            C.c_int(len(qn)), C.c_double(distance_threshold), C.c_double(min_normal_cosine),
+            C.c_double(min_slope), _p(np.ascontiguousarray(m), C.c_uint8), C.c_int(len(m)), _p(out["points"]),
+            _p(out["normals"]), _p(out["distances"]), _p(out["triangles"], C.c_int32),
+            _p(out["rejection"], C.c_int32), _p(ints, C.c_int32), _p(stats))
+        keys = ("total", "accepted", "rejected_distance", "rejected_normal", "rejected_slope", "rejected_masked")
+        out["counts"] = {**dict(zip(keys, ints.tolist())), "distance_mean": stats[0], "distance_p95": stats[1],
+                         "distance_max": stats[2]}
+        return out

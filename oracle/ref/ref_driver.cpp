@@ -23,6 +23,7 @@
 #include "energy/energy.h"
 #include "energy/robust.h"
 #include "geometry/closest_point.h"
+#include "solver/correspondence.h"
 #include "solver/fused_assembly.h"
 #include "solver/route_a.h"
 #ifdef NRICP_REF_GPU
@@ -497,6 +498,47 @@ int ref_clean_mesh(const double* points, int point_count, const int32_t* faces, 
     out_counts[2] = report.isolated_vertices;
     out_counts[3] = static_cast<int>(mesh.faces.size());
     return static_cast<int>(mesh.vertices.size());
+}
+
+// The reference's filtered correspondences (bindings.cpp:1187-1251) on its
+// own FP64 closest points; counts: the six integers, then mean, p95, max.
+void ref_find_correspondences(const double* target_points, int point_count, const int32_t* faces,
+                              int face_count, const double* queries, int query_count,
+                              const double* query_normals, int normal_count, double distance_threshold,
+                              double min_normal_cosine, double min_slope, const uint8_t* mask,
+                              int mask_count, double* out_points, double* out_normals,
+                              double* out_distances, int32_t* out_triangles, int32_t* out_rejection,
+                              int32_t* out_counts, double* out_stats) {
+    const nricp::Mesh target{points_of(target_points, point_count), faces_of(faces, face_count)};
+    nricp::VertexMask vertex_mask;
+    vertex_mask.active.assign(mask, mask + mask_count);
+    nricp::CorrespondenceSettings settings;
+    settings.distance_threshold = distance_threshold;
+    settings.min_normal_cosine = min_normal_cosine;
+    settings.min_slope = min_slope;
+    const nricp::TargetQueries queries_of(target);
+    const nricp::CorrespondenceSet set = nricp::find_correspondences(
+        queries_of, points_of(queries, query_count), points_of(query_normals, normal_count), settings,
+        vertex_mask.active.empty() ? nullptr : &vertex_mask);
+    for (int i = 0; i < query_count; ++i) {
+        const nricp::Correspondence& c = set.items[i];
+        out_points[i * 3] = c.point.x;
+        out_points[i * 3 + 1] = c.point.y;
+        out_points[i * 3 + 2] = c.point.z;
+        out_normals[i * 3] = c.normal.x;
+        out_normals[i * 3 + 1] = c.normal.y;
+        out_normals[i * 3 + 2] = c.normal.z;
+        out_distances[i] = c.distance;
+        out_triangles[i] = c.triangle;
+        out_rejection[i] = static_cast<int32_t>(c.rejection);
+    }
+    const auto& k = set.counts;
+    const int32_t ints[6] = {k.total, k.accepted, k.rejected_distance, k.rejected_normal, k.rejected_slope,
+                             k.rejected_masked};
+    std::memcpy(out_counts, ints, sizeof ints);
+    out_stats[0] = k.distance_mean;
+    out_stats[1] = k.distance_p95;
+    out_stats[2] = k.distance_max;
 }
 
 void ref_robust_weights(const char* kernel, const double* squared_residuals, int count,
