@@ -392,10 +392,15 @@ int nricp_lbvh_export(const double* target_points, int vertex_count,
  * static 8 MiB device array, so at most 262,144 faces (more returns
  * NRICP_ERR_CAPACITY).  `target_points` (V x 3), `faces` (F x 3), `codes`,
  * `order` (F), `left`, `right` (F - 1) and `bounds` (6) are device pointers;
- * the work runs on `stream` (a cudaStream_t, NULL for the default stream) and
- * the call returns once it has finished.  The first call on a device looks up
- * the array's address and should come before any stream capture.  All calls
- * share the array: calls whose work overlaps on the GPU race. */
+ * the work runs on `stream` (a cudaStream_t, NULL for the default stream).
+ * Every call synchronises `stream` (it reads back the face-index check before
+ * the build) and returns once the build has finished.  The array is reserved
+ * when the library's device code loads on a device, which under lazy module
+ * loading is the first call there: a caller that audits allocations after
+ * start-up makes one call per device during start-up, before any stream
+ * capture.  Every call looks up the array's address with the caller's device
+ * current.  All calls share the array: calls whose work overlaps on the GPU
+ * race. */
 int nricp_lbvh_export_static(const double* target_points, int vertex_count,
                              const int32_t* faces, int face_count, uint32_t* codes,
                              uint32_t* order, int32_t* left, int32_t* right,

@@ -397,7 +397,8 @@ uint32_t lbvh_build(const double* points, const int32_t* faces, int n, void* scr
     }
     const uint32_t* codes = keys[cur];
     const uint32_t* order = values[cur];
-    cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream);
+    check(cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream),
+          "hierarchy export: clearing the parent links");
     cudaMemsetAsync(arrivals, 0, sizeof(uint32_t) * n, stream);
     if (n > 1) {
         k_karras<<<blocks_for(n - 1), kThreads, 0, stream>>>(codes, n, left, right, parent);
@@ -788,6 +789,8 @@ __global__ void k_check_faces(const int32_t* __restrict__ faces, int count, int 
 
 }  // namespace
 
+void check(cudaError_t status, const char* what);  // throws CudaError (session.cu)
+
 size_t lbvh_export_scratch_bytes(int n) {
     const size_t tiles = (size_t)((n + kSortTile - 1) / kSortTile);
     const size_t pieces[] = {
@@ -829,11 +832,14 @@ bool lbvh_export_to_device(const double* points, int vertex_count, const int32_t
     int* flag = reinterpret_cast<int*>(carve(256));
 
     // the array keeps the previous call's contents: clear what starts at zero
-    cudaMemsetAsync(flag, 0, sizeof(int), stream);
+    check(cudaMemsetAsync(flag, 0, sizeof(int), stream), "hierarchy export: clearing the flag");
     k_check_faces<<<blocks_for((long)n * 3), kThreads, 0, stream>>>(faces, n, vertex_count, flag);
+    check(cudaGetLastError(), "hierarchy export: face check");
     int host_flag = 0;
-    cudaMemcpyAsync(&host_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, stream);
-    cudaStreamSynchronize(stream);
+    check(cudaMemcpyAsync(&host_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, stream),
+          "hierarchy export: reading the flag");
+    // the caller's stream is synchronised here, on every call
+    check(cudaStreamSynchronize(stream), "hierarchy export: face check");
     if (host_flag) return false;
 
     k_centroids<<<blocks_for(n), kThreads, 0, stream>>>(points, faces, n, centroids);
@@ -850,7 +856,8 @@ bool lbvh_export_to_device(const double* points, int vertex_count, const int32_t
         cur = 1 - cur;
     }
     // eight passes: the sorted arrays are back in the caller's buffers
-    cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream);
+    check(cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream),
+          "hierarchy export: clearing the parent links");
     if (n > 1) k_karras<<<blocks_for(n - 1), kThreads, 0, stream>>>(keys[cur], n, left, right, parent);
     return true;
 }

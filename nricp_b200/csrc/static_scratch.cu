@@ -8,16 +8,21 @@
 // one statically sized device array, defined below, so the call allocates
 // nothing (no cudaMalloc, no cudaFree, no allocating library routine).
 //
-// Limit: 262,144 triangles.  The array is 8 MiB on every GPU that loads this
-// library, held until the process exits.  The first call on each device looks
-// up the array's device address (cudaGetSymbolAddress, with that device
-// current); make that first call before any stream capture.  All calls share
-// the array: it keeps the previous call's contents (the build clears what
-// must start at zero), and two calls whose work overlaps on the GPU -- from
-// two host threads, or on two streams -- race on it.
+// Limit: 262,144 triangles.  The array is 8 MiB per device.  It is reserved
+// when this library's device code is loaded on that device -- with lazy module
+// loading (the CUDA 12 default) that is the first call on the device, not the
+// library's load -- and held until the process exits.  A caller that audits
+// allocations after start-up should therefore make one call per device during
+// start-up, before any stream capture.  Every call looks up the array's device
+// address (cudaGetSymbolAddress, with the caller's device current), so the
+// address stays right after the device's context is recreated.  Every call
+// also synchronises the caller's stream before it returns: it reads back the
+// face-index check before the build starts.  All calls share the array: it
+// keeps the previous call's contents (the build clears what must start at
+// zero), and two calls whose work overlaps on the GPU -- from two host
+// threads, or on two streams -- race on it.
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -40,23 +45,15 @@ constexpr size_t kStaticScratchBytes = 8u * 1024u * 1024u;
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-// The array's device address, resolved once per device with that device
-// current.  (In host code the array's name is only a stand-in for it.)
-constexpr int kMaxDevices = 64;
-std::mutex g_resolve_mutex;
-void* g_scratch_address[kMaxDevices] = {};
-
+// The array's device address on the current device.  In host code the
+// array's name is only a stand-in for it, so it is looked up on every call:
+// once the module is loaded this allocates nothing, and it never returns an
+// address from a context that has since been torn down.
 void* scratch_address() {
-    int device = 0;
-    check(cudaGetDevice(&device), "cudaGetDevice");
-    if (device < 0 || device >= kMaxDevices) throw CudaError("device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_resolve_mutex);
-    if (g_scratch_address[device] == nullptr) {
-        void* address = nullptr;
-        check(cudaGetSymbolAddress(&address, g_static_scratch), "cudaGetSymbolAddress");
-        g_scratch_address[device] = address;
-    }
-    return g_scratch_address[device];
+    void* address = nullptr;
+    check(cudaGetSymbolAddress(&address, g_static_scratch), "cudaGetSymbolAddress");
+    if (address == nullptr) throw CudaError("cudaGetSymbolAddress returned no address");
+    return address;
 }
 
 }  // namespace

@@ -978,3 +978,26 @@ def serialize_report(route: str, precision: str, setup_seconds: float, solve_sec
     out.append("}\n" if not settings else "\n  }\n")
     out.append("}\n")
     return "".join(out)
+
+
+# The reference module's entry points that this module does not provide, each
+# with the reason.  Reaching one raises AttributeError with that reason, so a
+# caller learns why instead of meeting a bare missing name.
+_NOT_PROVIDED = {
+    "solve_route_a": "the reference's FP64 CPU route (bindings.cpp:1490) is its parity reference, not "
+                     "a device route; this module runs the device routes: use solve_route_b or "
+                     "solve_route_c",
+    "energy_blocks": "the reference's CPU teaching interface (bindings.cpp:1094) is not provided",
+    "assemble_normal_equations": "the reference's CPU teaching interface (bindings.cpp:1314) is not "
+                                 "provided",
+    "solve_normal_equations": "the reference's CPU teaching interface (bindings.cpp:1371) is not "
+                              "provided",
+    "fused_system": "the reference's FP64 CPU assembly (bindings.cpp:1328) is not provided; the "
+                    "device assembly is reachable through nricp_session_inspect",
+}
+
+
+def __getattr__(name: str):
+    if name in _NOT_PROVIDED:
+        raise AttributeError(f"nricp_dp.{name} is not provided by this module: {_NOT_PROVIDED[name]}")
+    raise AttributeError(f"module 'nricp_dp' has no attribute {name!r}")

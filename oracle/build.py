@@ -4,7 +4,7 @@
   block_cholesky.c) into ``oracle/libnricp_oracle.so`` with gcc.
 * ``build_reference()`` compiles the reference's own FP64 route A from its
   sources where they lie under the reference checkout (``NRICP_REFERENCE_DIR``,
-  default ``/root/reference``) into ``oracle/_ref/libnricp_ref.so``.  The
+  default: a ``reference`` directory beside this repository) into ``oracle/_ref/libnricp_ref.so``.  The
   reference needs Eigen 3.4.0, a submodule that is not vendored with it, in two
   translation units: ``src/solver/direct_solve.cpp`` is replaced by
   ``ref/solve_direct.cpp`` (same signature, the block Cholesky restatement) and
@@ -68,7 +68,10 @@ def build_oracle(force: bool = False) -> Path:
 
 
 def reference_dir() -> Path:
-    return Path(os.environ.get("NRICP_REFERENCE_DIR", "/root/reference"))
+    """The reference checkout: NRICP_REFERENCE_DIR, else ``reference`` beside
+    this repository's root."""
+    env = os.environ.get("NRICP_REFERENCE_DIR")
+    return Path(env) if env else HERE.parent.parent / "reference"
 
 
 def build_reference(force: bool = False) -> Path | None:

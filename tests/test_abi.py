@@ -182,3 +182,15 @@ def test_device_info_without_a_device(dp):
         pytest.skip("a device is present")
     info = dp.device_info()
     assert info["available"] is False and info["device"]
+
+
+@pytest.mark.parametrize("name", ["solve_route_a", "energy_blocks", "assemble_normal_equations",
+                                  "solve_normal_equations", "fused_system"])
+def test_entry_points_not_provided_say_why(name):
+    """The reference module's FP64 CPU route and its CPU teaching interface
+    are not part of this device module: reaching one names the reason."""
+    import nricp_dp
+
+    with pytest.raises(AttributeError, match="is not provided by this module"):
+        getattr(nricp_dp, name)
+    assert not hasattr(nricp_dp, name)

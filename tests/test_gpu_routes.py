@@ -139,7 +139,7 @@ def test_a_batch_gives_each_wrap_the_result_it_gets_alone(dp, device):
 @pytest.mark.parametrize("route", ["route_b", "route_c"])
 def test_every_solve_cluster_size_gives_the_same_bits(dp, device, route):
     """The linear solve's cluster size (1 to 16 CTAs per wrap) only decides
-    which CTA computes which 8-node segment, never the order of a sum: the
+    which CTA computes which 4-node segment, never the order of a sum: the
     wraps' results must be bit-identical for every size, alone and batched."""
     cases = [S.small_case(seed=4, nodes_initial=40),           # 40 / 80 nodes: idle CTAs at 16
              S.config1(5),                                     # 50 / 100 / 200 nodes

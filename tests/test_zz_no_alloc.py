@@ -112,3 +112,31 @@ def test_static_export_rejects_meshes_beyond_its_limit(device):
     assert status == ERR_CAPACITY
     message = load().nricp_last_error().decode()
     assert "262144" in message and "nricp_lbvh_export" in message
+
+
+def _grid_at_the_limit(seed):
+    """A wavy 513 x 257 vertex grid: 2 * 512 * 256 = 262,144 triangles, the
+    static array's limit, so its largest layout (and the radix counts of every
+    sort tile) is exercised."""
+    rng = np.random.default_rng(seed)
+    ii, jj = np.meshgrid(np.arange(513), np.arange(257), indexing="ij")
+    x, y = ii / 512.0, jj / 256.0 * 0.5
+    z = 0.1 * np.sin(7.0 * x) * np.cos(11.0 * y) + rng.normal(scale=1e-3, size=x.shape)
+    points = np.stack([x, y, z], axis=-1).reshape(-1, 3)
+    v = (ii[:-1, :-1] * 257 + jj[:-1, :-1]).reshape(-1)
+    faces = np.concatenate([np.stack([v, v + 257, v + 1], 1), np.stack([v + 1, v + 257, v + 258], 1)])
+    assert len(faces) == STATIC_FACE_LIMIT
+    return np.ascontiguousarray(points, np.float64), np.ascontiguousarray(faces, np.int32)
+
+
+def test_static_export_at_exactly_its_limit(device):
+    from nricp_b200._abi import OK
+
+    points, faces = _grid_at_the_limit(5)
+    buffers = _device_buffers(points, faces)
+    status = _static_call(buffers, len(points), len(faces))
+    assert status == OK, f"status {status}"
+    got = _read(buffers, len(faces))
+    want = _host_export(points, faces)
+    for key in ("codes", "order", "left", "right", "bounds"):
+        assert np.array_equal(got[key], want[key]), key
