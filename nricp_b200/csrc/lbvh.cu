@@ -397,8 +397,7 @@ uint32_t lbvh_build(const double* points, const int32_t* faces, int n, void* scr
     }
     const uint32_t* codes = keys[cur];
     const uint32_t* order = values[cur];
-    check(cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream),
-          "hierarchy export: clearing the parent links");
+    cudaMemsetAsync(parent, 0xff, sizeof(int32_t) * 2 * n, stream);
     cudaMemsetAsync(arrivals, 0, sizeof(uint32_t) * n, stream);
     if (n > 1) {
         k_karras<<<blocks_for(n - 1), kThreads, 0, stream>>>(codes, n, left, right, parent);
