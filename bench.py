@@ -66,6 +66,12 @@ WORKLOAD = ("config 3: 64 uneven wraps batched (template 5k-50k vertices log-uni
             "nodes = V/15 over 4 levels, k=6, target 50k-500k triangles log-uniform), route B")
 INSTANCES = 64
 REFERENCE_SAMPLE = 16   # wraps per CPU-reference sample
+SAME_CONFIG_REASON = (
+    "the reference arm times the reference's FP64 route A on the 16 smallest of config 3's 64 wraps "
+    "at its own caps (k=4 bindings, 4-NN edges; src/core/sampling.h:17, graph.h:52-53), one process "
+    "per wrap: the reference cannot bind k=6, and its largest wraps take minutes each on one core. "
+    "Our line's value is all 64 wraps at k=6; its same_sample_as_reference field times this engine "
+    "on exactly the reference arm's sample and settings")
 
 
 def parse_args():
@@ -90,8 +96,16 @@ def parse_args():
                    help="profiler captures: the config-2 wrap through RouteBSession for this many "
                         "ticks, eager launches, nothing timed")
     p.add_argument("--precision-compare", metavar="IN.npz",
-                   help="CPU only: the reference's FP64 route A on config 5, against the GPU "
-                        "results of --precision")
+                   help="CPU only: the reference's FP64 route A on config 5 and its spread under "
+                        "perturbations, against the GPU results of --precision ('-': none)")
+    p.add_argument("--perturb-seeds", type=int, default=5,
+                   help="--precision-compare: independent perturbation draws per size")
+    p.add_argument("--perturb-sigmas", default="1e-12,1e-9",
+                   help="--precision-compare: perturbation sizes, relative to the target diagonal")
+    p.add_argument("--precision-cache", default=None, metavar="DIR",
+                   help="--precision-compare: store each route-A run here and reuse it")
+    p.add_argument("--precision-workers", type=int, default=0,
+                   help="--precision-compare: processes (default: the host's cores)")
     p.add_argument("--serve-rates", default="20,80",
                    help="Poisson arrival rates (requests/s) of the serving windows")
     p.add_argument("--serve-seconds", type=float, default=6.0,
@@ -293,6 +307,8 @@ def run_reference_arm(args, ranks):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded numpy generator, nricp_b200.synthetic.config3)",
         "config": {"workload": WORKLOAD, "inputs": "host memory"},
+        "same_config": False,
+        "same_config_reason": SAME_CONFIG_REASON,
         "cpu_baseline": {k: samples[-1][k] for k in ("kind", "cores", "sample")} | {
             "value": value, "unit": METRIC},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -547,7 +563,7 @@ def run_ours(args, ranks):
         roof, detail = roofline(batch, measured_peak())
 
     # ---- CPU reference sample and the fit against it ----
-    cpu, fit, reference_gpu = None, None, None
+    cpu, fit, reference_gpu, same_sample = None, None, None, None
     if ranks.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(args.seed, host_cores())
         idx = cpu.pop("indices")
@@ -570,6 +586,12 @@ def run_ours(args, ranks):
                "max_final_energy_rel_error": max(energy_errors),
                "wraps_within_1e-4": sum(1 for e in errors if e <= 1e-4)}
         reference_gpu = reference_gpu_sample(dp, cases, idx, ref_vertices)
+        same_sample = {
+            "sample": cpu["sample"], "unit": METRIC,
+            "reference_cpu_route_a": cpu["value"],
+            "ours_batched_from_host_arrays": reference_gpu.get("ours_batched"),
+            "ours_over_reference": (reference_gpu["ours_batched"] / cpu["value"]
+                                    if reference_gpu.get("ours_batched") and cpu["value"] else None)}
 
     # ---- serving: continuous batching under Poisson arrivals ----
     served = None
@@ -612,6 +634,9 @@ def run_ours(args, ranks):
         "plain": {"value": plain, "unit": METRIC,
                   "how": "the same 64 wraps one at a time (a batch of one each), device-resident"},
         "batched_vs_plain": value / plain if plain else None,
+        "same_config_as_reference": False,
+        "same_config_reason": SAME_CONFIG_REASON,
+        "same_sample_as_reference": same_sample,
         "bit_identical_alone_and_batched": f"{identical}/{len(cases)}",
         "latency_ms": {"plain_wrap": percentiles(plain_ms), "batch_step": percentiles(step_ms)},
         "gpu_launches": launches,
@@ -689,9 +714,15 @@ def run_precision_variant(args) -> None:
 def _route_a_config5(job):
     """The reference's FP64 route A on config 5 at its caps, in a worker; with
     `sigma` > 0 the template is first perturbed by N(0, sigma) per coordinate
-    (relative to the target's diagonal) -- the problem's own sensitivity."""
-    seed, sigma = job
+    (relative to the target's diagonal), drawn from generator `draw` -- the
+    problem's own sensitivity.  With a cache directory, a finished run is
+    stored there and read back instead of being solved again."""
+    seed, sigma, draw, cache = job
     sys.path.insert(0, str(ROOT))
+    path = Path(cache) / f"route_a_c5_seed{seed}_sigma{sigma:g}_draw{draw}.npz" if cache else None
+    if path is not None and path.exists():
+        done = np.load(path, allow_pickle=False)
+        return float(done["seconds"]), done["vertices"], str(done["report"])
     from nricp_b200 import synthetic as S
     from oracle.oracle import Oracle
 
@@ -700,51 +731,74 @@ def _route_a_config5(job):
     if sigma > 0.0:
         p = case.target_points
         diag = float(np.linalg.norm(p.max(0) - p.min(0)))
-        points = points + np.random.default_rng(seed + 1).normal(0.0, sigma * diag, size=points.shape)
+        points = points + np.random.default_rng(draw).normal(0.0, sigma * diag, size=points.shape)
     t0 = time.perf_counter()
     ref = Oracle("reference").solve(points, case.template_faces, case.target_points, case.target_faces,
                                     case.level_settings, **reference_options(case.options))
-    return time.perf_counter() - t0, ref["vertices"], ref["report"]
+    seconds = time.perf_counter() - t0
+    if path is not None:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        np.savez(path, seconds=seconds, vertices=ref["vertices"], report=ref["report"])
+    return seconds, ref["vertices"], ref["report"]
+
+
+def _against(vertices, report, ref_vertices, ref_report, diag) -> dict:
+    err = np.linalg.norm(np.asarray(vertices) - ref_vertices, axis=1) / diag
+    e, ref_e = json.loads(report)["energy"]["total"], json.loads(ref_report)["energy"]["total"]
+    levels, ref_levels = _level_energies(report), _level_energies(ref_report)
+    return {"max_vertex_error_over_diag": float(err.max()),
+            "rms_vertex_error_over_diag": float(np.sqrt(np.mean(err ** 2))),
+            "final_energy_rel_error": abs(e - ref_e) / abs(ref_e) if ref_e else abs(e),
+            "level_energy_rel_error": [abs(a - b) / abs(b) if b else abs(a)
+                                       for a, b in zip(levels, ref_levels)],
+            "level_energies": levels}
 
 
 def run_precision_compare(args) -> None:
     """The reference's FP64 route A (oracle/_ref) on config 5 at its caps, on
-    this host's CPU, against the GPU results in the --precision file; and
-    route A against itself on a template perturbed by 1e-9 of the diagonal."""
+    this host's CPU; route A again on templates perturbed by each of
+    --perturb-sigmas of the diagonal, each with --perturb-seeds independent
+    draws (the spread a perturbation of that size produces on its own); and,
+    unless IN.npz is '-', the GPU results of --precision placed in that
+    spread."""
     import multiprocessing as mp
 
     from nricp_b200 import synthetic as S
 
-    gpu = np.load(args.precision_compare, allow_pickle=False)
-    seed = int(gpu["seed"])
+    seed = args.seed
+    gpu = None
+    if args.precision_compare != "-":
+        gpu = np.load(args.precision_compare, allow_pickle=False)
+        seed = int(gpu["seed"])
+    sigmas = [float(x) for x in args.perturb_sigmas.split(",") if x]
+    jobs = [(seed, 0.0, 0, args.precision_cache)]
+    jobs += [(seed, sigma, 1000 + k, args.precision_cache) for sigma in sigmas for k in range(args.perturb_seeds)]
+    workers = max(1, min(args.precision_workers or host_cores(), len(jobs)))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        runs = pool.map(_route_a_config5, jobs, chunksize=1)
     case = S.config5(seed)
-    with mp.get_context("spawn").Pool(2) as pool:
-        (seconds, ref_vertices, ref_report), (_, pert_vertices, pert_report) = pool.map(
-            _route_a_config5, [(seed, 0.0), (seed, 1e-9)])
-    ref = {"vertices": ref_vertices, "report": ref_report}
     p = case.target_points
     diag = float(np.linalg.norm(p.max(0) - p.min(0)))
-    ref_v = ref["vertices"]
-    ref_e = json.loads(ref["report"])["energy"]["total"]
+    seconds, ref_v, ref_report = runs[0]
     line = {"workload": "config 5 at the reference's caps (k=4, 4-NN): GPU route B against the "
-                        "reference's FP64 route A",
-            "route_a": {"seconds": seconds, "level_energies": _level_energies(ref["report"]),
-                        "final_energy": ref_e}}
-    pert_err = np.linalg.norm(pert_vertices - ref_v, axis=1) / diag
-    pert_e = json.loads(pert_report)["energy"]["total"]
-    line["route_a_perturbed_1e-9"] = {"max_vertex_error_over_diag": float(pert_err.max()),
-                                      "rms_vertex_error_over_diag": float(np.sqrt(np.mean(pert_err ** 2))),
-                                      "final_energy_rel_error": abs(pert_e - ref_e) / abs(ref_e),
-                                      "level_energies": _level_energies(pert_report)}
-    for name in ("fp64_reductions", "fp32_reductions"):
-        v = gpu[f"{name}_capped_vertices"]
-        err = np.linalg.norm(v - ref_v, axis=1) / diag
-        report = str(gpu[f"{name}_capped_report"])
-        e = json.loads(report)["energy"]["total"]
-        line[name] = {"max_vertex_error_over_diag": float(err.max()),
-                      "rms_vertex_error_over_diag": float(np.sqrt(np.mean(err ** 2))),
-                      "final_energy_rel_error": abs(e - ref_e) / abs(ref_e) if ref_e else abs(e),
-                      "level_energies": _level_energies(report)}
+                        "reference's FP64 route A, and route A's own spread under perturbations "
+                        "of the template",
+            "route_a": {"seconds": seconds, "level_energies": _level_energies(ref_report),
+                        "final_energy": json.loads(ref_report)["energy"]["total"]},
+            "perturbed": {}}
+    for sigma in sigmas:
+        members = [_against(v, r, ref_v, ref_report, diag)
+                   for (sg, _, _, _), (_, v, r) in zip(jobs, runs) if sg == sigma]
+        spread = {k: [m[k] for m in members] for k in ("max_vertex_error_over_diag",
+                                                       "rms_vertex_error_over_diag",
+                                                       "final_energy_rel_error")}
+        spread["level_energy_rel_error"] = [list(x) for x in zip(*[m["level_energy_rel_error"]
+                                                                    for m in members])]
+        line["perturbed"][f"{sigma:g}"] = {"draws": len(members), **spread}
+    if gpu is not None:
+        for name in ("fp64_reductions", "fp32_reductions"):
+            line[name] = _against(gpu[f"{name}_capped_vertices"], str(gpu[f"{name}_capped_report"]),
+                                  ref_v, ref_report, diag)
     print(json.dumps(line), flush=True)
 
 

@@ -215,6 +215,9 @@ typedef struct NricpInspect {
     float* off_blocks;
     double damping;                              /* out: the next attempt's damping */
     double* delta;                               /* nodes x 6: the last converged solve's increment */
+    double* corr_distances;                      /* V (may be NULL): the correspondences' distances */
+    int pcg_ok, pcg_iterations;                  /* out: the last solve's outcome and iterations */
+    double pcg_residual;                         /* out: its |r| / |b| when it stopped */
 } NricpInspect;
 int nricp_session_inspect(NricpSession* session, NricpInspect* out);
 

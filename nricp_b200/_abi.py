@@ -127,6 +127,8 @@ class Inspect(C.Structure):
         ("diag", P(C.c_float)), ("rhs", P(C.c_float)),
         ("off_nodes", P(C.c_int32)), ("off_blocks", P(C.c_float)),
         ("damping", C.c_double), ("delta", P(C.c_double)),
+        ("corr_distances", P(C.c_double)), ("pcg_ok", C.c_int), ("pcg_iterations", C.c_int),
+        ("pcg_residual", C.c_double),
     ]
 
 

@@ -1031,7 +1031,11 @@ void Batch::inspect(int i, NricpInspect* out) {
     get(out->diag, D.diag[c.system], sizeof(float) * 36 * N);
     get(out->rhs, D.rhs[c.system], sizeof(float) * 6 * N);
     get(out->delta, D.delta, sizeof(double) * 6 * N);
+    if (out->corr_distances) get(out->corr_distances, D.corr_distance, sizeof(double) * V);
     out->damping = c.damping;
+    out->pcg_ok = c.pcg_ok;
+    out->pcg_iterations = c.pcg_iterations;
+    out->pcg_residual = c.pcg_residual;
     std::vector<float> rows(L.row_entry.size() / 2 * 36);
     if (!rows.empty()) get(rows.data(), D.offdiag[c.system], sizeof(float) * rows.size());
     check(cudaStreamSynchronize(stream_), "inspect");

@@ -323,7 +323,9 @@ class RouteBSession:
         reference counterpart; for checking the assembly): phase, level,
         accepted rotations / translations, correspondences in the solver's
         normalised frame, the FP32 diagonal blocks, right-hand side and
-        off-diagonal (a, b) blocks, and the accepted energy parts."""
+        off-diagonal (a, b) blocks, the accepted energy parts, the
+        correspondences' distances and the last linear solve's outcome
+        (converged, iterations, relative residual)."""
         n_max = max(self._levels)
         v = self._desc.template_points.shape[0]
         cap = max(1, n_max * 64)
@@ -332,7 +334,7 @@ class RouteBSession:
                "corr_robust": np.zeros(v), "corr_codes": np.zeros(v, np.uint8),
                "diag": np.zeros((n_max, 6, 6), np.float32), "rhs": np.zeros((n_max, 6), np.float32),
                "off_nodes": np.zeros((cap, 2), np.int32), "off_blocks": np.zeros((cap, 6, 6), np.float32),
-               "delta": np.zeros((n_max, 6))}
+               "delta": np.zeros((n_max, 6)), "corr_distances": np.zeros(v)}
         s = _abi.Inspect()
         s.off_capacity = cap
         P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
@@ -342,13 +344,15 @@ class RouteBSession:
         s.diag, s.rhs = P(out["diag"], C.c_float), P(out["rhs"], C.c_float)
         s.off_nodes, s.off_blocks = P(out["off_nodes"], C.c_int32), P(out["off_blocks"], C.c_float)
         s.delta = P(out["delta"], C.c_double)
+        s.corr_distances = P(out["corr_distances"], C.c_double)
         check(load().nricp_session_inspect(self._handle, C.byref(s)))
         n, k = s.node_count, s.off_count
         for key in ("rotations", "translations", "diag", "rhs", "delta"):
             out[key] = out[key][:n]
         out["off_nodes"], out["off_blocks"] = out["off_nodes"][:k], out["off_blocks"][:k]
         out.update(level=s.level, node_count=n, phase=s.phase, energies=list(s.energies),
-                   damping=s.damping)
+                   damping=s.damping, pcg_ok=bool(s.pcg_ok), pcg_iterations=s.pcg_iterations,
+                   pcg_residual=s.pcg_residual)
         return out
 
 

@@ -113,17 +113,20 @@ _REF_CUDA_SOURCES = ["assemble.cu", "deform_ops.cu", "gpu_level.cu", "gpu_solver
 
 
 def build_reference_gpu(force: bool = False) -> Path | None:
-    """The reference's own GPU route B (src/cuda, compiled for sm_100a with
+    """The reference's own GPU routes (src/cuda, compiled for sm_100a with
     nvcc, as its CMake does with --extended-lambda) beside its host sources,
-    with this driver's ref_solve_route_b; None when the checkout is absent.
-    A timed comparison only, never a checker."""
+    with this driver's ref_solve_route_b / ref_solve_route_c and
+    ref/ref_lbvh.cu's ref_lbvh_build; None when the checkout is absent.  Route
+    B is a timed comparison; route C and the hierarchy anchor the FP64 route-C
+    and LBVH restatements in the GPU tests."""
     src = reference_dir() / "src"
     if not (src / "cuda" / "gpu_solver.cu").exists():
         return REF_GPU_LIB if REF_GPU_LIB.exists() else None
     REF_DIR.mkdir(exist_ok=True)
     cuda_sources = [src / "cuda" / s for s in _REF_CUDA_SOURCES]
     host_sources = [src / s for s in _REF_SOURCES]
-    own = [HERE / "ref" / "ref_driver.cpp", HERE / "ref" / "solve_direct.cpp", HERE / "block_cholesky.c"]
+    own = [HERE / "ref" / "ref_driver.cpp", HERE / "ref" / "solve_direct.cpp", HERE / "block_cholesky.c",
+           HERE / "ref" / "ref_lbvh.cu"]
     deps = cuda_sources + host_sources + own
     if not (force or _stale(REF_GPU_LIB, deps)):
         return REF_GPU_LIB

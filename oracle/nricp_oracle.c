@@ -1229,6 +1229,36 @@ int oracle_solve_direct(int node_count, const double* diagonal, int off_count,
     return solve_damped(&s, damping, diagonal_scaling, delta);
 }
 
+/* The statistics step of find_correspondences (correspondence.cpp:59-94):
+ * tally each outcome; sort the accepted distances ascending, sum them in that
+ * order for the mean, take element floor(min(n - 1, 0.95 (n - 1))) as the
+ * 95th percentile and the last as the maximum. */
+void oracle_summarize(int count, const uint8_t* codes, const double* distances,
+                      int32_t counts[6], double stats[3]) {
+    for (int k = 0; k < 6; ++k) counts[k] = 0;
+    stats[0] = stats[1] = stats[2] = 0.0;
+    double* accepted = (double*)malloc(sizeof(double) * (size_t)(count > 0 ? count : 1));
+    int na = 0;
+    for (int i = 0; i < count; ++i) {
+        const int code = codes[i];
+        if (code > 4) continue;
+        counts[0]++;
+        counts[code == 0 ? 1 : code + 1]++;
+        if (code == 0) accepted[na++] = distances[i];
+    }
+    if (na > 0) {
+        qsort(accepted, (size_t)na, sizeof(double), cmp_double);
+        double sum = 0.0;
+        for (int i = 0; i < na; ++i) sum += accepted[i];
+        stats[0] = sum / na;
+        double pi = 0.95 * (double)(na - 1);
+        if (pi > (double)(na - 1)) pi = (double)(na - 1);
+        stats[1] = accepted[(size_t)pi];
+        stats[2] = accepted[na - 1];
+    }
+    free(accepted);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Route C (device global/local), FP64: src/cuda/local_global.cu             */
 /* ------------------------------------------------------------------------ */

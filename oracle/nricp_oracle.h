@@ -94,6 +94,13 @@ int oracle_solve_direct(int node_count, const double* diagonal, int off_count,
                         const double* off_blocks, const double* rhs,
                         double damping, int diagonal_scaling, double* delta);
 
+/* Correspondence statistics (correspondence.cpp:59-94) over per-vertex
+ * outcome codes (0 accepted, 1 distance, 2 normal, 3 slope, 4 masked) and
+ * distances: counts[6] = total, accepted, rejected by distance, normal,
+ * slope, masked; stats[3] = mean, p95, max of the accepted distances. */
+void oracle_summarize(int count, const uint8_t* codes, const double* distances,
+                      int32_t counts[6], double stats[3]);
+
 /* Horn's closed-form rotation from a 3x3 correlation (local_global.cu:53-157),
  * FP64 Jacobi on the 4x4. */
 void oracle_horn_rotation(const double correlation[9], double rotation[9]);

@@ -96,10 +96,14 @@ class Oracle:
                          level_settings, route=0, **kwargs)
         out = _abi.ResultBuffers(desc.template_points.shape[0], desc.level_node_counts())
         if self.kind in ("reference", "reference_gpu"):
-            if route != ROUTE_A:
+            if route != ROUTE_A and self.kind == "reference":
                 raise ValueError("the reference has no CPU route C")
-            # the GPU build runs the reference's route B on the device instead
-            fn = self.lib.ref_solve_route_b if self.kind == "reference_gpu" else self.lib.ref_solve_route_a
+            # the GPU build runs the reference's device routes instead: route B
+            # in place of route A, and its own route C
+            if self.kind == "reference_gpu":
+                fn = self.lib.ref_solve_route_c if route == ROUTE_C else self.lib.ref_solve_route_b
+            else:
+                fn = self.lib.ref_solve_route_a
             fn.argtypes = [C.POINTER(_abi.SolveDesc), C.POINTER(_abi.Result)]
             status = fn(C.byref(desc.struct), C.byref(out.struct))
             if status:
@@ -252,6 +256,37 @@ class Oracle:
                                      _p(b, C.c_int32), _p(blocks), _p(r), C.c_double(damping),
                                      C.c_int(int(diagonal_scaling)), _p(delta))
         return bool(ok), delta.reshape(-1, 6)
+
+    def summarize(self, codes, distances) -> dict:
+        """The correspondence statistics (correspondence.cpp:59-94) of
+        per-vertex outcome codes and distances, with the report's keys."""
+        lib = _load("restatement")
+        cd = np.ascontiguousarray(np.asarray(codes, dtype=np.uint8))
+        d = _f64(distances)
+        counts, stats = np.zeros(6, dtype=np.int32), np.zeros(3)
+        lib.oracle_summarize(C.c_int(len(cd)), _p(cd, C.c_uint8), _p(d), _p(counts, C.c_int32), _p(stats))
+        keys = ("total", "accepted", "rejected_distance", "rejected_normal", "rejected_slope", "rejected_masked")
+        return {**dict(zip(keys, counts.tolist())), "distance_mean": float(stats[0]),
+                "distance_p95": float(stats[1]), "distance_max": float(stats[2])}
+
+    def reference_lbvh(self, points, faces) -> dict:
+        """The reference's own device hierarchy (Lbvh::build, src/cuda/lbvh.cu:
+        553-668), read back: sorted codes, permutation and Karras children in
+        the export's numbering.  Needs the GPU build (kind "reference_gpu")."""
+        if self.kind != "reference_gpu":
+            raise ValueError("the reference's hierarchy needs Oracle('reference_gpu')")
+        pts, fcs = _f64(points), _i32(faces)
+        n = len(fcs)
+        out = dict(codes=np.zeros(n, np.uint32), order=np.zeros(n, np.uint32),
+                   left=np.zeros(max(1, n - 1), np.int32), right=np.zeros(max(1, n - 1), np.int32))
+        status = self.lib.ref_lbvh_build(_p(pts), C.c_int(len(pts)), _p(fcs, C.c_int32), C.c_int(n),
+                                         _p(out["codes"], C.c_uint32), _p(out["order"], C.c_uint32),
+                                         _p(out["left"], C.c_int32), _p(out["right"], C.c_int32))
+        if status:
+            self.lib.ref_lbvh_last_error.restype = C.c_char_p
+            raise RuntimeError(self.lib.ref_lbvh_last_error().decode())
+        out["left"], out["right"] = out["left"][: n - 1], out["right"][: n - 1]
+        return out
 
     def lbvh_build(self, points_f32, faces):
         lib = _load("restatement")

@@ -205,6 +205,16 @@ int ref_solve_route_b(const NricpSolveDesc* desc, NricpResult* out) {
         return nricp::solve_route_b(tpl, tgt, graph, settings, mask, landmarks);
     });
 }
+
+// The reference's own GPU route C (src/cuda/gpu_solver.cu, local_global.cu):
+// the anchor for the FP64 route-C restatement, which has no CPU counterpart.
+int ref_solve_route_c(const NricpSolveDesc* desc, NricpResult* out) {
+    return solve_with(desc, out, [](const nricp::Mesh& tpl, const nricp::Mesh& tgt, const nricp::TemplateGraph& graph,
+                                    const nricp::RouteSettings& settings, const nricp::VertexMask* mask,
+                                    const std::vector<nricp::Landmark>& landmarks) {
+        return nricp::solve_route_c(tpl, tgt, graph, settings, mask, landmarks);
+    });
+}
 #endif
 
 int ref_farthest_point_seeds(const double* points, int count, int seeds, int first,
