@@ -28,8 +28,10 @@ Printed (one JSON line on rank 0):
 * ``cpu_baseline`` the reference's own route A (compiled from its sources,
                    oracle/_ref) on the host cores, on a bounded sample,
 * ``served``       the same wraps as requests arriving in Poisson windows
-                   (20 and 80 per second by default) served with continuous
-                   batching: throughput and p50/p99 latency per window,
+                   (config 4's 5, 20 and 80 per second by default; 5 is below
+                   the server's capacity) served with continuous batching:
+                   throughput, p50/p99 latency and p50/p99 of each phase of
+                   a request's latency per window,
 * ``single_wrap``  the large single wrap of config 2 (25k vertices onto a
                    393k-triangle target, 2,000 nodes) one at a time.
 
@@ -106,7 +108,7 @@ def parse_args():
                    help="--precision-compare: store each route-A run here and reuse it")
     p.add_argument("--precision-workers", type=int, default=0,
                    help="--precision-compare: processes (default: the host's cores)")
-    p.add_argument("--serve-rates", default="20,80",
+    p.add_argument("--serve-rates", default="5,20,80",
                    help="Poisson arrival rates (requests/s) of the serving windows")
     p.add_argument("--serve-seconds", type=float, default=6.0,
                    help="length of each serving window (the full protocol: 60)")
@@ -421,11 +423,13 @@ def serve_window(server, cases, rate: float, seconds: float, rng, large=(), larg
         else:
             c = cases[int(rng.integers(len(cases)))]
         submitted.append((time.perf_counter(), server.submit(*c.args(), **c.options)))
-    latencies, finished = [], []
+    latencies, finished, phases = [], [], {k: [] for k in server.PHASES}
     for ts, rid in submitted:
         state, latency = server.wait(rid, timeout=900.0)
         if state != "done":
             raise RuntimeError(f"served request {rid} ended {state}")
+        for k, v in server.phases(rid).items():
+            phases[k].append(1000.0 * v)
         server.result(rid)
         latencies.append(1000.0 * latency)
         finished.append(ts + latency)
@@ -433,6 +437,8 @@ def serve_window(server, cases, rate: float, seconds: float, rng, large=(), larg
     out = {"rate_per_s": rate, "seconds": seconds, "requests": len(submitted), "large_requests": large_count,
            "wraps_per_second": len(submitted) / span if span > 0 else 0.0}
     out.update({f"latency_{k}_ms": v for k, v in percentiles(latencies).items() if k != "n"})
+    out["phase_ms"] = {k: {q: round(x, 2) for q, x in percentiles(v).items() if q != "n"}
+                       for k, v in phases.items()}
     return out
 
 

@@ -198,7 +198,9 @@ int nricp_session_ticks(NricpSession* session, long* ticks, long* launches);
  * Blocks appear once per smoothness edge and once per node pair that shares
  * a vertex, so one pair may appear twice; their sum is the system's block.
  * Also the damping of the next attempt and the last converged solve's
- * increment (nodes x 6). */
+ * increment (nodes x 6), the correspondences' distances, the last solve's
+ * outcome, and the target as the device holds it.  A NULL output pointer is
+ * skipped. */
 typedef struct NricpInspect {
     int level, node_count, phase, off_count;     /* out */
     int off_capacity;                            /* in */
@@ -218,6 +220,8 @@ typedef struct NricpInspect {
     double* corr_distances;                      /* V (may be NULL): the correspondences' distances */
     int pcg_ok, pcg_iterations;                  /* out: the last solve's outcome and iterations */
     double pcg_residual;                         /* out: its |r| / |b| when it stopped */
+    double* target_points;                       /* Vt x 3 (may be NULL): the target, normalised */
+    double* target_normals;                      /* Vt x 3 (may be NULL): its vertex normals */
 } NricpInspect;
 int nricp_session_inspect(NricpSession* session, NricpInspect* out);
 
@@ -323,6 +327,12 @@ int nricp_server_create(const NricpServerConfig* config, NricpServer** out);
 int nricp_server_submit(NricpServer* server, const NricpSolveDesc* desc, long* id);
 /* Status of a request and, once done, its latency (submit to result ready). */
 int nricp_server_poll(NricpServer* server, long id, int* status, double* latency_seconds);
+/* No reference counterpart.  Where a request's latency went, in seconds, so
+ * far: seconds[0] host preparation (graph, level layouts), [1] loading
+ * (waiting for memory, uploads, target hierarchy), [2] waiting for a slot,
+ * [3] on the device, [4] composing the result; a phase not reached yet is 0.
+ * Valid until nricp_server_result takes the request. */
+int nricp_server_phases(NricpServer* server, long id, double* seconds);
 /* Blocks until the request is done or failed, or `timeout_seconds` pass
  * (NRICP_ERR_TIMEOUT). */
 int nricp_server_wait(NricpServer* server, long id, double timeout_seconds);

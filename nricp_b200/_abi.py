@@ -128,7 +128,7 @@ class Inspect(C.Structure):
         ("off_nodes", P(C.c_int32)), ("off_blocks", P(C.c_float)),
         ("damping", C.c_double), ("delta", P(C.c_double)),
         ("corr_distances", P(C.c_double)), ("pcg_ok", C.c_int), ("pcg_iterations", C.c_int),
-        ("pcg_residual", C.c_double),
+        ("pcg_residual", C.c_double), ("target_points", P(C.c_double)), ("target_normals", P(C.c_double)),
     ]
 
 

@@ -86,6 +86,7 @@ def _declare(lib: C.CDLL) -> None:
         "nricp_server_create": (C.c_int, [P(_abi.ServerConfig), P(C.c_void_p)]),
         "nricp_server_submit": (C.c_int, [C.c_void_p, desc_p, P(C.c_long)]),
         "nricp_server_poll": (C.c_int, [C.c_void_p, C.c_long, P(C.c_int), P(C.c_double)]),
+        "nricp_server_phases": (C.c_int, [C.c_void_p, C.c_long, P(C.c_double)]),
         "nricp_server_wait": (C.c_int, [C.c_void_p, C.c_long, C.c_double]),
         "nricp_server_result": (C.c_int, [C.c_void_p, C.c_long, result_p]),
         "nricp_server_stats": (C.c_int, [C.c_void_p, P(_abi.ServerStats)]),

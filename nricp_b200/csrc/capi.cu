@@ -668,6 +668,13 @@ int nricp_server_poll(NricpServer* s, long id, int* status, double* latency_seco
     });
 }
 
+int nricp_server_phases(NricpServer* s, long id, double* seconds) {
+    return guarded([&] {
+        const auto [lane, inner] = s->find(id);
+        s->lanes[lane]->phases(inner, seconds);
+    });
+}
+
 int nricp_server_wait(NricpServer* s, long id, double timeout_seconds) {
     return guarded([&] {
         const auto [lane, inner] = s->find(id);

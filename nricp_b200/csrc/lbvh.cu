@@ -16,6 +16,9 @@
 // triangle it reaches is measured with the reference's FP64 closest-point
 // routine (src/geometry/closest_point.cpp:24-121), so the winner, its point,
 // normal and distance are those of an FP64 brute-force scan.
+#include <algorithm>
+#include <cmath>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -419,6 +422,414 @@ uint32_t lbvh_build(const double* points, const int32_t* faces, int n, void* scr
 }
 
 // ---------------------------------------------------------------------------
+// Hierarchical cell index over the target's triangles
+// ---------------------------------------------------------------------------
+//
+// A seeded query already knows a triangle at distance d; every triangle that
+// could beat it has a point within d of the query, so it overlaps one of the
+// cells that the box [q - d, q + d] touches, at the level it is listed in.
+// Those cells are computed from the query's coordinates, so a query reads
+// their entries with a few rounds of independent loads instead of a
+// root-to-leaf chain of dependent node fetches.  A triangle is listed at the
+// finest level whose cell is at least its largest box extent (so in at most
+// eight cells there): the long spikes that off-surface outlier vertices make
+// sit a level or two up instead of in hundreds of fine cells.
+
+namespace {
+
+// Level-0 cell size in mean triangle edges (the edge of an equilateral
+// triangle of the mean area); each level above is 4x coarser; the most cells
+// (all levels) per target triangle the index may take.
+constexpr double kCellEdges = 1.5;
+constexpr double kCellRatio = 4.0;
+constexpr long kCellsPerTriangle = 8;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+struct CellParams {
+    double origin[3];
+    double inv[kCellLevels];
+    int dims[kCellLevels][3];
+    long first[kCellLevels];
+    int levels;
+};
+
+__device__ inline void leaf_corners(const float4* leaves, int leaf, double c[9]) {
+    const double2* l = reinterpret_cast<const double2*>(leaves) + (long)leaf * kLeafFloat4s;
+    const double2 l0 = l[0], l1 = l[1], l2 = l[2], l3 = l[3], l4 = l[4];
+    c[0] = l0.x; c[1] = l0.y; c[2] = l1.x;
+    c[3] = l1.y; c[4] = l2.x; c[5] = l2.y;
+    c[6] = l3.x; c[7] = l3.y; c[8] = l4.x;
+}
+
+// A triangle's level and its cell range there, per axis.
+__host__ __device__ inline int triangle_cells(const double c[9], const double origin[3], const double* inv,
+                                              const int (*dims)[3], int levels, int lo[3], int hi[3]) {
+    double mn[3], mx[3], extent = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        mn[k] = fmin(c[k], fmin(c[3 + k], c[6 + k]));
+        mx[k] = fmax(c[k], fmax(c[3 + k], c[6 + k]));
+        extent = fmax(extent, mx[k] - mn[k]);
+    }
+    const int l = cell_level(extent, inv, levels);
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = cell_coord(mn[k], origin[k], inv[l], dims[l][k]);
+        hi[k] = cell_coord(mx[k], origin[k], inv[l], dims[l][k]);
+    }
+    return l;
+}
+
+__device__ inline long cell_id(const CellParams& P, int l, int x, int y, int z) {
+    return P.first[l] + x + (long)P.dims[l][0] * (y + (long)P.dims[l][1] * z);
+}
+
+__global__ void k_cell_count(const float4* __restrict__ leaves, int n, CellParams P,
+                             int32_t* __restrict__ counts) {
+    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    double c[9];
+    leaf_corners(leaves, leaf, c);
+    int lo[3], hi[3];
+    const int l = triangle_cells(c, P.origin, P.inv, P.dims, P.levels, lo, hi);
+    for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int x = lo[0]; x <= hi[0]; ++x) atomicAdd(&counts[cell_id(P, l, x, y, z)], 1);
+}
+
+// Each cell's counter starts at the cell's first entry; taking a slot moves it
+// on, so when every triangle is in, counter c holds the end of cell c.
+__global__ void k_cell_fill(const float4* __restrict__ leaves, int n, CellParams P,
+                            int32_t* __restrict__ cursor, float4* __restrict__ entries,
+                            int capacity, int* __restrict__ error) {
+    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    double c[9];
+    leaf_corners(leaves, leaf, c);
+    int lo[3], hi[3];
+    const int l = triangle_cells(c, P.origin, P.inv, P.dims, P.levels, lo, hi);
+    // the FP32 box the traversal prunes with (the corners rounded to FP32)
+    float blo[3], bhi[3];
+    for (int k = 0; k < 3; ++k) {
+        const float a = __double2float_rn(c[k]), b = __double2float_rn(c[3 + k]),
+                    d = __double2float_rn(c[6 + k]);
+        blo[k] = fminf(a, fminf(b, d));
+        bhi[k] = fmaxf(a, fmaxf(b, d));
+    }
+    const float4 e0 = make_float4(blo[0], blo[1], blo[2], __int_as_float(leaf));
+    const float4 e1 = make_float4(bhi[0], bhi[1], bhi[2], 0.0f);
+    for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int x = lo[0]; x <= hi[0]; ++x) {
+                const int at = atomicAdd(&cursor[cell_id(P, l, x, y, z)], 1);
+                if (at < 0 || at >= capacity) {
+                    atomicOr(error, 2);
+                    continue;
+                }
+                entries[(long)at * 2] = e0;
+                entries[(long)at * 2 + 1] = e1;
+            }
+}
+
+// Exclusive scan of n ints in place: tiles of kScanTile scanned by one block
+// each (their totals to `sums`), the totals scanned by one block, then added.
+__device__ inline int block_exclusive_scan(int value, int* warp_totals, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = value;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_totals[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        int t = lane < nw ? warp_totals[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < nw) warp_totals[lane] = t;  // inclusive
+        if (lane == 31) *total = t;
+    }
+    __syncthreads();
+    const int before = warp == 0 ? 0 : warp_totals[warp - 1];
+    return before + x - value;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __restrict__ data, long n,
+                                                            int32_t* __restrict__ sums) {
+    __shared__ int warp_totals[32];
+    __shared__ int total;
+    const long base = (long)blockIdx.x * kScanTile + (long)threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int local = 0;
+    for (int i = 0; i < kScanItems; ++i) {
+        v[i] = base + i < n ? data[base + i] : 0;
+        local += v[i];
+    }
+    int run = block_exclusive_scan(local, warp_totals, &total);
+    for (int i = 0; i < kScanItems; ++i) {
+        if (base + i < n) data[base + i] = run;
+        run += v[i];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int32_t* __restrict__ sums, int tiles) {
+    __shared__ int warp_totals[32];
+    __shared__ int total;
+    int carry = 0;
+    for (int base = 0; base < tiles; base += kScanThreads) {
+        const int i = base + (int)threadIdx.x;
+        const int v = i < tiles ? sums[i] : 0;
+        const int ex = block_exclusive_scan(v, warp_totals, &total);
+        if (i < tiles) sums[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_add(int32_t* __restrict__ data, long n,
+                                                          const int32_t* __restrict__ sums) {
+    const long base = (long)blockIdx.x * kScanTile + (long)threadIdx.x * kScanItems;
+    const int add = sums[blockIdx.x];
+    for (int i = 0; i < kScanItems; ++i)
+        if (base + i < n) data[base + i] += add;
+}
+
+}  // namespace
+
+CellPlan plan_cells(const double* p, int n, const int32_t* f, int F, const double center[3], double scale) {
+    CellPlan plan;
+    if (n <= 0 || F <= 0 || !(scale > 0.0)) return plan;
+    // the normalised box: normalisation is monotone in each coordinate, so its
+    // corners are the normalised corners of the caller's box
+    double lo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, hi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const double x = p[(long)i * 3 + k];
+            if (!std::isfinite(x)) return plan;  // the hierarchy alone handles such targets
+            lo[k] = std::min(lo[k], x);
+            hi[k] = std::max(hi[k], x);
+        }
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = (lo[k] - center[k]) * scale;
+        hi[k] = (hi[k] - center[k]) * scale;
+    }
+    // the mean triangle area, from an evenly spaced sample of the triangles
+    const int samples = std::min(F, 4096);
+    double area = 0.0;
+    for (int i = 0; i < samples; ++i) {
+        const int32_t* fc = f + (long)((long)i * F / samples) * 3;
+        if (fc[0] < 0 || fc[0] >= n || fc[1] < 0 || fc[1] >= n || fc[2] < 0 || fc[2] >= n) return plan;
+        const double* a = p + (long)fc[0] * 3;
+        const double* b = p + (long)fc[1] * 3;
+        const double* c = p + (long)fc[2] * 3;
+        const double u[3] = {(b[0] - a[0]) * scale, (b[1] - a[1]) * scale, (b[2] - a[2]) * scale};
+        const double v[3] = {(c[0] - a[0]) * scale, (c[1] - a[1]) * scale, (c[2] - a[2]) * scale};
+        const double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2],
+                     z = u[0] * v[1] - u[1] * v[0];
+        area += 0.5 * std::sqrt(x * x + y * y + z * z);
+    }
+    const double extent = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    if (!(extent > 0.0) || !std::isfinite(extent)) return plan;
+    double size = kCellEdges * std::sqrt(area / samples * (4.0 / std::sqrt(3.0)));
+    if (!(size > 0.0) || !std::isfinite(size)) size = extent / std::cbrt((double)F);
+    // the coarsest level must hold any triangle: its cell beyond the box's extent
+    const double top_size = extent / kCellFit * 1.0001;
+    const double widest = std::pow(kCellRatio, kCellLevels - 1);
+    size = std::max(size, top_size / widest);
+    const long cap = kCellsPerTriangle * (long)F + 4096;
+    for (int attempt = 0; attempt < 64; ++attempt) {
+        int levels = 1;
+        while (levels < kCellLevels && size * std::pow(kCellRatio, levels - 1) < top_size) ++levels;
+        plan.levels = levels;
+        plan.cells = 0;
+        for (int l = 0; l < levels; ++l) {
+            // the coarsest level is exactly one box-wide cell per axis or more
+            const double level_size = l + 1 == levels ? std::max(size * std::pow(kCellRatio, l), top_size)
+                                                      : size * std::pow(kCellRatio, l);
+            plan.inv[l] = 1.0 / level_size;
+            plan.first[l] = plan.cells;
+            long cells = 1;
+            for (int k = 0; k < 3; ++k) {
+                const double t = (hi[k] - lo[k]) * plan.inv[l];
+                plan.dims[l][k] = t < (double)(1 << 20) ? (int)t + 1 : (1 << 20);
+                cells *= plan.dims[l][k];
+            }
+            plan.cells += cells;
+        }
+        if (plan.cells <= cap) break;
+        size *= std::cbrt((double)plan.cells / (double)cap) * 1.01;
+    }
+    if (plan.cells > cap) return CellPlan();
+    for (int k = 0; k < 3; ++k) plan.origin[k] = lo[k];
+    plan.entries = 8L * F;
+    if (plan.entries >= (1L << 31)) return CellPlan();
+    plan.ok = true;
+    return plan;
+}
+
+size_t cells_scratch_bytes(long cells) {
+    return sizeof(int32_t) * (size_t)((cells + kScanTile - 1) / kScanTile + 1) + 256;
+}
+
+int cells_build_launches() { return 5; }
+
+void build_cells(const float4* leaves, int n, const CellPlan& plan, int32_t* ends, float4* entries,
+                 void* scratch, int* error, cudaStream_t stream) {
+    if (!plan.ok || n <= 0) return;
+    CellParams P;
+    for (int k = 0; k < 3; ++k) P.origin[k] = plan.origin[k];
+    for (int l = 0; l < kCellLevels; ++l) {
+        P.inv[l] = plan.inv[l];
+        P.first[l] = plan.first[l];
+        for (int k = 0; k < 3; ++k) P.dims[l][k] = plan.dims[l][k];
+    }
+    P.levels = plan.levels;
+    const long cells = plan.cells;
+    const int tiles = (int)((cells + kScanTile - 1) / kScanTile);
+    int32_t* sums = static_cast<int32_t*>(scratch);
+    cudaMemsetAsync(ends, 0, sizeof(int32_t) * cells, stream);
+    k_cell_count<<<blocks_for(n), kThreads, 0, stream>>>(leaves, n, P, ends);
+    k_scan_tiles<<<tiles, kScanThreads, 0, stream>>>(ends, cells, sums);
+    k_scan_sums<<<1, kScanThreads, 0, stream>>>(sums, tiles);
+    k_scan_add<<<tiles, kScanThreads, 0, stream>>>(ends, cells, sums);
+    k_cell_fill<<<blocks_for(n), kThreads, 0, stream>>>(leaves, n, P, ends, entries, (int)plan.entries, error);
+}
+
+// ---------------------------------------------------------------------------
+// Target ingestion: normalisation and vertex normals on the device
+// ---------------------------------------------------------------------------
+//
+// The target arrives in the caller's units.  Its points are moved into the
+// normalised frame in place, (p - center) * scale per coordinate with the two
+// roundings of the host's normalisation (mesh.cpp:183-187), and its
+// area-weighted vertex normals (mesh.cpp:71-88) are summed per vertex over
+// its faces in ascending face order, as the host's face loop adds them, then
+// normalised -- so both are bit-identical to the host's.  A vertex's faces
+// come from a stable sort of the (vertex, face) corner pairs by vertex.
+
+namespace {
+
+__global__ void k_normalize(double* __restrict__ p, long count, double cx, double cy, double cz,
+                            double scale) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int k = (int)(i % 3);
+    const double c = k == 0 ? cx : (k == 1 ? cy : cz);
+    p[i] = __dmul_rn(__dsub_rn(p[i], c), scale);
+}
+
+__global__ void k_corner_keys(const int32_t* __restrict__ faces, long corners, uint32_t* __restrict__ keys,
+                              uint32_t* __restrict__ values) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= corners) return;
+    keys[i] = (uint32_t)faces[i];
+    values[i] = (uint32_t)(i / 3);
+}
+
+__device__ inline long lower_bound_key(const uint32_t* __restrict__ keys, long n, uint32_t x) {
+    long lo = 0, hi = n;
+    while (lo < hi) {
+        const long mid = (lo + hi) >> 1;
+        if (keys[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_target_normals(const double* __restrict__ p, int n, const int32_t* __restrict__ faces,
+                                 const uint32_t* __restrict__ keys, const uint32_t* __restrict__ face_of,
+                                 long corners, double* __restrict__ normals) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    const long j0 = lower_bound_key(keys, corners, (uint32_t)v);
+    const long j1 = lower_bound_key(keys, corners, (uint32_t)v + 1u);
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (long j = j0; j < j1; ++j) {
+        const int32_t* f = faces + (long)face_of[j] * 3;
+        const double* a = p + (long)f[0] * 3;
+        const double* b = p + (long)f[1] * 3;
+        const double* c = p + (long)f[2] * 3;
+        const double e10 = __dsub_rn(b[0], a[0]), e11 = __dsub_rn(b[1], a[1]), e12 = __dsub_rn(b[2], a[2]);
+        const double e20 = __dsub_rn(c[0], a[0]), e21 = __dsub_rn(c[1], a[1]), e22 = __dsub_rn(c[2], a[2]);
+        t0 = __dadd_rn(t0, __dsub_rn(__dmul_rn(e11, e22), __dmul_rn(e12, e21)));
+        t1 = __dadd_rn(t1, __dsub_rn(__dmul_rn(e12, e20), __dmul_rn(e10, e22)));
+        t2 = __dadd_rn(t2, __dsub_rn(__dmul_rn(e10, e21), __dmul_rn(e11, e20)));
+    }
+    const double length =
+        __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(t0, t0), __dmul_rn(t1, t1)), __dmul_rn(t2, t2)));
+    double* out = normals + (long)v * 3;
+    if (length > 0.0) {
+        out[0] = __ddiv_rn(t0, length);
+        out[1] = __ddiv_rn(t1, length);
+        out[2] = __ddiv_rn(t2, length);
+    } else {
+        out[0] = out[1] = out[2] = 0.0;
+    }
+}
+
+// Radix passes that cover vertex indices below n, rounded up to an even
+// count so that the sorted arrays end in the first buffer.
+int corner_sort_passes(int n) {
+    int bits = 1;
+    while (bits < 32 && (1u << bits) < (uint32_t)n) ++bits;
+    const int passes = (bits + kRadixBits - 1) / kRadixBits;
+    return passes + (passes & 1);
+}
+
+}  // namespace
+
+size_t ingest_scratch_bytes(int n, int F) {
+    const size_t corners = (size_t)F * 3;
+    const size_t tiles = (corners + kSortTile - 1) / kSortTile;
+    const size_t pieces[] = {sizeof(uint32_t) * corners, sizeof(uint32_t) * corners,
+                             sizeof(uint32_t) * corners, sizeof(uint32_t) * corners,
+                             sizeof(uint32_t) * kRadix * (tiles + 1)};
+    size_t total = 0;
+    for (size_t bytes : pieces) total += (bytes + 255) & ~size_t(255);
+    (void)n;
+    return total + 256;
+}
+
+int ingest_launches(int n, int F) { return 2 + 3 * corner_sort_passes(n) + (F > 0 ? 1 : 0); }
+
+void ingest_target(double* points, int n, const int32_t* faces, int F, const double center[3], double scale,
+                   double* normals, void* scratch, cudaStream_t stream) {
+    k_normalize<<<blocks_for((long)n * 3), kThreads, 0, stream>>>(points, (long)n * 3, center[0], center[1],
+                                                                  center[2], scale);
+    const long corners = (long)F * 3;
+    char* base = static_cast<char*>(scratch);
+    auto carve = [&base](size_t bytes) {
+        char* q = base;
+        base += (bytes + 255) & ~size_t(255);
+        return q;
+    };
+    uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * corners)),
+                         reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * corners))};
+    uint32_t* values[2] = {reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * corners)),
+                           reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * corners))};
+    const int tiles = (int)((corners + kSortTile - 1) / kSortTile);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(carve(sizeof(uint32_t) * kRadix * (tiles + 1)));
+    if (F > 0) {
+        k_corner_keys<<<blocks_for(corners), kThreads, 0, stream>>>(faces, corners, keys[0], values[0]);
+        int cur = 0;
+        const int passes = corner_sort_passes(n);
+        for (int pass = 0; pass < passes; ++pass) {
+            const int shift = pass * kRadixBits;
+            k_radix_histogram<<<tiles, kThreads, 0, stream>>>(keys[cur], (int)corners, shift, counts, tiles);
+            k_radix_scan<<<1, 1024, 0, stream>>>(counts, kRadix * tiles);
+            k_radix_scatter<<<tiles, kThreads, 0, stream>>>(keys[cur], values[cur], (int)corners, shift,
+                                                            counts, tiles, keys[1 - cur], values[1 - cur]);
+            cur = 1 - cur;
+        }
+    }
+    k_target_normals<<<blocks_for(n), kThreads, 0, stream>>>(points, n, faces, keys[0], values[0], corners,
+                                                             normals);
+}
+
+// ---------------------------------------------------------------------------
 // Closest-point query
 // ---------------------------------------------------------------------------
 
@@ -548,6 +959,60 @@ __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* o
         }
     };
     if (seed >= 0 && seed < w.F) consider(seed, triangle_distance_fp64(w, q64, seed));
+    // The cell index, when the wrap has one and the search stays within a few
+    // level-0 cells: every triangle that could beat the bound is listed, at its
+    // level, in a cell that the box [q - r, q + r] touches, r = sqrt(best) +
+    // slack.  Level 0 goes first, so that the coarser levels' (few, large)
+    // triangles meet a tight bound.  Without a seed, the query's own cells
+    // give the first bound.
+    if (w.cell_ends != nullptr && isfinite(q64.x) && isfinite(q64.y) && isfinite(q64.z)) {
+        const double qc[3] = {q64.x, q64.y, q64.z};
+        auto scan_cell = [&](int cell) {
+            const int e1 = w.cell_ends[cell];
+            for (int e = cell > 0 ? w.cell_ends[cell - 1] : 0; e < e1; ++e) {
+                const float4 lo = __ldg(w.cell_entries + (long)e * 2);
+                const float4 hi = __ldg(w.cell_entries + (long)e * 2 + 1);
+                if (box_distance(q, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z) >= bound) continue;
+                const int leaf = __float_as_int(lo.w);
+                if ((unsigned)leaf >= (unsigned)w.F) continue;  // never: every listed slot was written
+                int tri;
+                const double d = leaf_distance(w, leaf, q64, &tri);
+                if (tri != best_tri) consider(tri, d);
+            }
+        };
+        auto cell_at = [&](int l, int x, int y, int z) {
+            return w.cell_first[l] + x + w.cell_dims[l][0] * (y + w.cell_dims[l][1] * z);
+        };
+        for (int l = 0; l < w.cell_levels && best_tri < 0; ++l) {
+            int c[3];
+            for (int k = 0; k < 3; ++k)
+                c[k] = cell_coord(qc[k], w.cell_origin[k], w.cell_inv[l], w.cell_dims[l][k]);
+            scan_cell(cell_at(l, c[0], c[1], c[2]));
+        }
+        if (best_tri >= 0) {
+            const double r = sqrt(best) + slack;
+            int lo[3], hi[3];
+            long cells = 1;
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = cell_coord(qc[k] - r, w.cell_origin[k], w.cell_inv[0], w.cell_dims[0][k]);
+                hi[k] = cell_coord(qc[k] + r, w.cell_origin[k], w.cell_inv[0], w.cell_dims[0][k]);
+                cells *= hi[k] - lo[k] + 1;
+            }
+            if (cells <= kMaxCellsPerQuery) {
+                for (int l = 0; l < w.cell_levels; ++l) {
+                    if (l > 0)
+                        for (int k = 0; k < 3; ++k) {
+                            lo[k] = cell_coord(qc[k] - r, w.cell_origin[k], w.cell_inv[l], w.cell_dims[l][k]);
+                            hi[k] = cell_coord(qc[k] + r, w.cell_origin[k], w.cell_inv[l], w.cell_dims[l][k]);
+                        }
+                    for (int z = lo[2]; z <= hi[2]; ++z)
+                        for (int y = lo[1]; y <= hi[1]; ++y)
+                            for (int x = lo[0]; x <= hi[0]; ++x) scan_cell(cell_at(l, x, y, z));
+                }
+                return best_tri;
+            }
+        }
+    }
     uint32_t stack[kStackDepth];
     float stack_d[kStackDepth];
     int sp = 0;

@@ -85,15 +85,19 @@ private:
 // target's diagonal: far above the rounding of FP32 boxes and queries.
 constexpr double kRankWindow = 4e-6;
 
-double target_diagonal(const double* p, size_t n) {
+// The bounding-box diagonal of the normalised target, from the caller's
+// points: normalisation ((p - center) * scale, scale > 0) is monotone in each
+// coordinate, so the normalised box's corners are the normalised corners.
+double normalized_diagonal(const double* p, size_t n, const double center[3], double scale) {
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     for (size_t i = 0; i < n; ++i)
         for (int k = 0; k < 3; ++k) {
             lo[k] = i ? std::min(lo[k], p[i * 3 + k]) : p[k];
             hi[k] = i ? std::max(hi[k], p[i * 3 + k]) : p[k];
         }
-    return std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
-                     (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = (hi[k] - center[k]) * scale - (lo[k] - center[k]) * scale;
+    return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
 }
 
 template <typename T>
@@ -168,6 +172,9 @@ struct Wrap {
     double* identity_rot = nullptr;  // device (in the arena): identity rotations
     LevelRecord* initial_records = nullptr;  // and the level records a run starts from
     size_t input_bytes = 0;          // the arena's prefix that holds the inputs
+    CellPlan cell_plan;              // the target's cell index (planned once)
+    bool cell_planned = false;
+    bool target_ingested = false;    // the device has normalised the target and its normals
     ~Wrap() { arena.release(); }
 };
 
@@ -299,9 +306,17 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_identity = a.reserve(sizeof(double) * 9 * N);
     const size_t o_init_records = a.reserve(sizeof(LevelRecord) * w.levels);
     w.input_bytes = a.size();
-    // the target's hierarchy
+    // the target's hierarchy and cell index (planned on the normalised target)
     const size_t o_bvh_nodes = a.reserve(sizeof(float4) * 4 * std::max(1, w.F - 1));
     const size_t o_bvh_leaves = a.reserve(sizeof(float4) * kLeafFloat4s * w.F);
+    if (!w.cell_planned) {
+        w.cell_plan = plan_cells(w.target_in.data(), w.Vt, w.target_faces.data(), w.F, w.graph.center,
+                                 w.graph.scale);
+        w.cell_planned = true;
+    }
+    const CellPlan& cells = w.cell_plan;
+    const size_t o_cell_ends = a.reserve(cells.ok ? sizeof(int32_t) * cells.cells : 0);
+    const size_t o_cell_entries = a.reserve(cells.ok ? sizeof(float4) * 2 * cells.entries : 0);
     // state and scratch
     size_t o_rot[2], o_trans[2], o_diag[2], o_rhs[2], o_off[2];
     for (int i = 0; i < 2; ++i) {
@@ -396,25 +411,19 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.pcg_max_iterations = std::max(1, d.pcg_max_iterations);
     D.pcg_tolerance = d.pcg_tolerance;
 
-    // template and target, normalised with the template's frame
-    // (written straight into the staging area when there is one)
-    std::vector<double> tpl_v, tgt_v, normals_v;
-    double *tpl, *tgt, *tgt_normals;
+    // the template normalised with its own frame (written straight into the
+    // staging area when there is one); the target goes up in the caller's
+    // units and is normalised on the device, with its normals (ingest_target)
+    std::vector<double> tpl_v;
+    double* tpl;
     if (staging) {
         tpl = reinterpret_cast<double*>(staging + o_tpl);
-        tgt = reinterpret_cast<double*>(staging + o_tgt);
-        tgt_normals = reinterpret_cast<double*>(staging + o_tgt_normals);
+        std::memcpy(staging + o_tgt, w.target_in.data(), sizeof(double) * 3 * w.Vt);
     } else {
         tpl_v.resize(static_cast<size_t>(V) * 3);
-        tgt_v.resize(static_cast<size_t>(w.Vt) * 3);
-        normals_v.resize(static_cast<size_t>(w.Vt) * 3);
         tpl = tpl_v.data();
-        tgt = tgt_v.data();
-        tgt_normals = normals_v.data();
     }
     normalized_into(w.template_in.data(), V, w.graph.center, w.graph.scale, tpl);
-    normalized_into(w.target_in.data(), w.Vt, w.graph.center, w.graph.scale, tgt);
-    vertex_normals_into(tgt, w.Vt, w.target_faces.data(), w.F, tgt_normals);
     std::vector<double> lm_target(static_cast<size_t>(V) * 3, 0.0);
     std::vector<uint8_t> lm_flag(V, 0);
     for (int i = 0; i < w.L; ++i) {
@@ -436,7 +445,20 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.tgt_faces = a.at<int32_t>(o_tgt_faces);
     D.bvh_nodes = a.at<float4>(o_bvh_nodes);
     D.bvh_leaves = a.at<float4>(o_bvh_leaves);
-    D.rank_window = static_cast<float>(kRankWindow * target_diagonal(tgt, static_cast<size_t>(w.Vt)));
+    D.rank_window = static_cast<float>(kRankWindow * normalized_diagonal(w.target_in.data(), w.Vt,
+                                                                         w.graph.center, w.graph.scale));
+    if (cells.ok) {
+        D.cell_ends = a.at<int32_t>(o_cell_ends);
+        D.cell_entries = a.at<float4>(o_cell_entries);
+        for (int k = 0; k < 3; ++k) D.cell_origin[k] = cells.origin[k];
+        for (int l = 0; l < kCellLevels; ++l) {
+            D.cell_inv[l] = cells.inv[l];
+            D.cell_first[l] = static_cast<int>(cells.first[l]);
+            for (int k = 0; k < 3; ++k) D.cell_dims[l][k] = cells.dims[l][k];
+        }
+        D.cell_levels = cells.levels;
+        D.cell_entry_count = static_cast<int>(cells.entries);
+    }
     if (!staging) in.put(const_cast<double*>(D.tpl), tpl_v);
     in.put(const_cast<int32_t*>(D.tpl_faces), w.template_faces);
     in.put(const_cast<int32_t*>(D.vf_begin), vf_begin);
@@ -445,10 +467,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     in.put(const_cast<double*>(D.lm_target), lm_target);
     in.put(const_cast<uint8_t*>(D.lm_flag), lm_flag);
     in.put(const_cast<int32_t*>(D.lm_vertices), w.landmark_indices);
-    if (!staging) {
-        in.put(const_cast<double*>(D.tgt_points), tgt_v);
-        in.put(const_cast<double*>(D.tgt_normals), normals_v);
-    }
+    if (!staging) in.put(const_cast<double*>(D.tgt_points), w.target_in);
     in.put(const_cast<int32_t*>(D.tgt_faces), w.target_faces);
 
     for (int l = 0; l < w.levels; ++l) {
@@ -550,18 +569,42 @@ void reset_device(Wrap& w, cudaStream_t stream, void* lbvh_scratch, LbvhExport* 
     c.damping = w.desc.initial_damping;
     check(cudaMemcpyAsync(w.control, &c, sizeof c, cudaMemcpyHostToDevice, stream), "init control");
 
-    // the target's hierarchy; the batch's build scratch (sized for its
-    // largest target) is reused by every wrap's build in stream order
+    // the target in the normalised frame and its normals, once after its
+    // upload; then its hierarchy.  The batch's build scratch (sized for its
+    // largest target) is reused by every wrap's build in stream order.
+    if (!w.target_ingested) {
+        ingest_target(const_cast<double*>(D.tgt_points), w.Vt, D.tgt_faces, w.F, w.graph.center,
+                      w.graph.scale, const_cast<double*>(D.tgt_normals), lbvh_scratch, stream);
+        check(cudaGetLastError(), "target ingestion");
+        w.target_ingested = true;
+    }
     const uint32_t root = lbvh_build(D.tgt_points, D.tgt_faces, w.F, lbvh_scratch,
                                      const_cast<float4*>(D.bvh_nodes), const_cast<float4*>(D.bvh_leaves),
                                      stream, lbvh_out);
     check(cudaGetLastError(), "lbvh build");
     D.bvh_root = static_cast<int>(root);
+    // the cell index, from the hierarchy's leaves, in the same scratch
+    build_cells(D.bvh_leaves, w.F, w.cell_plan, const_cast<int32_t*>(D.cell_ends),
+                const_cast<float4*>(D.cell_entries), lbvh_scratch, &w.control->error, stream);
+    check(cudaGetLastError(), "cell index build");
+}
+
+// Build scratch of one wrap's target structures (the hierarchy, then the cell
+// index, in stream order).
+size_t build_scratch_bytes(const Wrap& w) {
+    return std::max(std::max(lbvh_scratch_bytes(w.F), cells_scratch_bytes(w.cell_plan.cells)),
+                    ingest_scratch_bytes(w.Vt, w.F));
 }
 
 // Kernels one hierarchy build launches (lbvh_build): centroids, two bound
 // passes, Morton codes, 8 radix passes of 3 kernels, Karras, refit, 2 packs.
 int lbvh_build_launches(int n) { return 4 + 8 * 3 + (n > 1 ? 1 : 0) + 1 + (n > 1 ? 2 : 1); }
+
+// Kernels the target structures of a wrap launch: the hierarchy and, when the
+// wrap has one, the cell index.
+int target_build_launches(const Wrap& w) {
+    return lbvh_build_launches(w.F) + (w.cell_plan.ok ? cells_build_launches() : 0);
+}
 
 }  // namespace
 
@@ -708,7 +751,7 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
     check(cudaMalloc(&dev_controls_, sizeof(WrapControl) * W), "cudaMalloc(controls)");
     check(cudaMallocHost(&host_controls_, sizeof(WrapControl) * W), "cudaMallocHost(controls)");
     size_t scratch_bytes = 0;
-    for (const auto& w : wraps_) scratch_bytes = std::max(scratch_bytes, lbvh_scratch_bytes(w->F));
+    for (const auto& w : wraps_) scratch_bytes = std::max(scratch_bytes, build_scratch_bytes(*w));
     for (int k = 0; k < kBuildStreams; ++k) {
         check(cudaMallocFromPoolAsync(&build_scratch_[k], scratch_bytes, pool_, stream_),
               "cudaMallocFromPoolAsync(scratch)");
@@ -960,7 +1003,7 @@ double Batch::timed_step() {
     reset_all(nullptr, nullptr, nullptr);
     ticks_ = 0;
     launches_ = 0;
-    for (auto& w : wraps_) launches_ += lbvh_build_launches(w->F);
+    for (auto& w : wraps_) launches_ += target_build_launches(*w);
     run();
     check(cudaEventRecord(end, stream_), "event");
     check(cudaEventSynchronize(end), "step");
@@ -1019,8 +1062,8 @@ void Batch::inspect(int i, NricpInspect* out) {
     for (int k = 0; k < kEnergyKinds; ++k) out->energies[k] = c.energy_parts[k];
     if (out->off_capacity < K) throw InvalidArgument("off-diagonal capacity too small");
     const WrapDev& D = w.dev;
-    auto get = [this](void* dst, const void* src, size_t bytes) {
-        check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_), "inspect");
+    auto get = [this](void* dst, const void* src, size_t bytes) {  // a null output is skipped
+        if (dst) check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_), "inspect");
     };
     get(out->rotations, D.rot[c.state], sizeof(double) * 9 * N);
     get(out->translations, D.trans[c.state], sizeof(double) * 3 * N);
@@ -1031,15 +1074,17 @@ void Batch::inspect(int i, NricpInspect* out) {
     get(out->diag, D.diag[c.system], sizeof(float) * 36 * N);
     get(out->rhs, D.rhs[c.system], sizeof(float) * 6 * N);
     get(out->delta, D.delta, sizeof(double) * 6 * N);
-    if (out->corr_distances) get(out->corr_distances, D.corr_distance, sizeof(double) * V);
+    get(out->corr_distances, D.corr_distance, sizeof(double) * V);
+    get(out->target_points, D.tgt_points, sizeof(double) * 3 * w.Vt);
+    get(out->target_normals, D.tgt_normals, sizeof(double) * 3 * w.Vt);
     out->damping = c.damping;
     out->pcg_ok = c.pcg_ok;
     out->pcg_iterations = c.pcg_iterations;
     out->pcg_residual = c.pcg_residual;
-    std::vector<float> rows(L.row_entry.size() / 2 * 36);
+    std::vector<float> rows(out->off_nodes && out->off_blocks ? L.row_entry.size() / 2 * 36 : 0);
     if (!rows.empty()) get(rows.data(), D.offdiag[c.system], sizeof(float) * rows.size());
     check(cudaStreamSynchronize(stream_), "inspect");
-    for (int k = 0; k < K; ++k) {
+    for (int k = 0; k < K && !rows.empty(); ++k) {
         out->off_nodes[k * 2] = L.offdiag_nodes[k * 2];
         out->off_nodes[k * 2 + 1] = L.offdiag_nodes[k * 2 + 1];
         const float* block = rows.data() + static_cast<size_t>(L.offdiag_slots[k * 2]) * 36;
@@ -1248,7 +1293,10 @@ struct Server::Impl {
         int state = NRICP_REQUEST_WAITING;
         bool invalid = false;
         std::string error;
-        double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;
+        // submit, graph and layouts built, loader done (uploads and hierarchy
+        // enqueued), placed in a slot, finished on the device, result ready
+        double t_submit = 0.0, t_prepared = 0.0, t_loaded = 0.0, t_admit = 0.0, t_retired = 0.0,
+               t_done = 0.0;
         size_t bytes = 0;
         cudaEvent_t loaded = nullptr;  // the wrap's uploads and hierarchy are on the device
         std::unique_ptr<WrapDownload> download;  // a finished wrap's state, for the finisher
@@ -1379,6 +1427,7 @@ struct Server::Impl {
                 why = e.what();
             }
             std::lock_guard<std::mutex> lk(mu);
+            r->t_prepared = now_seconds();
             if (why.empty()) {
                 ready.push_back(r);
             } else {
@@ -1443,7 +1492,7 @@ struct Server::Impl {
             try {
                 Wrap& w = *r->wrap;
                 prepare_device(w, staging_controls + k, load_stream, false, pool);
-                const size_t need = lbvh_scratch_bytes(w.F);
+                const size_t need = build_scratch_bytes(w);
                 if (need > lbvh_bytes[k]) {
                     if (lbvh_scratch[k]) check(cudaFreeAsync(lbvh_scratch[k], load_stream), "scratch");
                     lbvh_scratch[k] = nullptr;
@@ -1458,6 +1507,7 @@ struct Server::Impl {
             }
             std::lock_guard<std::mutex> lk(mu);
             loading -= 1;
+            r->t_loaded = now_seconds();
             if (why.empty()) {
                 loaded.push_back(r);
             } else {
@@ -1737,6 +1787,7 @@ struct Server::Impl {
                 }
                 bury(r);
                 std::lock_guard<std::mutex> lk(mu);
+                r->t_retired = now_seconds();
                 slot_req[i] = nullptr;
                 running -= 1;
                 if (!why.empty()) {
@@ -1915,6 +1966,16 @@ int Server::poll(long id, double* latency_seconds) {
     if (latency_seconds)
         *latency_seconds = r->state == NRICP_REQUEST_DONE ? r->t_done - r->t_submit : 0.0;
     return r->state;
+}
+
+void Server::phases(long id, double seconds[5]) {
+    Impl& m = *impl_;
+    std::lock_guard<std::mutex> lk(m.mu);
+    auto it = m.requests.find(id);
+    if (it == m.requests.end()) throw InvalidArgument("unknown request " + std::to_string(id));
+    const auto& r = it->second;
+    const double t[6] = {r->t_submit, r->t_prepared, r->t_loaded, r->t_admit, r->t_retired, r->t_done};
+    for (int k = 0; k < 5; ++k) seconds[k] = t[k + 1] > 0.0 && t[k] > 0.0 ? t[k + 1] - t[k] : 0.0;
 }
 
 bool Server::wait(long id, double timeout_seconds) {

@@ -142,6 +142,10 @@ public:
     Server& operator=(const Server&) = delete;
     long submit(const NricpSolveDesc& desc);
     int poll(long id, double* latency_seconds);
+    // The request's time in each phase so far, in seconds: host preparation
+    // (graph, layouts), loading (waiting for memory, uploads, hierarchy),
+    // waiting for a slot, on the device, composing the result.
+    void phases(long id, double seconds[5]);
     bool wait(long id, double timeout_seconds);
     void result(long id, NricpResult* out);
     NricpServerStats stats();

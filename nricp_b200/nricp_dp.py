@@ -234,6 +234,17 @@ class WrapServer:
         check(load().nricp_server_poll(self._handle, request, C.byref(status), C.byref(latency)))
         return _abi.REQUEST_STATES[status.value], latency.value
 
+    PHASES = ("prepare", "load", "wait_for_slot", "device", "compose")
+
+    def phases(self, request: int) -> dict:
+        """Where the request's latency went so far, in seconds: host preparation
+        (graph, level layouts), loading (memory budget, uploads, target
+        hierarchy), waiting for a slot, on the device, composing the result.
+        Read it before ``result`` takes the request."""
+        out = (C.c_double * 5)()
+        check(load().nricp_server_phases(self._handle, request, out))
+        return dict(zip(self.PHASES, list(out)))
+
     def wait(self, request: int, timeout: float | None = None) -> tuple[str, float]:
         """Blocks until the request is done or failed; returns poll()."""
         check(load().nricp_server_wait(self._handle, request, float(timeout or 0.0)))
@@ -317,6 +328,19 @@ class RouteBSession:
         t, l = C.c_long(), C.c_long()
         check(load().nricp_session_ticks(self._handle, C.byref(t), C.byref(l)))
         return t.value, l.value
+
+    def target(self) -> dict:
+        """The target as the device holds it (no reference counterpart; for
+        checking its ingestion): points in the normalised frame and their
+        area-weighted vertex normals."""
+        vt = self._desc.target_points.shape[0]
+        out = {"points": np.zeros((vt, 3)), "normals": np.zeros((vt, 3))}
+        s = _abi.Inspect()
+        s.off_capacity = 1 << 30  # nothing else is read
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+        s.target_points, s.target_normals = P(out["points"], C.c_double), P(out["normals"], C.c_double)
+        check(load().nricp_session_inspect(self._handle, C.byref(s)))
+        return out
 
     def inspect(self) -> dict:
         """The current linear system and the state it was assembled at (no
