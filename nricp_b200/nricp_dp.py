@@ -143,6 +143,27 @@ class WrapBatch:
         check(load().nricp_batch_tune(self._handle, int(pcg_cluster), C.byref(out)))
         return out.value
 
+    # Candidate cluster settings of the linear solve that autotune() times:
+    # per-wrap classes halved once, unhalved, halved twice, and uniform sizes.
+    TUNE_CANDIDATES = (-1, 0, -2, 8, 16, 4)
+
+    def autotune(self, candidates=TUNE_CANDIDATES) -> dict:
+        """Picks the linear solve's cluster setting by measurement: one batch
+        step (device time) per candidate, the two fastest timed once more, the
+        fastest kept.  Every setting gives bit-identical results, so the
+        choice trades nothing but speed.  Returns the choice, the largest
+        cluster in effect and each candidate's best time in milliseconds."""
+        times = {}
+        for c in candidates:
+            self.tune(c)
+            times[c] = self.step()
+        for c in sorted(times, key=times.get)[:2]:  # one step is noisy
+            self.tune(c)
+            times[c] = min(times[c], self.step())
+        choice = min(times, key=times.get)
+        return {"choice": choice, "largest_cluster": self.tune(choice),
+                "ms": {str(c): round(t, 2) for c, t in times.items()}}
+
     def result(self, index: int) -> dict:
         out = _abi.ResultBuffers(self._descs[index].template_points.shape[0], self._plans[index])
         check(load().nricp_batch_result(self._handle, index, C.byref(out.struct)))
