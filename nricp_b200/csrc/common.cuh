@@ -19,9 +19,8 @@ constexpr int kMaxSlots = 8;        // binding support (the reference caps at 4)
 constexpr int kMaxLevels = 16;
 constexpr int kEnergyKinds = 5;     // p2p, plane, smoothness, anchor, landmark
 constexpr int kStackDepth = 64;     // LBVH traversal stack
-constexpr int kMaxCellsPerQuery = 64;  // more level-0 cells than this: the hierarchy walk instead
-constexpr int kCellLevels = 6;         // most cell index levels, each 4x coarser than the one below
-constexpr double kCellFit = 0.999;     // a listed triangle's extent is below this many cells
+constexpr int kMaxCellsPerQuery = 27;    // a query's cells beyond this: the hierarchy walk instead
+constexpr int kMaxEntriesPerQuery = 256; // and entries in those cells beyond this
 constexpr int kPartialStride = 8;   // doubles per energy partial record
 
 // Device phases of one wrap.  They mirror the reference session's
@@ -151,18 +150,19 @@ struct WrapDev {
     const float4* bvh_leaves;     // F x kLeafFloat4s: FP64 corners + triangle id, sorted
     int bvh_root;                 // encoded child (leaf flag in bit 31)
     float rank_window;            // FP32 box-pruning slack (distance, normalised units)
-    // hierarchical cell index over the same triangles (null when the wrap has
-    // none): level l's cell (i, j, k) is cell_first[l] + i + dims[l][0] (j +
-    // dims[l][1] k) and holds entries [cell ? cell_ends[cell - 1] : 0,
-    // cell_ends[cell]); an entry is two float4, (FP32 box lo, leaf index bits)
-    // and (FP32 box hi, 0)
-    const int32_t* cell_ends;     // cells of every level
-    const float4* cell_entries;   // 2 x entries
+    // uniform cell index over the same triangles (null when the wrap has none):
+    // cell (i, j, k) = i + dims[0] (j + dims[1] k) holds entries
+    // [cell ? cell_ends[cell - 1] : 0, cell_ends[cell]), the triangles whose
+    // surface crosses it; an entry is two float4, (FP32 box lo, leaf index
+    // bits) and (FP32 box hi, 0).  The index is usable only while *cell_total
+    // is within cell_entry_count.
+    const int32_t* cell_ends;     // cells
+    const unsigned long long* cell_total;  // every entry the build counted
+    const float4* cell_entries;   // 2 x cell_entry_count
     double cell_origin[3];
-    double cell_inv[kCellLevels]; // 1 / cell size of each level
-    int cell_dims[kCellLevels][3];
-    int cell_first[kCellLevels];
-    int cell_levels;
+    double cell_inv;              // 1 / cell size
+    int cell_dims[3];
+    int cell_count;
     int cell_entry_count;
     // levels
     LevelDev levels[kMaxLevels];
@@ -255,17 +255,6 @@ __host__ __device__ inline int cell_coord(double x, double origin, double inv, i
     if (!(t >= 0.0)) return 0;
     if (t >= (double)dim) return dim - 1;
     return (int)t;
-}
-
-// The level of the cell index a triangle is listed in: the finest whose cell
-// exceeds the triangle's largest box extent by a margin (kCellFit) that covers
-// the rounding of the cell arithmetic, so that it overlaps at most two cells
-// per axis there.  The coarsest level's cell exceeds the whole target's box
-// by the same margin, so every triangle fits somewhere.
-__host__ __device__ inline int cell_level(double extent, const double* inv, int levels) {
-    int l = 0;
-    while (l + 1 < levels && extent * inv[l] > kCellFit) ++l;
-    return l;
 }
 
 // Leaf / internal child encoding of the traversal hierarchy.

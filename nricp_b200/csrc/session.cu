@@ -315,7 +315,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
         w.cell_planned = true;
     }
     const CellPlan& cells = w.cell_plan;
-    const size_t o_cell_ends = a.reserve(cells.ok ? sizeof(int32_t) * cells.cells : 0);
+    const size_t o_cell_ends = a.reserve(cells.ok ? cells_ends_bytes(cells.cells) : 0);
     const size_t o_cell_entries = a.reserve(cells.ok ? sizeof(float4) * 2 * cells.entries : 0);
     // state and scratch
     size_t o_rot[2], o_trans[2], o_diag[2], o_rhs[2], o_off[2];
@@ -449,14 +449,14 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
                                                                          w.graph.center, w.graph.scale));
     if (cells.ok) {
         D.cell_ends = a.at<int32_t>(o_cell_ends);
+        D.cell_total = reinterpret_cast<const unsigned long long*>(D.cell_ends + cells_total_slot(cells.cells));
         D.cell_entries = a.at<float4>(o_cell_entries);
-        for (int k = 0; k < 3; ++k) D.cell_origin[k] = cells.origin[k];
-        for (int l = 0; l < kCellLevels; ++l) {
-            D.cell_inv[l] = cells.inv[l];
-            D.cell_first[l] = static_cast<int>(cells.first[l]);
-            for (int k = 0; k < 3; ++k) D.cell_dims[l][k] = cells.dims[l][k];
+        for (int k = 0; k < 3; ++k) {
+            D.cell_origin[k] = cells.origin[k];
+            D.cell_dims[k] = cells.dims[k];
         }
-        D.cell_levels = cells.levels;
+        D.cell_inv = cells.inv;
+        D.cell_count = static_cast<int>(cells.cells);
         D.cell_entry_count = static_cast<int>(cells.entries);
     }
     if (!staging) in.put(const_cast<double*>(D.tpl), tpl_v);
@@ -585,7 +585,7 @@ void reset_device(Wrap& w, cudaStream_t stream, void* lbvh_scratch, LbvhExport* 
     D.bvh_root = static_cast<int>(root);
     // the cell index, from the hierarchy's leaves, in the same scratch
     build_cells(D.bvh_leaves, w.F, w.cell_plan, const_cast<int32_t*>(D.cell_ends),
-                const_cast<float4*>(D.cell_entries), lbvh_scratch, &w.control->error, stream);
+                const_cast<float4*>(D.cell_entries), lbvh_scratch, stream);
     check(cudaGetLastError(), "cell index build");
 }
 
