@@ -19,8 +19,6 @@ constexpr int kMaxSlots = 8;        // binding support (the reference caps at 4)
 constexpr int kMaxLevels = 16;
 constexpr int kEnergyKinds = 5;     // p2p, plane, smoothness, anchor, landmark
 constexpr int kStackDepth = 64;     // LBVH traversal stack
-constexpr int kMaxCellsPerQuery = 27;    // a query's cells beyond this: the hierarchy walk instead
-constexpr int kMaxEntriesPerQuery = 256; // and entries in those cells beyond this
 constexpr int kPartialStride = 8;   // doubles per energy partial record
 
 // Device phases of one wrap.  They mirror the reference session's
@@ -150,20 +148,6 @@ struct WrapDev {
     const float4* bvh_leaves;     // F x kLeafFloat4s: FP64 corners + triangle id, sorted
     int bvh_root;                 // encoded child (leaf flag in bit 31)
     float rank_window;            // FP32 box-pruning slack (distance, normalised units)
-    // uniform cell index over the same triangles (null when the wrap has none):
-    // cell (i, j, k) = i + dims[0] (j + dims[1] k) holds entries
-    // [cell ? cell_ends[cell - 1] : 0, cell_ends[cell]), the triangles whose
-    // surface crosses it; an entry is two float4, (FP32 box lo, leaf index
-    // bits) and (FP32 box hi, 0).  The index is usable only while *cell_total
-    // is within cell_entry_count.
-    const int32_t* cell_ends;     // cells
-    const unsigned long long* cell_total;  // every entry the build counted
-    const float4* cell_entries;   // 2 x cell_entry_count
-    double cell_origin[3];
-    double cell_inv;              // 1 / cell size
-    int cell_dims[3];
-    int cell_count;
-    int cell_entry_count;
     // levels
     LevelDev levels[kMaxLevels];
     // state: two buffers, `control.state` selects the accepted one
@@ -244,17 +228,6 @@ __host__ __device__ inline F3 cross(F3 a, F3 b) {
 __device__ inline F3 mul3f(const float* m, F3 v) {
     return {m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
             m[6] * v.x + m[7] * v.y + m[8] * v.z};
-}
-
-// Cell of coordinate x along one axis of a uniform cell index: floor((x -
-// origin) / size), clamped to [0, dim).  Host and device evaluate it with the
-// same two rounded operations (no contraction is possible), so a triangle's
-// cells are the same on both.
-__host__ __device__ inline int cell_coord(double x, double origin, double inv, int dim) {
-    const double t = (x - origin) * inv;
-    if (!(t >= 0.0)) return 0;
-    if (t >= (double)dim) return dim - 1;
-    return (int)t;
 }
 
 // Leaf / internal child encoding of the traversal hierarchy.

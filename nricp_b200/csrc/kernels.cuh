@@ -21,36 +21,6 @@ size_t lbvh_scratch_bytes(int triangle_count);
 uint32_t lbvh_build(const double* points, const int32_t* faces, int triangle_count,
                     void* scratch, float4* nodes, float4* leaves, cudaStream_t stream,
                     LbvhExport* out);
-// A uniform cell index over a target's triangles: each triangle is listed in
-// the cells its surface crosses (a conservative separating-axis test against
-// each cell its box overlaps).  It is planned on the host for the normalised
-// frame (cell size, origin, dimensions: one pass over the points and a sample
-// of the triangles) and built on the device beside the hierarchy, from the
-// hierarchy's leaves.  The arena holds 8 entries per triangle; a build that
-// would need more, or meets a triangle whose box covers more than
-// kMaxCellsPerTriangle cells, leaves the index unusable and the queries walk
-// the hierarchy instead.
-struct CellPlan {
-    bool ok = false;
-    double origin[3] = {0.0, 0.0, 0.0};
-    double inv = 0.0;   // 1 / cell size
-    int dims[3] = {0, 0, 0};
-    long cells = 0;
-    long entries = 0;   // capacity: 8 per triangle
-};
-// From the target in the caller's units and the normalisation it will get.
-CellPlan plan_cells(const double* points, int point_count, const int32_t* faces, int face_count,
-                    const double center[3], double scale);
-size_t cells_scratch_bytes(long cells);
-// The ends array holds `cells` ends and then, at int index cells_total_slot
-// (8-byte aligned when the array is), the 64-bit count of all entries.
-long cells_total_slot(long cells);
-size_t cells_ends_bytes(long cells);
-// Fills `ends` (plan.cells) and `entries` (2 x plan.entries float4) from the
-// hierarchy's leaves (FP64 corners, Morton order).
-void build_cells(const float4* leaves, int face_count, const CellPlan& plan, int32_t* ends,
-                 float4* entries, void* scratch, cudaStream_t stream);
-int cells_build_launches();
 // The target's ingestion on the device, once after its upload in the caller's
 // units: its points normalised in place ((p - center) * scale) and its
 // area-weighted vertex normals, both bit-identical to the host's.

@@ -16,9 +16,6 @@
 // triangle it reaches is measured with the reference's FP64 closest-point
 // routine (src/geometry/closest_point.cpp:24-121), so the winner, its point,
 // normal and distance are those of an FP64 brute-force scan.
-#include <algorithm>
-#include <cmath>
-
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -422,315 +419,6 @@ uint32_t lbvh_build(const double* points, const int32_t* faces, int n, void* scr
 }
 
 // ---------------------------------------------------------------------------
-// Uniform cell index over the target's triangles
-// ---------------------------------------------------------------------------
-//
-// A seeded query already knows a triangle at distance d; every triangle that
-// could beat it has a point within d of the query, so its surface crosses one
-// of the cells that the box [q - d, q + d] touches.  Those cells are computed
-// from the query's coordinates, and a row of them (consecutive x) holds one
-// contiguous run of entries, so a query reads them with a few rounds of
-// independent loads instead of a root-to-leaf chain of dependent node fetches.
-// Each triangle is listed only in the cells its surface crosses -- a
-// separating-axis test of the triangle against each cell its box overlaps,
-// with the cell widened by a relative 1e-6 so that rounding can only add
-// cells -- so the long spikes that off-surface outlier vertices make sit in
-// the few cells along them, not in every cell of their boxes.
-
-namespace {
-
-// Cell size in mean triangle edges (the edge of an equilateral triangle of the
-// mean area); cells per triangle the index may take; and the widest box (in
-// cells) a triangle may have before the index gives up for that target.
-constexpr double kCellEdges = 1.5;
-constexpr long kCellsPerTriangle = 8;
-constexpr long kEntriesPerTriangle = 8;
-constexpr int kMaxCellsPerTriangle = 4096;
-constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 4;
-constexpr int kScanTile = kScanThreads * kScanItems;
-
-struct CellParams {
-    double origin[3];
-    double inv, size;
-    int dims[3];
-};
-
-__device__ inline void leaf_corners(const float4* leaves, int leaf, double c[9]) {
-    const double2* l = reinterpret_cast<const double2*>(leaves) + (long)leaf * kLeafFloat4s;
-    const double2 l0 = l[0], l1 = l[1], l2 = l[2], l3 = l[3], l4 = l[4];
-    c[0] = l0.x; c[1] = l0.y; c[2] = l1.x;
-    c[3] = l1.y; c[4] = l2.x; c[5] = l2.y;
-    c[6] = l3.x; c[7] = l3.y; c[8] = l4.x;
-}
-
-// The cell range of a triangle's FP64 box, per axis; returns the cells in it.
-__device__ inline long triangle_box_cells(const double c[9], const CellParams& P, int lo[3], int hi[3]) {
-    long cells = 1;
-    for (int k = 0; k < 3; ++k) {
-        const double mn = fmin(c[k], fmin(c[3 + k], c[6 + k]));
-        const double mx = fmax(c[k], fmax(c[3 + k], c[6 + k]));
-        lo[k] = cell_coord(mn, P.origin[k], P.inv, P.dims[k]);
-        hi[k] = cell_coord(mx, P.origin[k], P.inv, P.dims[k]);
-        cells *= hi[k] - lo[k] + 1;
-    }
-    return cells;
-}
-
-// Whether the triangle may touch cell (x, y, z): false only when one of the
-// nine edge-cross axes or the triangle's normal separates it from the cell
-// widened by a relative 1e-6 (the box axes are settled by the cell range).
-__device__ inline bool triangle_touches_cell(const double c[9], const CellParams& P, int x, int y, int z) {
-    const double half = 0.5 * P.size * (1.0 + 1e-6);
-    const double cx = P.origin[0] + (x + 0.5) * P.size, cy = P.origin[1] + (y + 0.5) * P.size,
-                 cz = P.origin[2] + (z + 0.5) * P.size;
-    double v[3][3];
-    for (int i = 0; i < 3; ++i) {
-        v[i][0] = c[i * 3] - cx;
-        v[i][1] = c[i * 3 + 1] - cy;
-        v[i][2] = c[i * 3 + 2] - cz;
-    }
-    const double e[3][3] = {{v[1][0] - v[0][0], v[1][1] - v[0][1], v[1][2] - v[0][2]},
-                            {v[2][0] - v[1][0], v[2][1] - v[1][1], v[2][2] - v[1][2]},
-                            {v[0][0] - v[2][0], v[0][1] - v[2][1], v[0][2] - v[2][2]}};
-    auto separated = [&](double ax, double ay, double az) {
-        const double r = half * (fabs(ax) + fabs(ay) + fabs(az));
-        const double p0 = ax * v[0][0] + ay * v[0][1] + az * v[0][2];
-        const double p1 = ax * v[1][0] + ay * v[1][1] + az * v[1][2];
-        const double p2 = ax * v[2][0] + ay * v[2][1] + az * v[2][2];
-        return fmin(p0, fmin(p1, p2)) > r || fmax(p0, fmax(p1, p2)) < -r;
-    };
-    for (int j = 0; j < 3; ++j) {
-        if (separated(0.0, -e[j][2], e[j][1])) return false;   // x cross e
-        if (separated(e[j][2], 0.0, -e[j][0])) return false;   // y cross e
-        if (separated(-e[j][1], e[j][0], 0.0)) return false;   // z cross e
-    }
-    const double nx = e[0][1] * e[1][2] - e[0][2] * e[1][1];
-    const double ny = e[0][2] * e[1][0] - e[0][0] * e[1][2];
-    const double nz = e[0][0] * e[1][1] - e[0][1] * e[1][0];
-    return !separated(nx, ny, nz);
-}
-
-// Counts each cell's entries and, in `total` (64-bit, so it cannot wrap), all
-// of them.  A triangle whose box covers more cells than kMaxCellsPerTriangle
-// adds more than the capacity to `total` instead: with the total beyond the
-// capacity, the queries walk the hierarchy.
-__global__ void k_cell_count(const float4* __restrict__ leaves, int n, CellParams P,
-                             int32_t* __restrict__ counts, unsigned long long* __restrict__ total,
-                             int capacity) {
-    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (leaf >= n) return;
-    double c[9];
-    leaf_corners(leaves, leaf, c);
-    int lo[3], hi[3];
-    const long box = triangle_box_cells(c, P, lo, hi);
-    if (box > kMaxCellsPerTriangle) {
-        atomicAdd(total, (unsigned long long)capacity + 1ull);
-        return;
-    }
-    unsigned long long mine = 0;
-    for (int z = lo[2]; z <= hi[2]; ++z)
-        for (int y = lo[1]; y <= hi[1]; ++y)
-            for (int x = lo[0]; x <= hi[0]; ++x)
-                if (box == 1 || triangle_touches_cell(c, P, x, y, z)) {
-                    atomicAdd(&counts[x + (long)P.dims[0] * (y + (long)P.dims[1] * z)], 1);
-                    ++mine;
-                }
-    atomicAdd(total, mine);
-}
-
-// Each cell's counter starts at the cell's first entry; taking a slot moves it
-// on, so when every triangle is in, counter c holds the end of cell c.  Slots
-// beyond the capacity are not written (the index is then unusable anyway).
-__global__ void k_cell_fill(const float4* __restrict__ leaves, int n, CellParams P,
-                            int32_t* __restrict__ cursor, float4* __restrict__ entries, int capacity) {
-    const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
-    if (leaf >= n) return;
-    double c[9];
-    leaf_corners(leaves, leaf, c);
-    int lo[3], hi[3];
-    const long box = triangle_box_cells(c, P, lo, hi);
-    if (box > kMaxCellsPerTriangle) return;
-    // the FP32 box the traversal prunes with (the corners rounded to FP32)
-    float blo[3], bhi[3];
-    for (int k = 0; k < 3; ++k) {
-        const float a = __double2float_rn(c[k]), b = __double2float_rn(c[3 + k]),
-                    d = __double2float_rn(c[6 + k]);
-        blo[k] = fminf(a, fminf(b, d));
-        bhi[k] = fmaxf(a, fmaxf(b, d));
-    }
-    const float4 e0 = make_float4(blo[0], blo[1], blo[2], __int_as_float(leaf));
-    const float4 e1 = make_float4(bhi[0], bhi[1], bhi[2], 0.0f);
-    for (int z = lo[2]; z <= hi[2]; ++z)
-        for (int y = lo[1]; y <= hi[1]; ++y)
-            for (int x = lo[0]; x <= hi[0]; ++x) {
-                if (box != 1 && !triangle_touches_cell(c, P, x, y, z)) continue;
-                const int at = atomicAdd(&cursor[x + (long)P.dims[0] * (y + (long)P.dims[1] * z)], 1);
-                if (at < 0 || at >= capacity) continue;
-                entries[(long)at * 2] = e0;
-                entries[(long)at * 2 + 1] = e1;
-            }
-}
-
-// Exclusive scan of n ints in place: tiles of kScanTile scanned by one block
-// each (their totals to `sums`), the totals scanned by one block, then added.
-__device__ inline int block_exclusive_scan(int value, int* warp_totals, int* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int x = value;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_totals[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = blockDim.x >> 5;
-        int t = lane < nw ? warp_totals[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= o) t += y;
-        }
-        if (lane < nw) warp_totals[lane] = t;  // inclusive
-        if (lane == 31) *total = t;
-    }
-    __syncthreads();
-    const int before = warp == 0 ? 0 : warp_totals[warp - 1];
-    return before + x - value;
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(int32_t* __restrict__ data, long n,
-                                                            int32_t* __restrict__ sums) {
-    __shared__ int warp_totals[32];
-    __shared__ int total;
-    const long base = (long)blockIdx.x * kScanTile + (long)threadIdx.x * kScanItems;
-    int v[kScanItems];
-    int local = 0;
-    for (int i = 0; i < kScanItems; ++i) {
-        v[i] = base + i < n ? data[base + i] : 0;
-        local += v[i];
-    }
-    int run = block_exclusive_scan(local, warp_totals, &total);
-    for (int i = 0; i < kScanItems; ++i) {
-        if (base + i < n) data[base + i] = run;
-        run += v[i];
-    }
-    if (threadIdx.x == 0) sums[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int32_t* __restrict__ sums, int tiles) {
-    __shared__ int warp_totals[32];
-    __shared__ int total;
-    int carry = 0;
-    for (int base = 0; base < tiles; base += kScanThreads) {
-        const int i = base + (int)threadIdx.x;
-        const int v = i < tiles ? sums[i] : 0;
-        const int ex = block_exclusive_scan(v, warp_totals, &total);
-        if (i < tiles) sums[i] = carry + ex;
-        carry += total;
-        __syncthreads();
-    }
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_scan_add(int32_t* __restrict__ data, long n,
-                                                          const int32_t* __restrict__ sums) {
-    const long base = (long)blockIdx.x * kScanTile + (long)threadIdx.x * kScanItems;
-    const int add = sums[blockIdx.x];
-    for (int i = 0; i < kScanItems; ++i)
-        if (base + i < n) data[base + i] += add;
-}
-
-}  // namespace
-
-CellPlan plan_cells(const double* p, int n, const int32_t* f, int F, const double center[3], double scale) {
-    CellPlan plan;
-    if (n <= 0 || F <= 0 || !(scale > 0.0)) return plan;
-    // the normalised box: normalisation is monotone in each coordinate, so its
-    // corners are the normalised corners of the caller's box
-    double lo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, hi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
-    for (int i = 0; i < n; ++i)
-        for (int k = 0; k < 3; ++k) {
-            const double x = p[(long)i * 3 + k];
-            if (!std::isfinite(x)) return plan;  // the hierarchy alone handles such targets
-            lo[k] = std::min(lo[k], x);
-            hi[k] = std::max(hi[k], x);
-        }
-    for (int k = 0; k < 3; ++k) {
-        lo[k] = (lo[k] - center[k]) * scale;
-        hi[k] = (hi[k] - center[k]) * scale;
-    }
-    // the mean triangle area, from an evenly spaced sample of the triangles
-    const int samples = std::min(F, 4096);
-    double area = 0.0;
-    for (int i = 0; i < samples; ++i) {
-        const int32_t* fc = f + (long)((long)i * F / samples) * 3;
-        if (fc[0] < 0 || fc[0] >= n || fc[1] < 0 || fc[1] >= n || fc[2] < 0 || fc[2] >= n) return plan;
-        const double* a = p + (long)fc[0] * 3;
-        const double* b = p + (long)fc[1] * 3;
-        const double* c = p + (long)fc[2] * 3;
-        const double u[3] = {(b[0] - a[0]) * scale, (b[1] - a[1]) * scale, (b[2] - a[2]) * scale};
-        const double v[3] = {(c[0] - a[0]) * scale, (c[1] - a[1]) * scale, (c[2] - a[2]) * scale};
-        const double x = u[1] * v[2] - u[2] * v[1], y = u[2] * v[0] - u[0] * v[2],
-                     z = u[0] * v[1] - u[1] * v[0];
-        area += 0.5 * std::sqrt(x * x + y * y + z * z);
-    }
-    const double extent = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
-    if (!(extent > 0.0) || !std::isfinite(extent)) return plan;
-    double size = kCellEdges * std::sqrt(area / samples * (4.0 / std::sqrt(3.0)));
-    if (!(size > 0.0) || !std::isfinite(size)) size = extent / std::cbrt((double)F);
-    const long cap = kCellsPerTriangle * (long)F + 4096;
-    for (int attempt = 0; attempt < 64; ++attempt) {
-        plan.inv = 1.0 / size;
-        plan.cells = 1;
-        for (int k = 0; k < 3; ++k) {
-            const double t = (hi[k] - lo[k]) * plan.inv;
-            plan.dims[k] = t < (double)(1 << 20) ? (int)t + 1 : (1 << 20);
-            plan.cells *= plan.dims[k];
-        }
-        if (plan.cells <= cap) break;
-        size *= std::cbrt((double)plan.cells / (double)cap) * 1.01;
-    }
-    if (plan.cells > cap) return CellPlan();
-    for (int k = 0; k < 3; ++k) plan.origin[k] = lo[k];
-    plan.entries = kEntriesPerTriangle * (long)F;
-    if (plan.entries >= (1L << 30)) return CellPlan();
-    plan.ok = true;
-    return plan;
-}
-
-long cells_total_slot(long cells) { return (cells + 1) & ~1L; }
-size_t cells_ends_bytes(long cells) { return sizeof(int32_t) * (size_t)(cells_total_slot(cells) + 2); }
-
-size_t cells_scratch_bytes(long cells) {
-    return sizeof(int32_t) * (size_t)((cells + kScanTile - 1) / kScanTile + 1) + 256;
-}
-
-int cells_build_launches() { return 5; }
-
-void build_cells(const float4* leaves, int n, const CellPlan& plan, int32_t* ends, float4* entries,
-                 void* scratch, cudaStream_t stream) {
-    if (!plan.ok || n <= 0) return;
-    CellParams P;
-    for (int k = 0; k < 3; ++k) {
-        P.origin[k] = plan.origin[k];
-        P.dims[k] = plan.dims[k];
-    }
-    P.inv = plan.inv;
-    P.size = 1.0 / plan.inv;
-    const long cells = plan.cells;
-    const int capacity = (int)plan.entries;
-    const int tiles = (int)((cells + kScanTile - 1) / kScanTile);
-    int32_t* sums = static_cast<int32_t*>(scratch);
-    // the ends, then the 64-bit total in the (8-byte aligned) slot after them
-    cudaMemsetAsync(ends, 0, cells_ends_bytes(cells), stream);
-    unsigned long long* total = reinterpret_cast<unsigned long long*>(ends + cells_total_slot(cells));
-    k_cell_count<<<blocks_for(n), kThreads, 0, stream>>>(leaves, n, P, ends, total, capacity);
-    k_scan_tiles<<<tiles, kScanThreads, 0, stream>>>(ends, cells, sums);
-    k_scan_sums<<<1, kScanThreads, 0, stream>>>(sums, tiles);
-    k_scan_add<<<tiles, kScanThreads, 0, stream>>>(ends, cells, sums);
-    k_cell_fill<<<blocks_for(n), kThreads, 0, stream>>>(leaves, n, P, ends, entries, capacity);
-}
-
-// ---------------------------------------------------------------------------
 // Target ingestion: normalisation and vertex normals on the device
 // ---------------------------------------------------------------------------
 //
@@ -986,89 +674,10 @@ __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* o
             best = d;
             best_tri = tri;
             const double r = sqrt(best) + slack;
-            bound = fminf(bound, __double2float_ru(r * r));  // never looser than a bound already held
+            bound = __double2float_ru(r * r);
         }
     };
     if (seed >= 0 && seed < w.F) consider(seed, triangle_distance_fp64(w, q64, seed));
-    // The cell index, when the wrap has a usable one and the search stays
-    // within a few cells: every triangle that could beat the bound crosses a
-    // cell that the box [q - r, q + r] touches, r = sqrt(best) + slack.  Each
-    // row of those cells (consecutive x) is one contiguous run of entries.  A
-    // first pass takes the farthest corner of each entry's FP32 box as an
-    // upper bound of its triangle's distance (plus the slack, which covers the
-    // FP32 rounding of the boxes), so the second pass measures in FP64 only
-    // the triangles whose boxes reach inside the best of those bounds.
-    // Without a seed, the query's own cell gives the first bound.
-    if (w.cell_ends != nullptr && isfinite(q64.x) && isfinite(q64.y) && isfinite(q64.z) &&
-        *w.cell_total <= (unsigned long long)w.cell_entry_count) {
-        const double qc[3] = {q64.x, q64.y, q64.z};
-        const int dx = w.cell_dims[0], dxy = w.cell_dims[0] * w.cell_dims[1];
-        auto span_begin = [&](int cell) { return cell > 0 ? w.cell_ends[cell - 1] : 0; };
-        auto measure = [&](int e0, int e1) {
-            for (int e = e0; e < e1; ++e) {
-                const float4 lo = __ldg(w.cell_entries + (long)e * 2);
-                const float4 hi = __ldg(w.cell_entries + (long)e * 2 + 1);
-                if (box_distance(q, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z) >= bound) continue;
-                const int leaf = __float_as_int(lo.w);
-                if ((unsigned)leaf >= (unsigned)w.F) continue;  // never: every listed slot was written
-                int tri;
-                const double d = leaf_distance(w, leaf, q64, &tri);
-                if (tri != best_tri) consider(tri, d);
-            }
-        };
-        int c0[3];
-        for (int k = 0; k < 3; ++k) c0[k] = cell_coord(qc[k], w.cell_origin[k], w.cell_inv, w.cell_dims[k]);
-        if (best_tri < 0) {
-            const int home = c0[0] + dx * c0[1] + dxy * c0[2];
-            const int e0 = span_begin(home), e1 = w.cell_ends[home];
-            if (e1 - e0 <= kMaxEntriesPerQuery) measure(e0, e1);
-        }
-        if (best_tri >= 0) {
-            const double r = sqrt(best) + slack;
-            int lo[3], hi[3];
-            int cells = 1;
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = cell_coord(qc[k] - r, w.cell_origin[k], w.cell_inv, w.cell_dims[k]);
-                hi[k] = cell_coord(qc[k] + r, w.cell_origin[k], w.cell_inv, w.cell_dims[k]);
-                cells *= hi[k] - lo[k] + 1;
-            }
-            int entries = 0;
-            if (cells <= kMaxCellsPerQuery)
-                for (int z = lo[2]; z <= hi[2]; ++z)
-                    for (int y = lo[1]; y <= hi[1]; ++y) {
-                        const int row = dx * y + dxy * z;
-                        entries += w.cell_ends[row + hi[0]] - span_begin(row + lo[0]);
-                    }
-            if (cells <= kMaxCellsPerQuery && entries <= kMaxEntriesPerQuery) {
-                // pass 1: the nearest farthest-corner over the entries' boxes
-                float upper = 3.4e38f;
-                for (int z = lo[2]; z <= hi[2]; ++z)
-                    for (int y = lo[1]; y <= hi[1]; ++y) {
-                        const int row = dx * y + dxy * z;
-                        const int e1 = w.cell_ends[row + hi[0]];
-                        for (int e = span_begin(row + lo[0]); e < e1; ++e) {
-                            const float4 bl = __ldg(w.cell_entries + (long)e * 2);
-                            const float4 bh = __ldg(w.cell_entries + (long)e * 2 + 1);
-                            const float fx = fmaxf(fabsf(q.x - bl.x), fabsf(q.x - bh.x));
-                            const float fy = fmaxf(fabsf(q.y - bl.y), fabsf(q.y - bh.y));
-                            const float fz = fmaxf(fabsf(q.z - bl.z), fabsf(q.z - bh.z));
-                            upper = fminf(upper, fx * fx + fy * fy + fz * fz);
-                        }
-                    }
-                if (upper < 3.4e38f) {
-                    const double u = sqrt((double)upper) + 2.0 * slack;
-                    bound = fminf(bound, __double2float_ru(u * u));
-                }
-                // pass 2: FP64 on the boxes that reach inside the bound
-                for (int z = lo[2]; z <= hi[2]; ++z)
-                    for (int y = lo[1]; y <= hi[1]; ++y) {
-                        const int row = dx * y + dxy * z;
-                        measure(span_begin(row + lo[0]), w.cell_ends[row + hi[0]]);
-                    }
-                return best_tri;
-            }
-        }
-    }
     uint32_t stack[kStackDepth];
     float stack_d[kStackDepth];
     int sp = 0;
@@ -1193,7 +802,7 @@ __global__ void k_query(const WrapDev* __restrict__ wraps) {
 // walk's length varies a lot from vertex to vertex, so fixed blocks hold an
 // SM until their slowest warp ends; here a warp that ends takes the next 32.
 // The grid is what fits on the device at once; `counter` starts at 0.
-__global__ void __launch_bounds__(128, 5) k_query_queue(const WrapDev* __restrict__ wraps, int wrap_count,
+__global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__ wraps, int wrap_count,
                                                     int* __restrict__ counter) {
     extern __shared__ int first[];  // wrap_count + 1: each querying wrap's first item
     for (int i = threadIdx.x; i < wrap_count; i += blockDim.x)

@@ -172,8 +172,6 @@ struct Wrap {
     double* identity_rot = nullptr;  // device (in the arena): identity rotations
     LevelRecord* initial_records = nullptr;  // and the level records a run starts from
     size_t input_bytes = 0;          // the arena's prefix that holds the inputs
-    CellPlan cell_plan;              // the target's cell index (planned once)
-    bool cell_planned = false;
     bool target_ingested = false;    // the device has normalised the target and its normals
     ~Wrap() { arena.release(); }
 };
@@ -306,17 +304,9 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_identity = a.reserve(sizeof(double) * 9 * N);
     const size_t o_init_records = a.reserve(sizeof(LevelRecord) * w.levels);
     w.input_bytes = a.size();
-    // the target's hierarchy and cell index (planned on the normalised target)
+    // the target's hierarchy
     const size_t o_bvh_nodes = a.reserve(sizeof(float4) * 4 * std::max(1, w.F - 1));
     const size_t o_bvh_leaves = a.reserve(sizeof(float4) * kLeafFloat4s * w.F);
-    if (!w.cell_planned) {
-        w.cell_plan = plan_cells(w.target_in.data(), w.Vt, w.target_faces.data(), w.F, w.graph.center,
-                                 w.graph.scale);
-        w.cell_planned = true;
-    }
-    const CellPlan& cells = w.cell_plan;
-    const size_t o_cell_ends = a.reserve(cells.ok ? cells_ends_bytes(cells.cells) : 0);
-    const size_t o_cell_entries = a.reserve(cells.ok ? sizeof(float4) * 2 * cells.entries : 0);
     // state and scratch
     size_t o_rot[2], o_trans[2], o_diag[2], o_rhs[2], o_off[2];
     for (int i = 0; i < 2; ++i) {
@@ -447,18 +437,6 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.bvh_leaves = a.at<float4>(o_bvh_leaves);
     D.rank_window = static_cast<float>(kRankWindow * normalized_diagonal(w.target_in.data(), w.Vt,
                                                                          w.graph.center, w.graph.scale));
-    if (cells.ok) {
-        D.cell_ends = a.at<int32_t>(o_cell_ends);
-        D.cell_total = reinterpret_cast<const unsigned long long*>(D.cell_ends + cells_total_slot(cells.cells));
-        D.cell_entries = a.at<float4>(o_cell_entries);
-        for (int k = 0; k < 3; ++k) {
-            D.cell_origin[k] = cells.origin[k];
-            D.cell_dims[k] = cells.dims[k];
-        }
-        D.cell_inv = cells.inv;
-        D.cell_count = static_cast<int>(cells.cells);
-        D.cell_entry_count = static_cast<int>(cells.entries);
-    }
     if (!staging) in.put(const_cast<double*>(D.tpl), tpl_v);
     in.put(const_cast<int32_t*>(D.tpl_faces), w.template_faces);
     in.put(const_cast<int32_t*>(D.vf_begin), vf_begin);
@@ -583,28 +561,20 @@ void reset_device(Wrap& w, cudaStream_t stream, void* lbvh_scratch, LbvhExport* 
                                      stream, lbvh_out);
     check(cudaGetLastError(), "lbvh build");
     D.bvh_root = static_cast<int>(root);
-    // the cell index, from the hierarchy's leaves, in the same scratch
-    build_cells(D.bvh_leaves, w.F, w.cell_plan, const_cast<int32_t*>(D.cell_ends),
-                const_cast<float4*>(D.cell_entries), lbvh_scratch, stream);
-    check(cudaGetLastError(), "cell index build");
 }
 
-// Build scratch of one wrap's target structures (the hierarchy, then the cell
-// index, in stream order).
+// Build scratch of one wrap's target structures (its ingestion, then its
+// hierarchy, in stream order).
 size_t build_scratch_bytes(const Wrap& w) {
-    return std::max(std::max(lbvh_scratch_bytes(w.F), cells_scratch_bytes(w.cell_plan.cells)),
-                    ingest_scratch_bytes(w.Vt, w.F));
+    return std::max(lbvh_scratch_bytes(w.F), ingest_scratch_bytes(w.Vt, w.F));
 }
 
 // Kernels one hierarchy build launches (lbvh_build): centroids, two bound
 // passes, Morton codes, 8 radix passes of 3 kernels, Karras, refit, 2 packs.
 int lbvh_build_launches(int n) { return 4 + 8 * 3 + (n > 1 ? 1 : 0) + 1 + (n > 1 ? 2 : 1); }
 
-// Kernels the target structures of a wrap launch: the hierarchy and, when the
-// wrap has one, the cell index.
-int target_build_launches(const Wrap& w) {
-    return lbvh_build_launches(w.F) + (w.cell_plan.ok ? cells_build_launches() : 0);
-}
+// Kernels the target structures of a wrap launch per reset: the hierarchy.
+int target_build_launches(const Wrap& w) { return lbvh_build_launches(w.F); }
 
 }  // namespace
 
