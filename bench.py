@@ -375,6 +375,11 @@ def roofline(batch, peak_gbs: float) -> tuple[dict, dict]:
     detail["timing"] = ("CUDA events per kernel group on a re-run whose ticks run the solve and refresh "
                         "branches one after the other; the timed step runs them side by side")
     detail["tick_ms_total"] = total_tick
+    # how the step's time is spread over its ticks: the share of each tenth of
+    # the ticks, in order (late tenths carry only the wraps still running)
+    tenth = max(1, len(records) // 10)
+    detail["tick_ms_by_tenth"] = [round(sum(r["tick_ms"] for r in records[i:i + tenth]), 1)
+                                  for i in range(0, len(records), tenth)]
     detail["work"] = work
     line = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak_gbs,
             "unit": "GB/s", "frac": achieved / peak_gbs if peak_gbs else None,
