@@ -801,7 +801,7 @@ def run_precision_compare(args) -> None:
             "perturbed": {}}
     for sigma in sigmas:
         members = [_against(v, r, ref_v, ref_report, diag)
-                   for (sg, _, _, _), (_, v, r) in zip(jobs, runs) if sg == sigma]
+                   for (_, sg, _, _), (_, v, r) in zip(jobs, runs) if sg == sigma]
         spread = {k: [m[k] for m in members] for k in ("max_vertex_error_over_diag",
                                                        "rms_vertex_error_over_diag",
                                                        "final_energy_rel_error")}
