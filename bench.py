@@ -68,6 +68,9 @@ WORKLOAD = ("config 3: 64 uneven wraps batched (template 5k-50k vertices log-uni
             "nodes = V/15 over 4 levels, k=6, target 50k-500k triangles log-uniform), route B")
 INSTANCES = 64
 REFERENCE_SAMPLE = 16   # wraps per CPU-reference sample
+# DRAM traffic of a seeded closest-point query over its algorithmic bytes,
+# measured with ncu on one config-2 wrap (median of 15 seeded launches)
+QUERY_TRAFFIC_RATIO = 1.22
 SAME_CONFIG_REASON = (
     "the reference arm times the reference's FP64 route A on the 16 smallest of config 3's 64 wraps "
     "at its own caps (k=4 bindings, 4-NN edges; src/core/sampling.h:17, graph.h:52-53), one process "
@@ -381,9 +384,15 @@ def roofline(batch, peak_gbs: float) -> tuple[dict, dict]:
     detail["tick_ms_by_tenth"] = [round(sum(r["tick_ms"] for r in records[i:i + tenth]), 1)
                                   for i in range(0, len(records), tenth)]
     detail["work"] = work
+    per_launch = nbytes[dominant] / max(1, launches)
+    traffic = QUERY_TRAFFIC_RATIO * per_launch if dominant == "query" else None
     line = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak_gbs,
             "unit": "GB/s", "frac": achieved / peak_gbs if peak_gbs else None,
-            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": None,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": traffic,
+            "traffic_source": (f"{QUERY_TRAFFIC_RATIO} x the algorithmic bytes per launch: the DRAM "
+                               "read+write of seeded query launches of one config-2 wrap over their "
+                               "algorithmic bytes (ncu, profiles/k_query_dram_config2_wrap.md)")
+                              if traffic is not None else None,
             "algorithmic_bytes_per_launch": nbytes[dominant] / max(1, launches),
             "avg_launch_us": 1000.0 * ms[dominant] / max(1, launches)}
     return line, detail
