@@ -19,7 +19,6 @@ constexpr int kMaxSlots = 8;        // binding support (the reference caps at 4)
 constexpr int kMaxLevels = 16;
 constexpr int kEnergyKinds = 5;     // p2p, plane, smoothness, anchor, landmark
 constexpr int kStackDepth = 64;     // LBVH traversal stack
-constexpr int kQueryCandidates = 32;  // leaves a query's walk may list for its FP64 pass
 constexpr int kPartialStride = 8;   // doubles per energy partial record
 
 // Device phases of one wrap.  They mirror the reference session's
@@ -163,8 +162,6 @@ struct WrapDev {
     double* corr_normal;          // V x 3
     double* corr_distance;        // V
     int32_t* corr_triangle;       // V (previous winner seeds the next search)
-    int32_t* query_candidates;    // V x kQueryCandidates: leaves the walk reached
-    int32_t* query_candidate_count;  // V (kQueryCandidates + 1: too many, walk again in full)
     uint8_t* corr_code;           // V rejection code
     double* robust;               // V
     float4* residual32;           // V: (o.x, o.y, o.z, plane value scale) per vertex

@@ -732,41 +732,52 @@ __device__ inline bool queries(int phase) {
     return phase == kPhaseTransfer || phase == kPhaseRefresh || phase == kPhaseFinal;
 }
 
-// The correspondence of template vertex v from its winning triangle `tri`
-// (-1: none), with the filters in the order the reference applies them
-// (correspondence.cpp:35-80) and the reweighting of route_a.cpp:19-38.
-__device__ void store_correspondence(const WrapDev& w, int level, int v, int tri) {
+// The correspondence of template vertex v, with the filters in the order the
+// reference applies them (correspondence.cpp:35-80) and the reweighting of
+// route_a.cpp:19-38.
+__device__ void query_vertex(const WrapDev& w, int level, int v) {
     uint8_t code = 0;
     D3 point = {0, 0, 0}, normal = {0, 0, 0};
     double distance = 0.0, robust = 1.0;
-    if (tri >= 0) {
-        const D3 q = load_d3(w.deformed, v);
-        const int32_t* f = w.tgt_faces + (long)tri * 3;
-        double bary[3];
-        point = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
-                                   load_d3(w.tgt_points, f[2]), bary);
-        const D3 d = vsub(point, q);
-        distance = __dsqrt_rn(vdot(d, d));
-        const D3 n0 = load_d3(w.tgt_normals, f[0]), n1 = load_d3(w.tgt_normals, f[1]),
-                 n2 = load_d3(w.tgt_normals, f[2]);
-        normal = vnormalized(vadd(vadd(vmul(n0, bary[0]), vmul(n1, bary[1])), vmul(n2, bary[2])));
-        if (distance > w.distance_threshold) {
-            code = 1;
-        } else if (vdot(load_d3(w.qnormals, v), normal) < w.min_normal_cosine) {
-            code = 2;
-        } else if (distance > 0.0) {
-            const D3 offset = vsub(q, point);
-            const double slope = __ddiv_rn(fabs(vdot(normal, offset)), distance);
-            if (slope < w.min_slope) code = 3;
-        }
-        if (code == 0) {
-            const D3 o = vsub(q, point);
-            const double squared = vdot(o, o);
-            const double threshold = w.robust_threshold[level];
-            robust = threshold > 0.0 ? robust_weight(w.robust_kernel[level], squared, threshold) : 1.0;
-        }
+    int tri = -1;
+    if (w.mask && !w.mask[v]) {
+        code = 4;
+        tri = w.corr_triangle[v];
     } else {
-        code = 1;
+        const float4 q32 = w.deformed32[v];
+        int overflow = 0;
+        tri = nearest_triangle(w, {q32.x, q32.y, q32.z}, load_d3(w.deformed, v), w.corr_triangle[v],
+                               &overflow);
+        if (overflow) atomicOr(&w.control->error, 1);
+        if (tri >= 0) {
+            const D3 q = load_d3(w.deformed, v);
+            const int32_t* f = w.tgt_faces + (long)tri * 3;
+            double bary[3];
+            point = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
+                                       load_d3(w.tgt_points, f[2]), bary);
+            const D3 d = vsub(point, q);
+            distance = __dsqrt_rn(vdot(d, d));
+            const D3 n0 = load_d3(w.tgt_normals, f[0]), n1 = load_d3(w.tgt_normals, f[1]),
+                     n2 = load_d3(w.tgt_normals, f[2]);
+            normal = vnormalized(vadd(vadd(vmul(n0, bary[0]), vmul(n1, bary[1])), vmul(n2, bary[2])));
+            if (distance > w.distance_threshold) {
+                code = 1;
+            } else if (vdot(load_d3(w.qnormals, v), normal) < w.min_normal_cosine) {
+                code = 2;
+            } else if (distance > 0.0) {
+                const D3 offset = vsub(q, point);
+                const double slope = __ddiv_rn(fabs(vdot(normal, offset)), distance);
+                if (slope < w.min_slope) code = 3;
+            }
+            if (code == 0) {
+                const D3 o = vsub(q, point);
+                const double squared = vdot(o, o);
+                const double threshold = w.robust_threshold[level];
+                robust = threshold > 0.0 ? robust_weight(w.robust_kernel[level], squared, threshold) : 1.0;
+            }
+        } else {
+            code = 1;
+        }
     }
     store_d3(w.corr_point, v, point);
     store_d3(w.corr_normal, v, normal);
@@ -776,198 +787,7 @@ __device__ void store_correspondence(const WrapDev& w, int level, int v, int tri
     w.robust[v] = robust;
 }
 
-// A masked vertex keeps its previous triangle and takes no correspondence.
-__device__ inline void store_masked(const WrapDev& w, int v) {
-    store_d3(w.corr_point, v, {0, 0, 0});
-    store_d3(w.corr_normal, v, {0, 0, 0});
-    w.corr_distance[v] = 0.0;
-    w.corr_code[v] = 4;
-    w.robust[v] = 1.0;
-}
-
-// The whole query of vertex v in one pass (the combined exact walk).
-__device__ void query_vertex(const WrapDev& w, int level, int v) {
-    if (w.mask && !w.mask[v]) {
-        store_masked(w, v);
-        return;
-    }
-    const float4 q32 = w.deformed32[v];
-    int overflow = 0;
-    const int tri = nearest_triangle(w, {q32.x, q32.y, q32.z}, load_d3(w.deformed, v), w.corr_triangle[v],
-                                     &overflow);
-    if (overflow) atomicOr(&w.control->error, 1);
-    store_correspondence(w, level, v, tri);
-}
-
-// ---- the query in two passes ---------------------------------------------
-//
-// The walk (pass 1) uses FP32 only: boxes to prune, and at each leaf the FP32
-// closest-point routine's point to bound the triangle's distance from above.
-// Where FP32 misplaces the point (sliver triangles) the point still lies on
-// the triangle, so its distance is still an upper bound, up to a rounding far
-// below the slack.  The walk lists every leaf it reaches; the exact winner's
-// box always lies inside the bound, so the winner is always listed.  Pass 2
-// measures the listed triangles with the FP64 routine and takes the winner by
-// the exact rule (smallest FP64 distance, ties to the lowest index), so the
-// result is the combined walk's.  Splitting them keeps the walk's loop free
-// of the FP64 routine's branches and registers, so more walks run at once.
-// A walk that reaches more than kQueryCandidates leaves stops, and pass 2
-// runs the combined walk for that vertex.
-
-// Squared distance from q to the FP32 closest point of triangle (a, b, c):
-// the closest-point routine's steps (closest_point.cpp:24-121) in FP32.
-__device__ float triangle_upper_fp32(F3 p, F3 a, F3 b, F3 c) {
-    const F3 ab = b - a, ac = c - a, ap = p - a;
-    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
-    F3 x;
-    if (d1 <= 0.0f && d2 <= 0.0f) {
-        x = a;
-    } else {
-        const F3 bp = p - b;
-        const float d3 = dot(ab, bp), d4 = dot(ac, bp);
-        const float vc = d1 * d4 - d3 * d2;
-        const F3 cp = p - c;
-        const float d5 = dot(ab, cp), d6 = dot(ac, cp);
-        const float vb = d5 * d2 - d1 * d6;
-        const float va = d3 * d6 - d5 * d4;
-        if (d3 >= 0.0f && d4 <= d3) {
-            x = b;
-        } else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
-            const float den = d1 - d3;
-            x = a + ab * (den != 0.0f ? fminf(fmaxf(d1 / den, 0.0f), 1.0f) : 0.0f);
-        } else if (d6 >= 0.0f && d5 <= d6) {
-            x = c;
-        } else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
-            const float den = d2 - d6;
-            x = a + ac * (den != 0.0f ? fminf(fmaxf(d2 / den, 0.0f), 1.0f) : 0.0f);
-        } else if (va <= 0.0f && d4 - d3 >= 0.0f && d5 - d6 >= 0.0f) {
-            const float den = (d4 - d3) + (d5 - d6);
-            x = b + (c - b) * (den != 0.0f ? fminf(fmaxf((d4 - d3) / den, 0.0f), 1.0f) : 0.0f);
-        } else {
-            const float den = va + vb + vc;
-            float v = den != 0.0f ? vb / den : 0.0f, u = den != 0.0f ? vc / den : 0.0f;
-            v = fminf(fmaxf(v, 0.0f), 1.0f);
-            u = fminf(fmaxf(u, 0.0f), 1.0f - v);  // a convex combination: a point of the triangle
-            x = a + ab * v + ac * u;
-        }
-    }
-    const F3 d = p - x;
-    return dot(d, d);
-}
-
-__device__ inline F3 leaf_corner32(const double2* l, int k) {
-    // corners k = 0, 1, 2 of a leaf: (l0.x, l0.y, l1.x), (l1.y, l2.x, l2.y), (l3.x, l3.y, l4.x)
-    if (k == 0) return {__double2float_rn(l[0].x), __double2float_rn(l[0].y), __double2float_rn(l[1].x)};
-    if (k == 1) return {__double2float_rn(l[1].y), __double2float_rn(l[2].x), __double2float_rn(l[2].y)};
-    return {__double2float_rn(l[3].x), __double2float_rn(l[3].y), __double2float_rn(l[4].x)};
-}
-
-__device__ void walk_vertex(const WrapDev& w, int v) {
-    int32_t* list = w.query_candidates + (long)v * kQueryCandidates;
-    if (w.mask && !w.mask[v]) {
-        w.query_candidate_count[v] = 0;
-        return;
-    }
-    const float4 q4 = w.deformed32[v];
-    const F3 q = {q4.x, q4.y, q4.z};
-    const double slack = (double)w.rank_window;
-    float best = 3.4e38f;   // FP32 squared upper bound of the nearest triangle's distance
-    float bound = 3.4e38f;  // pruning radius^2: (sqrt(best) + slack)^2, rounded up
-    auto tighten = [&](float u) {
-        if (u < best) {
-            best = u;
-            const double r = sqrt((double)u) + slack;
-            bound = __double2float_ru(r * r);
-        }
-    };
-    const int seed = w.corr_triangle[v];
-    if (seed >= 0 && seed < w.F) {
-        const int32_t* f = w.tgt_faces + (long)seed * 3;
-        auto corner = [&](int k) {
-            const double* pt = w.tgt_points + (long)f[k] * 3;
-            return F3{__double2float_rn(pt[0]), __double2float_rn(pt[1]), __double2float_rn(pt[2])};
-        };
-        tighten(triangle_upper_fp32(q, corner(0), corner(1), corner(2)));
-    }
-    int count = 0;
-    uint32_t stack[kStackDepth];
-    float stack_d[kStackDepth];
-    int sp = 0;
-    uint32_t node = (uint32_t)w.bvh_root;
-    const long step_limit = 4L * (long)w.F + 1024;
-    long steps = 0;
-    while (true) {
-        if (++steps > step_limit) {
-            atomicOr(&w.control->error, 1);
-            break;
-        }
-        if (node & kLeafBit) {
-            const int leaf = (int)(node & ~kLeafBit);
-            if (count == kQueryCandidates) {  // too many: pass 2 walks this vertex in full
-                count = kQueryCandidates + 1;
-                break;
-            }
-            list[count++] = leaf;
-            const double2* l = reinterpret_cast<const double2*>(w.bvh_leaves) + (long)leaf * kLeafFloat4s;
-            tighten(triangle_upper_fp32(q, leaf_corner32(l, 0), leaf_corner32(l, 1), leaf_corner32(l, 2)));
-        } else {
-            const float4* nd = w.bvh_nodes + (long)node * 4;
-            const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
-            const float dl = box_distance(q, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
-            const float dr = box_distance(q, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
-            const uint32_t cl = __float_as_uint(n3.x), cr = __float_as_uint(n3.y);
-            const bool hl = dl < bound, hr = dr < bound;
-            if (hl && hr) {
-                const bool left_first = dl <= dr;
-                if (sp < kStackDepth) {
-                    stack[sp] = left_first ? cr : cl;
-                    stack_d[sp] = left_first ? dr : dl;
-                    ++sp;
-                } else {
-                    atomicOr(&w.control->error, 1);
-                }
-                node = left_first ? cl : cr;
-                continue;
-            }
-            if (hl) { node = cl; continue; }
-            if (hr) { node = cr; continue; }
-        }
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            if (stack_d[sp] < bound) { node = stack[sp]; found = true; break; }
-        }
-        if (!found) break;
-    }
-    w.query_candidate_count[v] = count;
-}
-
-__device__ void finish_vertex(const WrapDev& w, int level, int v) {
-    if (w.mask && !w.mask[v]) {
-        store_masked(w, v);
-        return;
-    }
-    const int count = w.query_candidate_count[v];
-    if (count > kQueryCandidates) {
-        query_vertex(w, level, v);
-        return;
-    }
-    const D3 q64 = load_d3(w.deformed, v);
-    const int32_t* list = w.query_candidates + (long)v * kQueryCandidates;
-    double best = 1e300;
-    int best_tri = -1;
-    for (int i = 0; i < count; ++i) {
-        int tri;
-        const double d = leaf_distance(w, list[i], q64, &tri);
-        if (d < best || (d == best && tri < best_tri)) {
-            best = d;
-            best_tri = tri;
-        }
-    }
-    store_correspondence(w, level, v, best_tri);
-}
-
-// Thread per vertex, block row per wrap: the combined walk.
+// Thread per vertex, block row per wrap.
 __global__ void k_query(const WrapDev* __restrict__ wraps) {
     const WrapDev& w = wraps[blockIdx.y];
     const WrapControl c = *w.control;
@@ -982,8 +802,6 @@ __global__ void k_query(const WrapDev* __restrict__ wraps) {
 // walk's length varies a lot from vertex to vertex, so fixed blocks hold an
 // SM until their slowest warp ends; here a warp that ends takes the next 32.
 // The grid is what fits on the device at once; `counter` starts at 0.
-// kPass 0 walks (pass 1 above), kPass 1 measures and stores (pass 2).
-template <int kPass>
 __global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__ wraps, int wrap_count,
                                                     int* __restrict__ counter) {
     extern __shared__ int first[];  // wrap_count + 1: each querying wrap's first item
@@ -1020,11 +838,7 @@ __global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__
             if (first[mid] <= item) lo = mid; else hi = mid - 1;
         }
         const WrapDev& w = wraps[lo];
-        if (kPass == 0) {
-            walk_vertex(w, item - first[lo]);
-        } else {
-            finish_vertex(w, w.control->level, item - first[lo]);
-        }
+        query_vertex(w, w.control->level, item - first[lo]);
     }
 }
 
@@ -1067,20 +881,16 @@ void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaSt
         k_query<<<grid, 128, 0, stream>>>(wraps);
         return;
     }
-    auto resident = [](const void* kernel) {  // blocks of a queue that fit on the device at once
+    static const int resident = [] {  // blocks of the queue that fit on the device at once
         int device = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, sizeof(int) * 1025);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_queue, 128, sizeof(int) * 1025);
         const int blocks = sms * (per_sm > 0 ? per_sm : 1);
         return blocks > 0 ? blocks : 1;
-    };
-    static const int walkers = resident(reinterpret_cast<const void*>(k_query_queue<0>));
-    static const int finishers = resident(reinterpret_cast<const void*>(k_query_queue<1>));
-    // `counter` holds the two passes' queue heads
-    cudaMemsetAsync(counter, 0, 2 * sizeof(int), stream);
-    k_query_queue<0><<<walkers, 128, sizeof(int) * (wrap_count + 1), stream>>>(wraps, wrap_count, counter);
-    k_query_queue<1><<<finishers, 128, sizeof(int) * (wrap_count + 1), stream>>>(wraps, wrap_count, counter + 1);
+    }();
+    cudaMemsetAsync(counter, 0, sizeof(int), stream);
+    k_query_queue<<<resident, 128, sizeof(int) * (wrap_count + 1), stream>>>(wraps, wrap_count, counter);
 }
 
 void launch_closest_points(const WrapDev* wrap, const double* queries, int count,

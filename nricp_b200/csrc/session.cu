@@ -324,8 +324,6 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_cn = a.reserve(sizeof(double) * 3 * V);
     const size_t o_cd = a.reserve(sizeof(double) * V);
     const size_t o_ct = a.reserve(sizeof(int32_t) * V);
-    const size_t o_qcand = a.reserve(sizeof(int32_t) * kQueryCandidates * V);
-    const size_t o_qcount = a.reserve(sizeof(int32_t) * V);
     const size_t o_cc = a.reserve(V);
     const size_t o_rb = a.reserve(sizeof(double) * V);
     const size_t o_r0 = a.reserve(sizeof(float4) * V);
@@ -501,8 +499,6 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.corr_normal = a.at<double>(o_cn);
     D.corr_distance = a.at<double>(o_cd);
     D.corr_triangle = a.at<int32_t>(o_ct);
-    D.query_candidates = a.at<int32_t>(o_qcand);
-    D.query_candidate_count = a.at<int32_t>(o_qcount);
     D.corr_code = a.at<uint8_t>(o_cc);
     D.robust = a.at<double>(o_rb);
     D.residual32 = a.at<float4>(o_r0);
@@ -754,7 +750,7 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
         if (!failure[i].empty()) throw std::runtime_error(failure[i]);
     shape_ = TickShape{};
     shape_.wraps = W;
-    check(cudaMalloc(&query_counter_, 2 * sizeof(int)), "cudaMalloc(query queues)");
+    check(cudaMalloc(&query_counter_, sizeof(int)), "cudaMalloc(query queue)");
     shape_.query_counter = query_counter_;
     if (!side_stream_) {
         check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "stream");
@@ -1832,7 +1828,7 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     }
     check(cudaMalloc(&m.staging_controls, sizeof(WrapControl) * Impl::kLoaders), "cudaMalloc(staging control)");
     check(cudaEventCreate(&m.tick_begin), "event");
-    check(cudaMalloc(&m.query_counter, 2 * sizeof(int)), "cudaMalloc(query queues)");
+    check(cudaMalloc(&m.query_counter, sizeof(int)), "cudaMalloc(query queue)");
     m.shape.query_counter = m.query_counter;
     check(cudaStreamCreateWithFlags(&m.shape.side_stream, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&m.shape.side_fork, cudaEventDisableTiming), "event");

@@ -1769,7 +1769,6 @@ int tick_kernel_launches(const TickShape& s, bool timed) {
     // an untimed tick with a side stream assembles and decides in each branch
     const int per_chain = (s.max_pairs > 0 ? 5 : 4) + 1;  // residual, node, pair, edge, decide; evaluate
     return (s.max_pairs > 0 ? 14 : 13) - (s.route_c ? 0 : 2) + (s.pcg_groups > 0 ? s.pcg_groups : 1) +
-           (s.query_counter ? 1 : 0) +  // the query's second pass
            (s.side_stream && !timed ? per_chain : 0);
 }
 
