@@ -37,7 +37,7 @@ struct LevelDev {
     int node_count;
     int edge_count;        // smoothness edges (a < b)
     int pair_count;        // node-pair groups sharing a vertex (a < b)
-    int offdiag_count;     // edge_count + pair_count blocks
+    int offdiag_count;     // blocks: pair_count, then the edges whose pair shares no vertex
     const double* rest;            // node rest positions, N x 3
     const int32_t* bind_nodes;     // V x kMaxSlots, -1 padded, usable slots only
     const double* bind_weights;    // V x kMaxSlots
@@ -57,7 +57,8 @@ struct LevelDev {
     // touch it; entry = block * 2 + (1 if the node is the block's b side)
     const int32_t* row_begin;      // N + 1
     const int32_t* row_entry;      // pairs: (block * 2 + side, other node)
-    const int32_t* offdiag_nodes;  // offdiag_count x 2 (edges first, then pairs)
+    const int32_t* offdiag_nodes;  // offdiag_count x 2 (pair groups first, then edge-only pairs)
+    const int32_t* edge_block;     // edge_count: the block edge e adds to (< pair_count) or owns
     const int32_t* offdiag_slots;  // offdiag_count x 2: row-entry slots of B (a) and B^T (b)
     int row_entries;               // 2 x offdiag_count
     // warm start from the previous level (level > 0): 4 source nodes + weights

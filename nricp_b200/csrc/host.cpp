@@ -694,10 +694,29 @@ LevelLayout build_layout(const TemplateGraph& graph, int level, int V) {
         L.pair_count = static_cast<int>(L.pair_nodes.size() / 2);
         L.pair_begin.push_back(static_cast<int32_t>(L.pair_entry.size()));
     }
-    // off-diagonal blocks: smoothness edges, then pair groups
-    L.offdiag_nodes = L.edges;
-    L.offdiag_nodes.insert(L.offdiag_nodes.end(), L.pair_nodes.begin(), L.pair_nodes.end());
-    const int B = L.edge_count + L.pair_count;
+    // off-diagonal blocks: one per node pair that shares a vertex (in pair
+    // order), then one per smoothness edge whose pair shares none (in edge
+    // order).  An edge whose pair shares a vertex adds into that pair's block,
+    // so each node pair the system couples has exactly one block.
+    L.offdiag_nodes = L.pair_nodes;
+    L.edge_block.assign(L.edge_count, 0);
+    for (int e = 0; e < L.edge_count; ++e) {
+        const int a = L.edges[e * 2], b = L.edges[e * 2 + 1];
+        int lo = 0, hi = L.pair_count;  // pairs are sorted by (a, b)
+        while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            const int pa = L.pair_nodes[mid * 2], pb = L.pair_nodes[mid * 2 + 1];
+            if (pa < a || (pa == a && pb < b)) lo = mid + 1; else hi = mid;
+        }
+        if (lo < L.pair_count && L.pair_nodes[lo * 2] == a && L.pair_nodes[lo * 2 + 1] == b) {
+            L.edge_block[e] = lo;
+        } else {
+            L.edge_block[e] = static_cast<int32_t>(L.offdiag_nodes.size() / 2);
+            L.offdiag_nodes.push_back(a);
+            L.offdiag_nodes.push_back(b);
+        }
+    }
+    const int B = static_cast<int>(L.offdiag_nodes.size() / 2);
     L.row_begin.assign(N + 1, 0);
     for (int k = 0; k < B; ++k) {
         L.row_begin[L.offdiag_nodes[k * 2] + 1]++;

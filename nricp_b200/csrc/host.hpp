@@ -48,6 +48,9 @@ struct LevelLayout {
     std::vector<int32_t> node_edge_begin, node_edge_list, edges;
     std::vector<int32_t> pair_nodes, pair_begin, pair_entry;
     std::vector<int32_t> row_begin, row_entry, offdiag_nodes, offdiag_slots;
+    // the off-diagonal block that holds smoothness edge e: a node pair's own
+    // block when the pair shares a vertex (< pair_count), else one of its own
+    std::vector<int32_t> edge_block;
     std::vector<int32_t> transfer_nodes, transfer_counts;
     std::vector<double> transfer_weights;
 };

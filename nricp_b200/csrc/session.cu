@@ -240,7 +240,7 @@ void envelope(Wrap& w) {
         w.max_nodes = std::max(w.max_nodes, L.node_count);
         w.max_edges = std::max(w.max_edges, L.edge_count);
         w.max_pairs = std::max(w.max_pairs, L.pair_count);
-        w.max_offdiag = std::max(w.max_offdiag, L.edge_count + L.pair_count);
+        w.max_offdiag = std::max(w.max_offdiag, static_cast<int>(L.offdiag_nodes.size() / 2));
     }
 }
 
@@ -262,12 +262,13 @@ void prepare_host(Wrap& w) {
 }
 
 size_t bytes_of_layout(const LevelLayout& L) {
-    return 256 * 26 + sizeof(double) * (L.rest.size() + L.bind_weights.size() + L.transfer_weights.size()) +
+    return 256 * 27 + sizeof(double) * (L.rest.size() + L.bind_weights.size() + L.transfer_weights.size()) +
            sizeof(int32_t) * (L.bind_nodes.size() + L.bind_counts.size() + L.gather_begin.size() +
                               L.gather_entry.size() + L.node_edge_begin.size() +
                               L.node_edge_list.size() + L.edges.size() + L.pair_nodes.size() +
                               L.pair_begin.size() + L.pair_entry.size() + L.row_begin.size() +
                               L.row_entry.size() + L.offdiag_nodes.size() + L.offdiag_slots.size() +
+                              L.edge_block.size() +
                               L.transfer_nodes.size() +
                               L.transfer_counts.size());
 }
@@ -462,7 +463,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
         G.node_count = L.node_count;
         G.edge_count = L.edge_count;
         G.pair_count = L.pair_count;
-        G.offdiag_count = L.edge_count + L.pair_count;
+        G.offdiag_count = static_cast<int>(L.offdiag_nodes.size() / 2);
         G.rest = put(L.rest);
         G.bind_nodes = put(L.bind_nodes);
         G.bind_weights = put(L.bind_weights);
@@ -479,6 +480,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
         G.row_entry = put(L.row_entry);
         G.offdiag_nodes = put(L.offdiag_nodes);
         G.offdiag_slots = put(L.offdiag_slots);
+        G.edge_block = put(L.edge_block);
         G.row_entries = static_cast<int>(L.row_entry.size() / 2);
         G.transfer_nodes = put(L.transfer_nodes);
         G.transfer_weights = put(L.transfer_weights);
@@ -1024,7 +1026,7 @@ void Batch::inspect(int i, NricpInspect* out) {
     const int level = std::min(c.level, w.levels - 1);
     const LevelLayout& L = w.layouts[level];
     const int N = L.node_count, V = w.V;
-    const int K = L.edge_count + L.pair_count;
+    const int K = static_cast<int>(L.offdiag_nodes.size() / 2);
     out->level = level;
     out->node_count = N;
     out->phase = c.phase;

@@ -1397,6 +1397,18 @@ __device__ inline void store_block_pair(float* out, const LevelDev& L, int k, co
         }
 }
 
+// Adds block k into the system, both ways (the smoothness edge of a node pair
+// whose shared-vertex block is already there).
+__device__ inline void add_block_pair(float* out, const LevelDev& L, int k, const float* blk) {
+    float* A = out + (long)L.offdiag_slots[k * 2] * 36;
+    float* T = out + (long)L.offdiag_slots[k * 2 + 1] * 36;
+    for (int r = 0; r < 6; ++r)
+        for (int q = 0; q < 6; ++q) {
+            A[r * 6 + q] += blk[r * 6 + q];
+            T[q * 6 + r] += blk[r * 6 + q];
+        }
+}
+
 // Warp per node pair: lanes stride over the vertices the two nodes share,
 // each lane keeps a 6x6 block in registers, one butterfly reduction.
 __device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part, int bx) {
@@ -1450,7 +1462,7 @@ __device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part,
         for (int r = 0; r < 6; ++r)
             for (int q = 0; q < 6; ++q)
                 if (r < 3 || q < 3) blk[r * 6 + q] = 0.0f;
-    if (lane == 0) store_block_pair(w.offdiag[1 - c.system], L, L.edge_count + p, blk);
+    if (lane == 0) store_block_pair(w.offdiag[1 - c.system], L, p, blk);
 }
 
 __global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
@@ -1500,7 +1512,14 @@ __device__ __forceinline__ void k_edge_assemble_body(const WrapDev& w, int part,
                 }
                 blk[3 * 6 + 3] = -ws; blk[4 * 6 + 4] = -ws; blk[5 * 6 + 5] = -ws;
             }
-            store_block_pair(w.offdiag[1 - c.system], L, e, blk);
+            // into the pair's block when the pair shares a vertex (the pair
+            // assembly, launched before on the same stream, wrote it this tick)
+            const int k = L.edge_block[e];
+            if (k < L.pair_count) {
+                add_block_pair(w.offdiag[1 - c.system], L, k, blk);
+            } else {
+                store_block_pair(w.offdiag[1 - c.system], L, k, blk);
+            }
         }
     }
     __shared__ double scratch[33];

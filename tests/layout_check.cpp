@@ -78,8 +78,25 @@ void check_level(const TemplateGraph& g, int level, int V) {
     begin.push_back(static_cast<int32_t>(entries.size()));
     expect(L.pair_nodes == nodes && L.pair_begin == begin && L.pair_entry == codes &&
            L.pair_count == static_cast<int>(nodes.size() / 2), "pair groups", V, level);
-    // smoothness edges, then pair groups, each seen from both of its nodes
-    const int B = L.edge_count + L.pair_count;
+    // off-diagonal blocks: the pair groups, then each smoothness edge whose
+    // node pair shares no vertex, in edge order; an edge whose pair shares one
+    // adds into that pair's block
+    std::vector<int32_t> blocks = nodes, edge_block;
+    for (int e = 0; e < static_cast<int>(G.edges.size() / 2); ++e) {
+        const int a = G.edges[e * 2], b = G.edges[e * 2 + 1];
+        int found = -1;
+        for (int p = 0; p < static_cast<int>(nodes.size() / 2) && found < 0; ++p)
+            if (nodes[p * 2] == a && nodes[p * 2 + 1] == b) found = p;
+        if (found < 0) {
+            found = static_cast<int>(blocks.size() / 2);
+            blocks.push_back(a);
+            blocks.push_back(b);
+        }
+        edge_block.push_back(found);
+    }
+    expect(L.offdiag_nodes == blocks && L.edge_block == edge_block, "off-diagonal blocks", V, level);
+    // each block seen from both of its nodes
+    const int B = static_cast<int>(blocks.size() / 2);
     bool rows = L.edges == G.edges && static_cast<int>(L.offdiag_nodes.size()) == 2 * B;
     for (int k = 0; k < B && rows; ++k) {
         const int a = L.offdiag_nodes[k * 2], b = L.offdiag_nodes[k * 2 + 1];

@@ -1,6 +1,6 @@
 """The host level layouts (build_layout in nricp_b200/csrc/host.cpp): the
-usable bindings, gather lists, node-pair groups, off-diagonal rows and
-warm-start bindings the device kernels walk, each checked against a direct
+usable bindings, gather lists, node-pair groups, off-diagonal blocks (one per
+coupled node pair) and rows, and warm-start bindings the device kernels walk, each checked against a direct
 restatement (tests/layout_check.cpp) on seeded graphs with planted repeated
 nodes, zero weights and out-of-range nodes."""
 
