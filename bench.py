@@ -339,8 +339,8 @@ def query_bytes(s: dict) -> float:
 
 
 def pcg_bytes(s: dict) -> float:
-    # per iteration: N x 504 + (E + G) x 248
-    return s["nodes"] * 504 + (s["edges"] + s["pairs"]) * 248
+    # per iteration: N x 504 + B x 248 (B off-diagonal blocks, one per coupled node pair)
+    return s["nodes"] * 504 + s["offdiag_blocks"] * 248
 
 
 def assembly_bytes(s: dict) -> float:

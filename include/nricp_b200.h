@@ -268,11 +268,12 @@ typedef struct NricpTickRecord {
 } NricpTickRecord;
 int nricp_batch_tick_records(NricpBatch* batch, NricpTickRecord* out, int capacity,
                              int* count);
-/* Sizes of one level of one wrap (14 entries): nodes, smoothness edges,
+/* Sizes of one level of one wrap (15 entries): nodes, smoothness edges,
  * node-pair groups, (vertex, slot) entries, pair entries, template vertices,
  * target triangles, target vertices, template triangles, level count; then
  * the work the last run did in the level: solves, PCG iterations,
- * closest-point queries (passes over the template), assemblies. */
+ * closest-point queries (passes over the template), assemblies; last, the
+ * system's off-diagonal blocks (one per node pair it couples). */
 int nricp_batch_level_sizes(NricpBatch* batch, int index, int level, int32_t* sizes);
 void nricp_batch_destroy(NricpBatch* batch);
 /* One call: create, run, results, destroy. */

@@ -1006,6 +1006,8 @@ void Batch::level_sizes(int i, int level, int* sizes) const {
     sizes[11] = r.pcg_iterations;
     sizes[12] = r.queries;
     sizes[13] = r.assemblies;
+    sizes[14] = static_cast<int>(L.offdiag_nodes.size() / 2);
+    static_assert(kLevelSizeEntries == 15, "entries written above");
 }
 
 void Batch::finish() {

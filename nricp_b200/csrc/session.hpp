@@ -64,7 +64,7 @@ public:
     // Device time of reset() + run() on the batch's stream (CUDA events).
     double timed_step();
     // Sizes and work counters of one level (kLevelSizeEntries ints).
-    static constexpr int kLevelSizeEntries = 14;
+    static constexpr int kLevelSizeEntries = 15;
     void level_sizes(int i, int level, int* sizes) const;
     // Cluster size of the solve launch.  > 0: that size for every wrap; 0:
     // each wrap its own latency cluster (about 128 nodes per CTA), one launch

@@ -219,6 +219,33 @@ __device__ inline T warp_sum(T v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// Warp sums of N values at once, by recursive halving: at lane distance
+// o = 16, 8, .., 1 each lane keeps half of its values (the upper half when
+// its lane bit o is set) and adds its partner's copy of that half.  Each
+// total is formed by the same additions as `warp_sum` of that value (x + y
+// and y + x round alike), so the bits are the same, with ~N shuffles instead
+// of 5N.  Afterwards this lane holds the totals of values
+// [first, first + count) in v[0 .. count).
+template <int N, int O = 16>
+__device__ __forceinline__ void warp_sum_halving(float* v, int lane, int& first, int& count) {
+    if constexpr (O >= 1) {
+        constexpr int H = (N + 1) / 2;
+        const bool upper = (lane & O) != 0;
+#pragma unroll
+        for (int i = 0; i < H; ++i) {
+            const float lo = v[i];
+            const float hi = i + H < N ? v[i + H] : 0.0f;
+            v[i] = (upper ? hi : lo) + __shfl_xor_sync(0xffffffffu, upper ? lo : hi, O);
+        }
+        if (upper) {
+            first += H;
+            count = count > H ? count - H : 0;
+        } else {
+            count = count < H ? count : H;
+        }
+        warp_sum_halving<H, O / 2>(v, lane, first, count);
+    }
+}
 // Block sum in a fixed order; every thread returns the total.
 template <int kThreadsT>
 __device__ inline double block_sum(double v, double* scratch) {
@@ -1354,19 +1381,30 @@ __device__ __forceinline__ void k_node_assemble_body(const WrapDev& w, int part,
             }
         }
         if (build) {
-            for (int i = 0; i < 21; ++i) d[i] = warp_sum(d[i]);
-            for (int i = 0; i < 6; ++i) g[i] = warp_sum(g[i]);
-            if (lane == 0) {
+            // the 21 upper-triangle sums and the 6 of the rhs, spread over the
+            // lanes; each lane stores what it holds
+            float v[27];
+            for (int i = 0; i < 21; ++i) v[i] = d[i];
+            for (int i = 0; i < 6; ++i) v[21 + i] = g[i];
+            int first = 0, count = 27;
+            warp_sum_halving<27>(v, lane, first, count);
+            if (count > 0) {
                 float* D = w.diag[next] + node * 36;
                 float* G = w.rhs[next] + node * 6;
                 const bool restricted = c.route == 1;
-                for (int r = 0; r < 6; ++r)
-                    for (int q = 0; q < 6; ++q) {
-                        float value = r <= q ? d[tri_index(r, q)] : d[tri_index(q, r)];
-                        if (restricted && (r < 3 || q < 3)) value = (r == q) ? 1.0f : 0.0f;
-                        D[r * 6 + q] = value;
-                    }
-                for (int k = 0; k < 6; ++k) G[k] = (restricted && k < 3) ? 0.0f : g[k];
+                const int j = first;
+                if (j < 21) {
+                    int r = 0;
+                    while (tri_index(r + 1, r + 1) <= j) ++r;  // row of upper-triangle entry j
+                    const int q = j - tri_index(r, r) + r;
+                    float value = v[0];
+                    if (restricted && (r < 3 || q < 3)) value = (r == q) ? 1.0f : 0.0f;
+                    D[r * 6 + q] = value;
+                    D[q * 6 + r] = value;
+                } else {
+                    const int k = j - 21;
+                    G[k] = (restricted && k < 3) ? 0.0f : v[0];
+                }
             }
         }
     }
@@ -1457,12 +1495,20 @@ __device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part,
                 for (int q = 0; q < 6; ++q) blk[r * 6 + q] += s * ua[r] * ub[q];
         }
     }
-    for (int i = 0; i < 36; ++i) blk[i] = warp_sum(blk[i]);
-    if (c.route == 1)
-        for (int r = 0; r < 6; ++r)
-            for (int q = 0; q < 6; ++q)
-                if (r < 3 || q < 3) blk[r * 6 + q] = 0.0f;
-    if (lane == 0) store_block_pair(w.offdiag[1 - c.system], L, p, blk);
+    // the 36 sums spread over the lanes (two each at most); each lane stores
+    // what it holds, both ways
+    int first = 0, count = 36;
+    warp_sum_halving<36>(blk, lane, first, count);
+    float* A = w.offdiag[1 - c.system] + (long)L.offdiag_slots[p * 2] * 36;
+    float* T = w.offdiag[1 - c.system] + (long)L.offdiag_slots[p * 2 + 1] * 36;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        if (i >= count) break;
+        const int j = first + i, r = j / 6, q = j - r * 6;
+        const float value = (c.route == 1 && (r < 3 || q < 3)) ? 0.0f : blk[i];
+        A[r * 6 + q] = value;
+        T[q * 6 + r] = value;
+    }
 }
 
 __global__ void __launch_bounds__(kNodeThreads, 3) k_pair_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {

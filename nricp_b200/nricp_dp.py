@@ -190,11 +190,11 @@ class WrapBatch:
                  "tick_ms": r.tick_ms} for r in records[:count.value]]
 
     def level_sizes(self, index: int, level: int) -> dict:
-        sizes = (C.c_int32 * 14)()
+        sizes = (C.c_int32 * 15)()
         check(load().nricp_batch_level_sizes(self._handle, index, level, sizes))
         keys = ("nodes", "edges", "pairs", "entries", "pair_entries", "vertices",
                 "target_triangles", "target_vertices", "template_triangles", "levels",
-                "solves", "pcg_iterations", "queries", "assemblies")
+                "solves", "pcg_iterations", "queries", "assemblies", "offdiag_blocks")
         return dict(zip(keys, list(sizes)))
 
 
