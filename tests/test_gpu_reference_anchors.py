@@ -14,10 +14,13 @@ from its src/cuda by oracle/build.py).
   by a fixed 12 sweeps of FP32 Jacobi, assembly with atomics -- and its
   replace-not-step rotation update carries those differences forward, so it
   is held here the way the reference's own tests hold a route
-  (tests/test_route_c.py:126-148): the same schedule (outer iterations equal,
-  inner iterations within 2 per level), fit quality within 10 % (mean
+  (tests/test_route_c.py:126-148): the same schedule (outer iterations within
+  1 and inner iterations within 2 per level), fit quality within 10 % (mean
   distance to the ground truth, which is the target's vertex of the same
-  index), and final energy within 10 %.  The largest vertex gap is printed:
+  index), and final energy within 10 %.  The reference's route C sums its
+  assembly with FP32 atomics, so its own schedule is not the same from run
+  to run: on the session fixture its second level took 4 outer iterations in
+  four runs of this test and 3 in a fifth.  The largest vertex gap is printed:
   measured, 1.3e-2 to 2.2e-2 of unit-scale coordinates on the mirror-symmetric
   fixtures, 1e-3 on the asymmetric one.  On the asymmetric fixture, which has
   no exact closest-point ties, this library's route C must lie within 1e-4 of
@@ -133,7 +136,8 @@ def test_route_c_restatement_agrees_with_the_references_route_c(dp, device, orac
     gap = np.abs(np.asarray(theirs["vertices"]) - np.asarray(restated["vertices"])).max()
     print(f"{name}: iterations {t_iter} (reference) {r_iter} (restatement); mean fit {t_fit:.4e} / "
           f"{r_fit:.4e}; energy {t_e:.6e} / {r_e:.6e}; largest vertex gap {gap:.2e}")
-    assert [o for o, _ in t_iter] == [o for o, _ in r_iter]
+    assert len(t_iter) == len(r_iter)
+    assert all(abs(a - b) <= 1 for (a, _), (b, _) in zip(t_iter, r_iter))
     assert all(abs(a - b) <= 2 for (_, a), (_, b) in zip(t_iter, r_iter))
     assert abs(r_fit - t_fit) <= 0.10 * t_fit
     assert abs(r_e - t_e) <= 0.10 * abs(t_e)
