@@ -100,6 +100,10 @@ def parse_args():
     p.add_argument("--capture-steps", type=int, default=0,
                    help="profiler captures: the config-2 wrap through RouteBSession for this many "
                         "ticks, eager launches, nothing timed")
+    p.add_argument("--capture-batch", type=int, default=0, metavar="N",
+                   help="profiler captures: one step of a batch of config 3's first N wraps with "
+                        "eager launches (the kernel-group re-run, branches one after the other), "
+                        "nothing timed")
     p.add_argument("--precision-compare", metavar="IN.npz",
                    help="CPU only: the reference's FP64 route A on config 5 and its spread under "
                         "perturbations, against the GPU results of --precision ('-': none)")
@@ -843,6 +847,24 @@ def run_capture(args) -> None:
     print(json.dumps({"capture_steps": args.capture_steps, "ticks": session.ticks()[0]}), flush=True)
 
 
+def run_capture_batch(args) -> None:
+    """One batch step of config 3's first N wraps with eager launches, for
+    an ncu launch list of the batch's kernels: the re-run that times the
+    kernel groups (reset, hierarchy builds, every tick with its solve and
+    refresh branches one after the other) and nothing else."""
+    import torch
+
+    from nricp_b200 import nricp_dp as dp
+    from nricp_b200 import synthetic as S
+
+    cases = [S.config3_case(spec) for spec in S.config3_specs(args.seed)[: args.capture_batch]]
+    batch = dp.WrapBatch([(*c.args(), c.options) for c in cases])
+    batch.tune(-1)
+    records = batch.profile()
+    torch.cuda.synchronize()
+    print(json.dumps({"capture_batch": args.capture_batch, "ticks": len(records)}), flush=True)
+
+
 # Host allocator settings of a long-running caller: glibc keeps freed memory
 # instead of returning it to the system after every batch, so the next batch
 # does not fault it in again (without them an end-to-end call of the 64-wrap
@@ -857,6 +879,8 @@ def main():
         os.execv(sys.executable, [sys.executable, *sys.argv])  # the same process, the settings in force
     if args.capture_steps:
         return run_capture(args)
+    if args.capture_batch:
+        return run_capture_batch(args)
     if args.precision_variant:
         return run_precision_variant(args)
     if args.precision_compare:
