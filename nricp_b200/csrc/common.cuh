@@ -19,6 +19,7 @@ constexpr int kMaxSlots = 8;        // binding support (the reference caps at 4)
 constexpr int kMaxLevels = 16;
 constexpr int kEnergyKinds = 5;     // p2p, plane, smoothness, anchor, landmark
 constexpr int kStackDepth = 64;     // LBVH traversal stack
+constexpr int kLongCap = 256;       // long walks a wrap lists for its next query's warps
 constexpr int kPartialStride = 8;   // doubles per energy partial record
 
 // Device phases of one wrap.  They mirror the reference session's
@@ -99,6 +100,7 @@ struct WrapControl {
     int error;            // sticky device error (traversal overflow, ...)
     int steps;            // ticks that did work for this wrap
     int tick_phase;       // the phase at the start of the current tick
+    int long_cur;         // the list of long walks the next query reads (0 / 1)
     double damping;
     double energy;              // accepted energy with the current correspondences
     double energy_parts[kEnergyKinds];
@@ -163,6 +165,12 @@ struct WrapDev {
     double* corr_normal;          // V x 3
     double* corr_distance;        // V
     int32_t* corr_triangle;       // V (previous winner seeds the next search)
+    // Vertices whose last walk was long, for the next query to give a warp
+    // each: two lists (the one the query reads, long_cur, and the one it
+    // fills), their counts and a flag per vertex and list.
+    int32_t* long_list;           // 2 x kLongCap
+    int32_t* long_count;          // 2
+    uint8_t* long_flag;           // 2 x V
     uint8_t* corr_code;           // V rejection code
     double* robust;               // V
     float4* residual32;           // V: (o.x, o.y, o.z, plane value scale) per vertex

@@ -30,9 +30,10 @@ void ingest_target(double* points, int vertex_count, const int32_t* faces, int f
                    cudaStream_t stream);
 int ingest_launches(int vertex_count, int face_count);
 
-// The closest-point query of every querying wrap: with `counter` (a device
-// int), one queue of vertices over a grid that fits on the device at once;
-// without, a block row per wrap.
+// The closest-point query of every querying wrap: with `counter` (two device
+// ints), over a grid that fits on the device at once, the wraps' listed long
+// walks a warp each, then a queue of the other vertices a thread each;
+// without, a thread per vertex in a block row per wrap.
 void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaStream_t stream,
                   int* counter = nullptr);
 void launch_closest_points(const WrapDev* wrap, const double* queries, int count, double* points,
@@ -61,7 +62,7 @@ struct TickShape {
     const int* pcg_group_index[5];       // device: wrap indices of the group
     cudaStream_t pcg_streams[5];         // branch streams (index 0 unused)
     cudaEvent_t pcg_fork, pcg_join[5];
-    int* query_counter;                  // device: the query queue's next item (null: no queue)
+    int* query_counter;                  // device: the query queues' heads, 2 ints (null: no queue)
     // The refresh chain's branch (null: one chain on the tick's stream).
     cudaStream_t side_stream;
     cudaEvent_t side_fork, side_join;

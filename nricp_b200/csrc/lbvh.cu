@@ -663,8 +663,10 @@ __device__ inline double leaf_distance(const WrapDev& w, int leaf, D3 q, int* tr
 // boxes and query; every triangle reached is measured in FP64 -- an FP32
 // closest-point routine can misplace its point on thin sliver triangles by
 // far more than any fixed window.  `seed` is a triangle whose distance bounds
-// the search from the start.  Returns the winner, or -1.
-__device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* overflow) {
+// the search from the start.  Returns the winner, or -1; `steps_taken` (if
+// given) receives the nodes and leaves visited.
+__device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* overflow,
+                                long* steps_taken = nullptr) {
     const double slack = (double)w.rank_window;
     double best = 1e300;     // FP64 squared distance of the best triangle so far
     float bound = 3.4e38f;   // FP32 pruning radius^2: (sqrt(best) + slack)^2, rounded up
@@ -725,6 +727,132 @@ __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* o
         }
         if (!found) break;
     }
+    if (steps_taken) *steps_taken = steps;
+    return best_tri;
+}
+
+// Walks longer than this many steps put their vertex on the wrap's list for
+// its next query, where a warp walks it (a vertex over a hole in the target,
+// or above the fan of slivers at a lat-long pole, stays far from the nearest
+// triangles and walks hundreds to thousands of steps query after query).
+constexpr long kLongWalk = 512;
+// A warp's stack: 32 entries for each of 32 levels of pending subtrees.
+constexpr int kWarpStack = 1024;
+
+// The nearest triangle for `q` found by the 32 lanes of a warp together: the
+// same pruning and the same winner rule as `nearest_triangle`, so the same
+// answer, with up to 32 pending subtrees taken from the stack at a time, so
+// that a walk of thousands of steps takes tens to a hundred dependent rounds.
+// `nodes` / `dists` are the warp's stack.  Should the stack not hold a
+// round's children, the rest of the walk is left to one lane
+// (`*unfinished`), seeded with the winner so far, which is returned.  Every
+// lane returns the same triangle; `*work` is the entries taken.
+__device__ int nearest_triangle_warp(const WrapDev& w, F3 q, D3 q64, int seed, uint32_t* nodes,
+                                     float* dists, int* overflow, bool* unfinished, long* work) {
+    const int lane = threadIdx.x & 31;
+    const double slack = (double)w.rank_window;
+    double best = 1e300;
+    int best_tri = -1;
+    float bound = 3.4e38f;
+    if (seed >= 0 && seed < w.F) {
+        best = triangle_distance_fp64(w, q64, seed);
+        best_tri = seed;
+        const double r = sqrt(best) + slack;
+        bound = __double2float_ru(r * r);
+    }
+    if (lane == 0) {
+        nodes[0] = (uint32_t)w.bvh_root;
+        dists[0] = 0.0f;
+    }
+    int sp = 1;  // warp-uniform
+    const long round_limit = 4L * (long)w.F + 1024;
+    long rounds = 0, taken = 0;
+    *unfinished = false;
+    __syncwarp();
+    while (sp > 0) {
+        if (++rounds > round_limit) {  // a corrupt hierarchy: report, do not loop
+            *overflow = 1;
+            break;
+        }
+        const int take = sp < 32 ? sp : 32;
+        sp -= take;
+        taken += take;
+        uint32_t node = 0;
+        bool live = false;
+        if (lane < take) {
+            node = nodes[sp + lane];
+            live = dists[sp + lane] < bound;
+        }
+        __syncwarp();
+        // leaves: FP64 distance, then the warp's winner under the exact rule
+        double d = 1e300;
+        int tri = 0x7fffffff;
+        if (live && (node & kLeafBit)) {
+            int t;
+            const double x = leaf_distance(w, (int)(node & ~kLeafBit), q64, &t);
+            if (t != seed) {
+                d = x;
+                tri = t;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double od = __shfl_xor_sync(0xffffffffu, d, o);
+            const int ot = __shfl_xor_sync(0xffffffffu, tri, o);
+            if (od < d || (od == d && ot < tri)) {
+                d = od;
+                tri = ot;
+            }
+        }
+        if (d < best || (d == best && tri < best_tri)) {
+            best = d;
+            best_tri = tri;
+            const double r = sqrt(best) + slack;
+            bound = __double2float_ru(r * r);
+        }
+        // internal nodes: the children that can still hold something closer,
+        // the nearer one pushed last (taken first)
+        uint32_t push[2] = {0, 0};
+        float push_d[2] = {0.0f, 0.0f};
+        int pushes = 0;
+        if (live && !(node & kLeafBit)) {
+            const float4* nd = w.bvh_nodes + (long)node * 4;
+            const float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+            const float dl = box_distance(q, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
+            const float dr = box_distance(q, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
+            const uint32_t cl = __float_as_uint(n3.x), cr = __float_as_uint(n3.y);
+            const bool hl = dl < bound, hr = dr < bound;
+            const bool left_first = dl <= dr;
+            if (hl && hr) {
+                push[0] = left_first ? cr : cl;
+                push_d[0] = left_first ? dr : dl;
+                push[1] = left_first ? cl : cr;
+                push_d[1] = left_first ? dl : dr;
+                pushes = 2;
+            } else if (hl || hr) {
+                push[0] = hl ? cl : cr;
+                push_d[0] = hl ? dl : dr;
+                pushes = 1;
+            }
+        }
+        int at = pushes;  // inclusive prefix over the lanes, then exclusive
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, at, o);
+            if (lane >= o) at += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, at, 31);
+        at -= pushes;
+        if (sp + total > kWarpStack) {  // the rest by one lane, from the winner so far
+            *unfinished = true;
+            break;
+        }
+        for (int k = 0; k < pushes; ++k) {
+            nodes[sp + at + k] = push[k];
+            dists[sp + at + k] = push_d[k];
+        }
+        sp += total;
+        __syncwarp();
+    }
+    *work = taken;
     return best_tri;
 }
 
@@ -732,52 +860,41 @@ __device__ inline bool queries(int phase) {
     return phase == kPhaseTransfer || phase == kPhaseRefresh || phase == kPhaseFinal;
 }
 
-// The correspondence of template vertex v, with the filters in the order the
-// reference applies them (correspondence.cpp:35-80) and the reweighting of
-// route_a.cpp:19-38.
-__device__ void query_vertex(const WrapDev& w, int level, int v) {
+// The correspondence of template vertex v to triangle `tri` (-1: none), with
+// the filters in the order the reference applies them
+// (correspondence.cpp:35-80) and the reweighting of route_a.cpp:19-38.
+__device__ void store_correspondence(const WrapDev& w, int level, int v, int tri) {
     uint8_t code = 0;
     D3 point = {0, 0, 0}, normal = {0, 0, 0};
     double distance = 0.0, robust = 1.0;
-    int tri = -1;
-    if (w.mask && !w.mask[v]) {
-        code = 4;
-        tri = w.corr_triangle[v];
-    } else {
-        const float4 q32 = w.deformed32[v];
-        int overflow = 0;
-        tri = nearest_triangle(w, {q32.x, q32.y, q32.z}, load_d3(w.deformed, v), w.corr_triangle[v],
-                               &overflow);
-        if (overflow) atomicOr(&w.control->error, 1);
-        if (tri >= 0) {
-            const D3 q = load_d3(w.deformed, v);
-            const int32_t* f = w.tgt_faces + (long)tri * 3;
-            double bary[3];
-            point = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
-                                       load_d3(w.tgt_points, f[2]), bary);
-            const D3 d = vsub(point, q);
-            distance = __dsqrt_rn(vdot(d, d));
-            const D3 n0 = load_d3(w.tgt_normals, f[0]), n1 = load_d3(w.tgt_normals, f[1]),
-                     n2 = load_d3(w.tgt_normals, f[2]);
-            normal = vnormalized(vadd(vadd(vmul(n0, bary[0]), vmul(n1, bary[1])), vmul(n2, bary[2])));
-            if (distance > w.distance_threshold) {
-                code = 1;
-            } else if (vdot(load_d3(w.qnormals, v), normal) < w.min_normal_cosine) {
-                code = 2;
-            } else if (distance > 0.0) {
-                const D3 offset = vsub(q, point);
-                const double slope = __ddiv_rn(fabs(vdot(normal, offset)), distance);
-                if (slope < w.min_slope) code = 3;
-            }
-            if (code == 0) {
-                const D3 o = vsub(q, point);
-                const double squared = vdot(o, o);
-                const double threshold = w.robust_threshold[level];
-                robust = threshold > 0.0 ? robust_weight(w.robust_kernel[level], squared, threshold) : 1.0;
-            }
-        } else {
+    if (tri >= 0) {
+        const D3 q = load_d3(w.deformed, v);
+        const int32_t* f = w.tgt_faces + (long)tri * 3;
+        double bary[3];
+        point = closest_point_fp64(q, load_d3(w.tgt_points, f[0]), load_d3(w.tgt_points, f[1]),
+                                   load_d3(w.tgt_points, f[2]), bary);
+        const D3 d = vsub(point, q);
+        distance = __dsqrt_rn(vdot(d, d));
+        const D3 n0 = load_d3(w.tgt_normals, f[0]), n1 = load_d3(w.tgt_normals, f[1]),
+                 n2 = load_d3(w.tgt_normals, f[2]);
+        normal = vnormalized(vadd(vadd(vmul(n0, bary[0]), vmul(n1, bary[1])), vmul(n2, bary[2])));
+        if (distance > w.distance_threshold) {
             code = 1;
+        } else if (vdot(load_d3(w.qnormals, v), normal) < w.min_normal_cosine) {
+            code = 2;
+        } else if (distance > 0.0) {
+            const D3 offset = vsub(q, point);
+            const double slope = __ddiv_rn(fabs(vdot(normal, offset)), distance);
+            if (slope < w.min_slope) code = 3;
         }
+        if (code == 0) {
+            const D3 o = vsub(q, point);
+            const double squared = vdot(o, o);
+            const double threshold = w.robust_threshold[level];
+            robust = threshold > 0.0 ? robust_weight(w.robust_kernel[level], squared, threshold) : 1.0;
+        }
+    } else {
+        code = 1;
     }
     store_d3(w.corr_point, v, point);
     store_d3(w.corr_normal, v, normal);
@@ -785,6 +902,29 @@ __device__ void query_vertex(const WrapDev& w, int level, int v) {
     w.corr_triangle[v] = tri;
     w.corr_code[v] = code;
     w.robust[v] = robust;
+}
+
+// A masked vertex keeps its previous triangle and takes no correspondence.
+__device__ inline void store_masked(const WrapDev& w, int v) {
+    store_d3(w.corr_point, v, {0, 0, 0});
+    store_d3(w.corr_normal, v, {0, 0, 0});
+    w.corr_distance[v] = 0.0;
+    w.corr_code[v] = 4;
+    w.robust[v] = 1.0;
+}
+
+// The correspondence of template vertex v, found by one thread.
+__device__ void query_vertex(const WrapDev& w, int level, int v) {
+    if (w.mask && !w.mask[v]) {
+        store_masked(w, v);
+        return;
+    }
+    const float4 q32 = w.deformed32[v];
+    int overflow = 0;
+    const int tri = nearest_triangle(w, {q32.x, q32.y, q32.z}, load_d3(w.deformed, v), w.corr_triangle[v],
+                                     &overflow);
+    if (overflow) atomicOr(&w.control->error, 1);
+    store_correspondence(w, level, v, tri);
 }
 
 // Thread per vertex, block row per wrap.
@@ -797,34 +937,101 @@ __global__ void k_query(const WrapDev* __restrict__ wraps) {
     query_vertex(w, c.level, v);
 }
 
-// The same work as one queue: the vertices of every querying wrap, in wrap
-// then vertex order, handed out 32 at a time to whichever warp is free.  A
-// walk's length varies a lot from vertex to vertex, so fixed blocks hold an
-// SM until their slowest warp ends; here a warp that ends takes the next 32.
-// The grid is what fits on the device at once; `counter` starts at 0.
+// Puts vertex v on the wrap's list of long walks for its next query (list
+// 1 - long_cur), unless the list is full.
+__device__ inline void list_long_walk(const WrapDev& w, int next, int v) {
+    const int at = atomicAdd(w.long_count + next, 1);
+    if (at < kLongCap) {
+        w.long_list[next * kLongCap + at] = v;
+        w.long_flag[(long)next * w.V + v] = 1;
+    }
+}
+
+// The same work as queues over a grid that fits on the device at once.
+// First, the vertices whose walk was long at the wrap's previous query (its
+// list), a warp each.  Then every other vertex of every querying wrap, in
+// wrap then vertex order, handed out 32 at a time to whichever warp is free
+// (a walk's length varies a lot from vertex to vertex, so fixed blocks would
+// hold an SM until their slowest warp ends).  A launch lasts as long as its
+// longest walks: the warps take those at its start, in tens of dependent
+// rounds, beside the threads' walks instead of after them.  A walk longer
+// than kLongWalk steps lists its vertex for the wrap's next query.
+// counter[0]: the vertices' queue head; counter[1]: the long walks'; both
+// start at 0.
 __global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__ wraps, int wrap_count,
                                                     int* __restrict__ counter) {
-    extern __shared__ int first[];  // wrap_count + 1: each querying wrap's first item
-    for (int i = threadIdx.x; i < wrap_count; i += blockDim.x)
-        first[i + 1] = queries(wraps[i].control->tick_phase) ? wraps[i].V : 0;
-    __syncthreads();
-    if (threadIdx.x < 32) {  // inclusive scan by warp 0, 32 wraps at a time
-        const int lane = threadIdx.x;
-        int carry = 0;
-        for (int base = 0; base < wrap_count; base += 32) {
-            int x = base + lane < wrap_count ? first[base + lane + 1] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (base + lane < wrap_count) first[base + lane + 1] = carry + x;
-            carry += __shfl_sync(0xffffffffu, x, 31);
-        }
-        if (lane == 0) first[0] = 0;
+    extern __shared__ float4 query_shared[];  // 4 warps' stacks, then 2 x (wrap_count + 1) ints
+    uint32_t* stack_nodes = reinterpret_cast<uint32_t*>(query_shared);
+    float* stack_dists = reinterpret_cast<float*>(stack_nodes + 4 * kWarpStack);
+    int* first = reinterpret_cast<int*>(stack_dists + 4 * kWarpStack);  // each wrap's first vertex item
+    int* first_long = first + wrap_count + 1;                             // and first long-walk item
+    for (int i = threadIdx.x; i < wrap_count; i += blockDim.x) {
+        const WrapDev& w = wraps[i];
+        const bool on = queries(w.control->tick_phase);
+        first[i + 1] = on ? w.V : 0;
+        first_long[i + 1] = on ? min(w.long_count[w.control->long_cur], kLongCap) : 0;
     }
     __syncthreads();
-    const int total = first[wrap_count];
+    if (threadIdx.x < 32) {  // inclusive scans by warp 0, 32 wraps at a time
+        const int lane = threadIdx.x;
+        for (int k = 0; k < 2; ++k) {
+            int* f = k == 0 ? first : first_long;
+            int carry = 0;
+            for (int base = 0; base < wrap_count; base += 32) {
+                int x = base + lane < wrap_count ? f[base + lane + 1] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (base + lane < wrap_count) f[base + lane + 1] = carry + x;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) f[0] = 0;
+        }
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
+    auto wrap_of = [&](const int* f, int item) {  // the last wrap whose first item is <= item
+        int lo = 0, hi = wrap_count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (f[mid] <= item) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    };
+    // ---- the listed long walks, a warp each ----
+    {
+        const int total = first_long[wrap_count];
+        uint32_t* nodes = stack_nodes + (threadIdx.x >> 5) * kWarpStack;
+        float* dists = stack_dists + (threadIdx.x >> 5) * kWarpStack;
+        while (true) {
+            int item = 0;
+            if (lane == 0) item = atomicAdd(counter + 1, 1);
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if (item >= total) break;
+            const int wi = wrap_of(first_long, item);
+            const WrapDev& w = wraps[wi];
+            const int cur = w.control->long_cur;
+            const int v = w.long_list[cur * kLongCap + item - first_long[wi]];
+            const float4 q32 = w.deformed32[v];
+            const F3 q = {q32.x, q32.y, q32.z};
+            const D3 q64 = load_d3(w.deformed, v);
+            int overflow = 0;
+            bool unfinished = false;
+            long work = 0;
+            int tri = nearest_triangle_warp(w, q, q64, w.corr_triangle[v], nodes, dists, &overflow,
+                                            &unfinished, &work);
+            if (lane == 0) {
+                if (unfinished) tri = nearest_triangle(w, q, q64, tri, &overflow);
+                if (overflow) atomicOr(&w.control->error, 1);
+                store_correspondence(w, w.control->level, v, tri);
+                if (unfinished || work > kLongWalk) list_long_walk(w, 1 - cur, v);
+            }
+            __syncwarp();
+        }
+    }
+    // ---- every other vertex, a thread each ----
+    const int total = first[wrap_count];
     while (true) {
         int base = 0;
         if (lane == 0) base = atomicAdd(counter, 32);
@@ -832,13 +1039,23 @@ __global__ void __launch_bounds__(128) k_query_queue(const WrapDev* __restrict__
         if (base >= total) break;
         const int item = base + lane;
         if (item >= total) continue;
-        int lo = 0, hi = wrap_count - 1;  // the last wrap whose first item is <= item
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (first[mid] <= item) lo = mid; else hi = mid - 1;
+        const int wi = wrap_of(first, item);
+        const WrapDev& w = wraps[wi];
+        const int v = item - first[wi];
+        if (w.mask && !w.mask[v]) {
+            store_masked(w, v);
+            continue;
         }
-        const WrapDev& w = wraps[lo];
-        query_vertex(w, w.control->level, item - first[lo]);
+        const int cur = w.control->long_cur;
+        if (w.long_flag[(long)cur * w.V + v]) continue;  // a warp's walk, above
+        const float4 q32 = w.deformed32[v];
+        int overflow = 0;
+        long steps = 0;
+        const int tri = nearest_triangle(w, {q32.x, q32.y, q32.z}, load_d3(w.deformed, v),
+                                         w.corr_triangle[v], &overflow, &steps);
+        if (overflow) atomicOr(&w.control->error, 1);
+        store_correspondence(w, w.control->level, v, tri);
+        if (steps > kLongWalk) list_long_walk(w, 1 - cur, v);
     }
 }
 
@@ -881,16 +1098,20 @@ void launch_query(const WrapDev* wraps, int wrap_count, int max_vertices, cudaSt
         k_query<<<grid, 128, 0, stream>>>(wraps);
         return;
     }
+    // the warps' stacks, then two scans over the wraps (1024 at most)
+    constexpr size_t kStackBytes = (sizeof(uint32_t) + sizeof(float)) * kWarpStack * 4;
     static const int resident = [] {  // blocks of the queue that fit on the device at once
         int device = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_queue, 128, sizeof(int) * 1025);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_query_queue, 128,
+                                                      kStackBytes + 2 * sizeof(int) * 1025);
         const int blocks = sms * (per_sm > 0 ? per_sm : 1);
         return blocks > 0 ? blocks : 1;
     }();
-    cudaMemsetAsync(counter, 0, sizeof(int), stream);
-    k_query_queue<<<resident, 128, sizeof(int) * (wrap_count + 1), stream>>>(wraps, wrap_count, counter);
+    cudaMemsetAsync(counter, 0, 2 * sizeof(int), stream);
+    k_query_queue<<<resident, 128, kStackBytes + 2 * sizeof(int) * (wrap_count + 1), stream>>>(
+        wraps, wrap_count, counter);
 }
 
 void launch_closest_points(const WrapDev* wrap, const double* queries, int count,

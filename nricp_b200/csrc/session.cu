@@ -325,6 +325,9 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_cn = a.reserve(sizeof(double) * 3 * V);
     const size_t o_cd = a.reserve(sizeof(double) * V);
     const size_t o_ct = a.reserve(sizeof(int32_t) * V);
+    const size_t o_ll = a.reserve(sizeof(int32_t) * 2 * kLongCap);
+    const size_t o_lc = a.reserve(sizeof(int32_t) * 2);
+    const size_t o_lf = a.reserve(2 * static_cast<size_t>(V));
     const size_t o_cc = a.reserve(V);
     const size_t o_rb = a.reserve(sizeof(double) * V);
     const size_t o_r0 = a.reserve(sizeof(float4) * V);
@@ -501,6 +504,9 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.corr_normal = a.at<double>(o_cn);
     D.corr_distance = a.at<double>(o_cd);
     D.corr_triangle = a.at<int32_t>(o_ct);
+    D.long_list = a.at<int32_t>(o_ll);
+    D.long_count = a.at<int32_t>(o_lc);
+    D.long_flag = a.at<uint8_t>(o_lf);
     D.corr_code = a.at<uint8_t>(o_cc);
     D.robust = a.at<double>(o_rb);
     D.residual32 = a.at<float4>(o_r0);
@@ -535,6 +541,8 @@ void reset_device(Wrap& w, cudaStream_t stream, void* lbvh_scratch, LbvhExport* 
           "init rot");
     check(cudaMemsetAsync(D.trans[0], 0, sizeof(double) * 3 * N, stream), "init trans");
     check(cudaMemsetAsync(D.corr_triangle, 0xff, sizeof(int32_t) * V, stream), "init corr");
+    check(cudaMemsetAsync(D.long_count, 0, sizeof(int32_t) * 2, stream), "init long walks");
+    check(cudaMemsetAsync(D.long_flag, 0, 2 * static_cast<size_t>(V), stream), "init long walks");
     check(cudaMemsetAsync(D.corr_code, 0, V, stream), "init code");
     check(cudaMemcpyAsync(D.records, w.initial_records, sizeof(LevelRecord) * w.levels,
                           cudaMemcpyDeviceToDevice, stream), "init records");
@@ -752,7 +760,7 @@ void Batch::upload_all(LbvhExport* lbvh_out) {
         if (!failure[i].empty()) throw std::runtime_error(failure[i]);
     shape_ = TickShape{};
     shape_.wraps = W;
-    check(cudaMalloc(&query_counter_, sizeof(int)), "cudaMalloc(query queue)");
+    check(cudaMalloc(&query_counter_, 2 * sizeof(int)), "cudaMalloc(query queues)");
     shape_.query_counter = query_counter_;
     if (!side_stream_) {
         check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "stream");
@@ -1334,7 +1342,7 @@ struct Server::Impl {
     long submitted = 0, completed = 0, failed = 0, ticks = 0, launches = 0, captures = 0;
     double busy_seconds = 0.0;
     cudaEvent_t tick_begin = nullptr, tick_end = nullptr;
-    int* query_counter = nullptr;        // the query queue's next item
+    int* query_counter = nullptr;        // the query queues' heads (vertices, long walks)
     std::vector<double> latencies, queue_waits;
     double first_submit = -1.0, last_done = 0.0;
 
@@ -1832,7 +1840,7 @@ Server::Server(const NricpServerConfig& config) : impl_(std::make_unique<Impl>()
     }
     check(cudaMalloc(&m.staging_controls, sizeof(WrapControl) * Impl::kLoaders), "cudaMalloc(staging control)");
     check(cudaEventCreate(&m.tick_begin), "event");
-    check(cudaMalloc(&m.query_counter, sizeof(int)), "cudaMalloc(query queue)");
+    check(cudaMalloc(&m.query_counter, 2 * sizeof(int)), "cudaMalloc(query queues)");
     m.shape.query_counter = m.query_counter;
     check(cudaStreamCreateWithFlags(&m.shape.side_stream, cudaStreamNonBlocking), "stream");
     check(cudaEventCreateWithFlags(&m.shape.side_fork, cudaEventDisableTiming), "event");

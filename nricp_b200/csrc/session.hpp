@@ -110,7 +110,7 @@ private:
     cudaEvent_t build_fork_ = nullptr, build_done_[kBuildStreams] = {};
     void* build_scratch_[kBuildStreams] = {};
     cudaMemPool_t pool_ = nullptr;  // the arenas' and the scratch's (batch_pool)
-    int* query_counter_ = nullptr;  // the query queue's next item
+    int* query_counter_ = nullptr;  // the query queues' heads (vertices, long walks)
     cudaStream_t side_stream_ = nullptr;  // the tick's refresh branch
     cudaEvent_t side_fork_ = nullptr, side_join_ = nullptr;
     int* pcg_index_ = nullptr;      // wraps ordered by solve class (device)

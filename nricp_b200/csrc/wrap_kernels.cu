@@ -1623,9 +1623,24 @@ __global__ void k_decide(const WrapDev* __restrict__ wraps, int part) {
         }
         __syncthreads();
     }
+    // the long walks this tick's query took from its list are done: clear
+    // their flags and empty the list, which the next query but one fills
+    const bool queried = c0.tick_phase == kPhaseTransfer || c0.tick_phase == kPhaseRefresh ||
+                         c0.tick_phase == kPhaseFinal;
+    if (queried) {
+        const int cur = c0.long_cur;
+        const int taken = min(w.long_count[cur], kLongCap);
+        for (int i = threadIdx.x; i < taken; i += blockDim.x)
+            w.long_flag[(long)cur * w.V + w.long_list[cur * kLongCap + i]] = 0;
+        __syncthreads();
+    }
     if (threadIdx.x != 0) return;
     WrapControl c = c0;
     c.steps += 1;
+    if (queried) {
+        w.long_count[c.long_cur] = 0;
+        c.long_cur ^= 1;
+    }
     const double total = parts_s[0] + parts_s[1] + parts_s[2] + parts_s[3] + parts_s[4];
     LevelRecord& rec = w.records[c.level];
     if (c.phase == kPhaseSolve) {
