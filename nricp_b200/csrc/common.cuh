@@ -19,7 +19,7 @@ constexpr int kMaxSlots = 8;        // binding support (the reference caps at 4)
 constexpr int kMaxLevels = 16;
 constexpr int kEnergyKinds = 5;     // p2p, plane, smoothness, anchor, landmark
 constexpr int kStackDepth = 64;     // LBVH traversal stack
-constexpr int kLongCap = 256;       // long walks a wrap lists for its next query's warps
+constexpr int kLongCap = 2048;      // long walks a wrap lists for its next query's warps
 constexpr int kPartialStride = 8;   // doubles per energy partial record
 
 // Device phases of one wrap.  They mirror the reference session's

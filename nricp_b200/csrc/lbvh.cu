@@ -735,7 +735,7 @@ __device__ int nearest_triangle(const WrapDev& w, F3 q, D3 q64, int seed, int* o
 // its next query, where a warp walks it (a vertex over a hole in the target,
 // or above the fan of slivers at a lat-long pole, stays far from the nearest
 // triangles and walks hundreds to thousands of steps query after query).
-constexpr long kLongWalk = 512;
+constexpr long kLongWalk = 256;
 // A warp's stack: 32 entries for each of 32 levels of pending subtrees.
 constexpr int kWarpStack = 1024;
 
