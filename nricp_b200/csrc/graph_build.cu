@@ -352,10 +352,6 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
     int max_levels = 0, max_points = 0;
     for (int t = 0; t < W; ++t) {
         const GraphRequest& r = requests[t];
-        TemplateGraph& g = out[t];
-        compute_normalization(r.points, r.count, g.center, &g.scale);
-        const std::vector<double> norm = normalized(r.points, r.count, g.center, g.scale);
-        points.insert(points.end(), norm.begin(), norm.end());
         point_offset[t] = total_points;
         point_count[t] = r.count;
         total_points += r.count;
@@ -371,6 +367,16 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
         total_seeds += most;
         max_levels = std::max(max_levels, levels);
         max_points = std::max(max_points, r.count);
+    }
+    // every template normalised on its own host thread, into its place
+    points.resize(static_cast<size_t>(total_points) * 3);
+#pragma omp parallel for schedule(dynamic, 1) if (W > 1)
+    for (int t = 0; t < W; ++t) {
+        const GraphRequest& r = requests[t];
+        TemplateGraph& g = out[t];
+        compute_normalization(r.points, r.count, g.center, &g.scale);
+        const std::vector<double> norm = normalized(r.points, r.count, g.center, g.scale);
+        std::copy(norm.begin(), norm.end(), points.begin() + point_offset[t] * 3);
     }
     std::vector<void*> owned;
     double* d_points = to_device(points, owned, stream);
@@ -431,7 +437,8 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
 
     // seeds: a cluster of 1-16 CTAs per template (4,096 points per CTA), one
     // launch per cluster size; a single block for templates beyond 65,536
-    // points
+    // points.  The launches touch different templates, so each runs on a
+    // stream of its own, beside the others.
     {
         std::vector<std::vector<int>> by_size(5);
         std::vector<int> single;
@@ -449,13 +456,26 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
             return true;
         }();
         (void)enabled;
+        const int* d_group[5] = {};
+        for (int g = 0; g < 5; ++g)
+            if (!by_size[g].empty()) d_group[g] = to_device(by_size[g], owned, stream);
+        const int* d_single = single.empty() ? nullptr : to_device(single, owned, stream);
+        cudaStream_t lanes[6] = {};
+        cudaEvent_t fork = nullptr, join[6] = {};
+        check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+        check(cudaEventRecord(fork, stream), "event");
+        for (int k = 0; k < 6; ++k) {
+            check(cudaStreamCreateWithFlags(&lanes[k], cudaStreamNonBlocking), "stream");
+            check(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming), "event");
+            check(cudaStreamWaitEvent(lanes[k], fork, 0), "wait");
+        }
         for (int g = 0; g < 5; ++g) {
             if (by_size[g].empty()) continue;
-            const int* d_templates = to_device(by_size[g], owned, stream);
+            const int* d_templates = d_group[g];
             cudaLaunchConfig_t config = {};
             config.gridDim = dim3(1 << g, static_cast<unsigned>(by_size[g].size()));
             config.blockDim = dim3(kFpsClusterThreads);
-            config.stream = stream;
+            config.stream = lanes[g];
             cudaLaunchAttribute attribute[1];
             attribute[0].id = cudaLaunchAttributeClusterDimension;
             attribute[0].val.clusterDim.x = 1 << g;
@@ -469,11 +489,19 @@ std::vector<TemplateGraph> device_template_graphs(const std::vector<GraphRequest
                   "farthest-point seeds");
         }
         if (!single.empty()) {
-            const int* d_templates = to_device(single, owned, stream);
-            k_fps<<<static_cast<int>(single.size()), kFpsThreads, 0, stream>>>(
-                d_points, d_point_offset, d_point_count, d_seed_count, d_seed_offset, d_templates, d_nearest,
+            k_fps<<<static_cast<int>(single.size()), kFpsThreads, 0, lanes[5]>>>(
+                d_points, d_point_offset, d_point_count, d_seed_count, d_seed_offset, d_single, d_nearest,
                 d_seeds);
         }
+        for (int k = 0; k < 6; ++k) {
+            check(cudaEventRecord(join[k], lanes[k]), "event");
+            check(cudaStreamWaitEvent(stream, join[k], 0), "wait");
+        }
+        for (int k = 0; k < 6; ++k) {
+            cudaStreamDestroy(lanes[k]);  // released once its work is done
+            cudaEventDestroy(join[k]);
+        }
+        cudaEventDestroy(fork);
     }
     check(cudaGetLastError(), "farthest-point seeds");
     check(cudaMemcpyAsync(seeds, d_seeds, sizeof(int) * std::max<long>(1, total_seeds), cudaMemcpyDeviceToHost,
