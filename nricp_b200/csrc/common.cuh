@@ -194,7 +194,7 @@ struct WrapDev {
     // reductions
     double* partials;             // energy_blocks x kPartialStride
     double* edge_partials;        // edge blocks x 1 (smoothness energy)
-    double* node_partials;        // node blocks x 1 (anchor energy)
+    double* node_partials;        // N: each node's anchor energy (the decision kernel sums them)
     int* counts;                  // stats scratch
     // report
     LevelRecord* records;         // level_count

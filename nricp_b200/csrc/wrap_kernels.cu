@@ -1408,13 +1408,13 @@ __device__ __forceinline__ void k_node_assemble_body(const WrapDev& w, int part,
             }
         }
     }
-    __shared__ double scratch[33];
-    const double total = block_sum<kNodeThreads>(e_anchor, scratch);
-    if (threadIdx.x == 0) w.node_partials[bx] = total;
+    // the node's anchor energy; the decision kernel sums them as a block sum
+    // over this block's warps would (no block barrier here)
+    if (lane == 0 && node < L.node_count) w.node_partials[node] = e_anchor;
 }
 
 __global__ void __launch_bounds__(kNodeThreads, 3) k_node_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks<true>(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1612,7 +1612,18 @@ __global__ void k_decide(const WrapDev* __restrict__ wraps, int part) {
             s4 += w.partials[(long)i * kPartialStride + 2];
         }
         for (int i = threadIdx.x; i < eb; i += blockDim.x) s2 += w.edge_partials[i];
-        for (int i = threadIdx.x; i < nb; i += blockDim.x) s3 += w.node_partials[i];
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+            // node block i's anchor energy, summed in the order of a block sum
+            // over its 8 warps (lane 0 of warp j holds node 8i + j; the other
+            // lanes add zeros, which change nothing)
+            static_assert(kNodeThreads == 8 * 32, "eight nodes per node block");
+            double v[8];
+            for (int j = 0; j < 8; ++j) {
+                const int n = i * 8 + j;
+                v[j] = n < L.node_count ? w.node_partials[n] : 0.0;
+            }
+            s3 += ((v[0] + v[4]) + (v[2] + v[6])) + ((v[1] + v[5]) + (v[3] + v[7]));
+        }
         const double t0 = block_sum<256>(s0, scratch);
         const double t1 = block_sum<256>(s1, scratch);
         const double t2 = block_sum<256>(s2, scratch);
