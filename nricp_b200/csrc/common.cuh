@@ -176,6 +176,8 @@ struct WrapDev {
     float4* residual32;           // V: (o.x, o.y, o.z, plane value scale) per vertex
     float4* resid_aux32;          // V: (n.x, n.y, n.z, p2p scale)
     float4* lm_resid32;           // V: landmark offset (xyz), w
+    float4* offsets32;            // V x kMaxSlots: each binding's node-local offset R (p - g), FP32,
+                                  // for the tick's assembly (xyz, unused)
     // systems: two buffers, `control.system` selects the current one
     float* diag[2];               // N x 36
     float* rhs[2];                // N x 6

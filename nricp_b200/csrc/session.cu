@@ -333,6 +333,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_r0 = a.reserve(sizeof(float4) * V);
     const size_t o_r1 = a.reserve(sizeof(float4) * V);
     const size_t o_r2 = a.reserve(sizeof(float4) * V);
+    const size_t o_off32 = a.reserve(sizeof(float4) * kMaxSlots * V);
     const size_t o_factor = a.reserve(sizeof(float) * 36 * N);
     const size_t o_delta = a.reserve(sizeof(double) * 6 * N);
     const size_t o_x = a.reserve(sizeof(double) * 6 * N);
@@ -512,6 +513,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     D.residual32 = a.at<float4>(o_r0);
     D.resid_aux32 = a.at<float4>(o_r1);
     D.lm_resid32 = a.at<float4>(o_r2);
+    D.offsets32 = a.at<float4>(o_off32);
     D.factor = a.at<float>(o_factor);
     D.delta = a.at<double>(o_delta);
     D.pcg_x = a.at<double>(o_x);

@@ -1201,6 +1201,12 @@ __global__ void k_normals(const WrapDev* __restrict__ wraps, int wrap_count, int
 // per-vertex residuals, the data and landmark energies (FP64), and the FP32
 // residual records the assembly reads (fused_assembly.cpp:185-216, 262-280)
 // ---------------------------------------------------------------------------
+// The node-local offset R (p_v - g_node) of vertex v bound to `node`, FP32.
+__device__ inline F3 node_offset32(const WrapDev& w, const LevelDev& L, int node, int v) {
+    const D3 p = load_d3(w.tpl, v) - load_d3(L.rest, node);
+    return mul3f(w.rot32 + node * 9, {(float)p.x, (float)p.y, (float)p.z});
+}
+
 __device__ __forceinline__ void k_residual_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
     if (!in_part(c, part)) return;
@@ -1244,6 +1250,14 @@ __device__ __forceinline__ void k_residual_body(const WrapDev& w, int part, int 
         w.residual32[v] = r0;
         w.resid_aux32[v] = r1;
         w.lm_resid32[v] = r2;
+        // each binding's offset, once for the node and pair assembly that follow
+        if (bound && assembles(c))
+            for (int k = 0; k < L.bind_counts[v]; ++k) {
+                const int node = L.bind_nodes[v * kMaxSlots + k];
+                if (node < 0) continue;
+                const F3 a = node_offset32(w, L, node, v);
+                w.offsets32[v * kMaxSlots + k] = make_float4(a.x, a.y, a.z, 0.0f);
+            }
     }
     __shared__ double scratch[33];
     const double s0 = block_sum<kVertexThreads>(e_p2p, scratch);
@@ -1272,10 +1286,6 @@ __global__ void __launch_bounds__(kVertexThreads) k_residual(const WrapDev* __re
 // the smoothness blocks.  Closed forms of sum_rows J^T J for an offset
 // residual replace the reference's row-by-row outer products.
 // ---------------------------------------------------------------------------
-__device__ inline F3 node_offset32(const WrapDev& w, const LevelDev& L, int node, int v) {
-    const D3 p = load_d3(w.tpl, v) - load_d3(L.rest, node);
-    return mul3f(w.rot32 + node * 9, {(float)p.x, (float)p.y, (float)p.z});
-}
 
 __device__ __forceinline__ void k_node_assemble_body(const WrapDev& w, int part, int bx) {
     const WrapControl c = *w.control;
@@ -1299,7 +1309,8 @@ __device__ __forceinline__ void k_node_assemble_body(const WrapDev& w, int part,
                 const int entry = L.gather_entry[i];
                 const int v = entry / kMaxSlots;
                 const float wgt = (float)L.bind_weights[entry];
-                const F3 a = node_offset32(w, L, node, v);
+                const float4 a4 = w.offsets32[entry];
+                const F3 a = {a4.x, a4.y, a4.z};
                 const float4 r0 = w.residual32[v];
                 const float4 r1 = w.resid_aux32[v];
                 const float4 r2 = w.lm_resid32[v];
@@ -1457,7 +1468,6 @@ __device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part,
     const int p = (bx * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (p >= L.pair_count) return;
-    const int na = L.pair_nodes[p * 2], nb = L.pair_nodes[p * 2 + 1];
     float blk[36];
     for (int i = 0; i < 36; ++i) blk[i] = 0.0f;
     for (int i = L.pair_begin[p] + lane; i < L.pair_begin[p + 1]; i += 32) {
@@ -1465,8 +1475,9 @@ __device__ __forceinline__ void k_pair_assemble_body(const WrapDev& w, int part,
         const int v = code >> 6, sa = (code >> 3) & 7, sb = code & 7;
         const float wa = (float)L.bind_weights[v * kMaxSlots + sa];
         const float wb = (float)L.bind_weights[v * kMaxSlots + sb];
-        const F3 aa = node_offset32(w, L, na, v);
-        const F3 ab = node_offset32(w, L, nb, v);
+        const float4 a4 = w.offsets32[v * kMaxSlots + sa], b4 = w.offsets32[v * kMaxSlots + sb];
+        const F3 aa = {a4.x, a4.y, a4.z};
+        const F3 ab = {b4.x, b4.y, b4.z};
         const float4 r0 = w.residual32[v], r1 = w.resid_aux32[v], r2 = w.lm_resid32[v];
         const float coef = (r0.w + r2.w) * wa * wb;  // p2p and landmark share the form
         if (coef > 0.0f) {
