@@ -599,6 +599,8 @@ Batch::Batch() {
 
 Batch::~Batch() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (tail_graph_) cudaGraphExecDestroy(tail_graph_);
+    if (tail_index_) cudaFree(tail_index_);
     if (stream_) cudaStreamSynchronize(stream_);
     if (pool_) {  // back to the pool in stream order, without a device-wide wait
         for (auto& w : wraps_) w->arena.release_async(stream_);
@@ -824,10 +826,11 @@ void Batch::reset() {
 }
 
 void Batch::tick(KernelTimers* timers) {
-    launch_tick(dev_wraps_, shape_, stream_, timers);
+    const TickShape& shape = tail_on_ ? tail_shape_ : shape_;
+    launch_tick(dev_wraps_, shape, stream_, timers);
     check(cudaGetLastError(), "tick launch");
     ticks_ += 1;
-    launches_ += tick_kernel_launches(shape_, timers && timers->active);
+    launches_ += tick_kernel_launches(shape, timers && timers->active);
 }
 
 void Batch::pull_controls() {
@@ -860,23 +863,35 @@ int Batch::default_pcg_cluster() const {
 }
 
 void Batch::set_pcg_cluster(int cluster) {
-    int device = 0, sms = 148;
+    int device = 0;
     check(cudaGetDevice(&device), "device");
-    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device");
+    check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device), "device");
+    pcg_cluster_size(shape_.max_nodes, static_cast<int>(wraps_.size()), sms_);  // enables the launch attributes
+    for (cudaGraphExec_t* g : {&graph_exec_, &tail_graph_})
+        if (*g) {
+            cudaGraphExecDestroy(*g);
+            *g = nullptr;
+        }
+    tail_ready_ = tail_on_ = false;
+    solve_shape(cluster, shape_, pcg_index_, nullptr);
+    if (cluster < 0) {  // halved classes: halved once less for the tail
+        tail_shape_ = shape_;
+        solve_shape(cluster + 1, tail_shape_, tail_index_, &tail_cls_);
+        tail_ready_ = true;
+    }
+}
+
+void Batch::solve_shape(int cluster, TickShape& shape, int*& index, std::vector<int>* cls_out) {
     const int W = static_cast<int>(wraps_.size());
     std::vector<int> nodes(W);
     for (int i = 0; i < W; ++i) nodes[i] = wraps_[i]->max_nodes;
-    pcg_cluster_size(shape_.max_nodes, W, sms);  // enables the launch attributes
-    if (graph_exec_) {
-        cudaGraphExecDestroy(graph_exec_);
-        graph_exec_ = nullptr;
-    }
-    shape_.pcg_groups = 0;
+    shape.pcg_groups = 0;
     if (cluster > 0) {
         if (cluster > 16 || (cluster & (cluster - 1)) != 0)
             throw InvalidArgument("the solve's cluster size is a power of two from 1 to 16");
-        shape_.pcg_cluster = cluster;
-        shape_.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), W, cluster);
+        shape.pcg_cluster = cluster;
+        shape.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), W, cluster);
+        if (cls_out) cls_out->assign(W, cluster);
         return;
     }
     if (cluster < -4) throw InvalidArgument("the solve's class shift is 0 to 4");
@@ -884,15 +899,16 @@ void Batch::set_pcg_cluster(int cluster) {
     const int shift = -cluster;
     std::vector<int> cls(W);
     for (int i = 0; i < W; ++i) cls[i] = std::max(1, pcg_latency_cluster(nodes[i]) >> shift);
+    if (cls_out) *cls_out = cls;
     std::vector<int> sizes;
     for (int c = 16; c >= 1; c /= 2)
         if (std::count(cls.begin(), cls.end(), c) > 0) sizes.push_back(c);
     if (sizes.size() == 1) {
-        shape_.pcg_cluster = sizes[0];
-        shape_.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), W, sizes[0]);
+        shape.pcg_cluster = sizes[0];
+        shape.pcg_shared_bytes = pcg_shared_bytes(nodes.data(), W, sizes[0]);
         return;
     }
-    if (!pcg_index_) check(cudaMalloc(&pcg_index_, sizeof(int) * W), "cudaMalloc(solve groups)");
+    if (!index) check(cudaMalloc(&index, sizeof(int) * W), "cudaMalloc(solve groups)");
     std::vector<int> order;
     for (size_t g = 0; g < sizes.size(); ++g) {
         const int first = static_cast<int>(order.size());
@@ -902,46 +918,63 @@ void Batch::set_pcg_cluster(int cluster) {
         std::vector<int> member_nodes;
         for (int i : members) member_nodes.push_back(nodes[i]);
         order.insert(order.end(), members.begin(), members.end());
-        shape_.pcg_group_cluster[g] = sizes[g];
-        shape_.pcg_group_count[g] = static_cast<int>(members.size());
-        shape_.pcg_group_shared[g] = pcg_shared_bytes(member_nodes.data(), (int)members.size(), sizes[g]);
-        shape_.pcg_group_index[g] = pcg_index_ + first;
+        shape.pcg_group_cluster[g] = sizes[g];
+        shape.pcg_group_count[g] = static_cast<int>(members.size());
+        shape.pcg_group_shared[g] = pcg_shared_bytes(member_nodes.data(), (int)members.size(), sizes[g]);
+        shape.pcg_group_index[g] = index + first;
         if (g > 0 && !pcg_streams_[g]) {
             check(cudaStreamCreateWithFlags(&pcg_streams_[g], cudaStreamNonBlocking), "stream");
             check(cudaEventCreateWithFlags(&pcg_join_[g], cudaEventDisableTiming), "event");
         }
-        shape_.pcg_streams[g] = pcg_streams_[g];
-        shape_.pcg_join[g] = pcg_join_[g];
+        shape.pcg_streams[g] = pcg_streams_[g];
+        shape.pcg_join[g] = pcg_join_[g];
     }
     if (!pcg_fork_) check(cudaEventCreateWithFlags(&pcg_fork_, cudaEventDisableTiming), "event");
-    shape_.pcg_fork = pcg_fork_;
-    check(cudaMemcpy(pcg_index_, order.data(), sizeof(int) * W, cudaMemcpyHostToDevice), "solve groups");
-    shape_.pcg_groups = static_cast<int>(sizes.size());
-    shape_.pcg_cluster = sizes[0];
-    shape_.pcg_shared_bytes = shape_.pcg_group_shared[0];
+    shape.pcg_fork = pcg_fork_;
+    check(cudaMemcpy(index, order.data(), sizeof(int) * W, cudaMemcpyHostToDevice), "solve groups");
+    shape.pcg_groups = static_cast<int>(sizes.size());
+    shape.pcg_cluster = sizes[0];
+    shape.pcg_shared_bytes = shape.pcg_group_shared[0];
+}
+
+bool Batch::tail_due() const {
+    long ctas = 0;
+    for (size_t i = 0; i < wraps_.size(); ++i)
+        if (host_controls_[i].phase != kPhaseDone) ctas += tail_cls_[i];
+    return ctas <= sms_;
+}
+
+cudaGraphExec_t Batch::capture(const TickShape& shape) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+    launch_tick(dev_wraps_, shape, stream_, nullptr);
+    check(cudaStreamEndCapture(stream_, &graph), "capture end");
+    check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    return exec;
 }
 
 void Batch::run(int max_ticks) {
-    if (!graph_exec_) {
-        cudaGraph_t graph = nullptr;
-        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
-        launch_tick(dev_wraps_, shape_, stream_, nullptr);
-        check(cudaStreamEndCapture(stream_, &graph), "capture end");
-        check(cudaGraphInstantiate(&graph_exec_, graph, 0), "graph instantiate");
-        cudaGraphDestroy(graph);
-    }
+    if (!graph_exec_) graph_exec_ = capture(shape_);
     pull_controls();
+    tail_on_ = false;
     int chunk = 4;
     while (!all_done()) {
         if (ticks_ >= max_ticks) throw StateError("the schedule did not finish within the tick limit");
+        if (!tail_on_ && tail_ready_ && tail_due()) {
+            tail_on_ = true;
+            if (!tail_graph_) tail_graph_ = capture(tail_shape_);
+        }
         for (int i = 0; i < chunk; ++i) {
-            check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+            check(cudaGraphLaunch(tail_on_ ? tail_graph_ : graph_exec_, stream_), "graph launch");
             ticks_ += 1;
-            launches_ += tick_kernel_launches(shape_);
+            launches_ += tick_kernel_launches(tail_on_ ? tail_shape_ : shape_);
         }
         pull_controls();
         chunk = std::min(chunk * 2, 16);
     }
+    tail_on_ = false;
     finish();
 }
 
@@ -952,8 +985,10 @@ void Batch::run_timed(KernelTimers* timers, std::vector<float>* query_ms, std::v
     check(cudaEventCreate(&tick_begin), "event");
     check(cudaEventCreate(&tick_end), "event");
     pull_controls();
+    tail_on_ = false;
     while (!all_done()) {
         if (ticks_ >= max_ticks) throw StateError("the schedule did not finish within the tick limit");
+        if (!tail_on_ && tail_ready_ && tail_due()) tail_on_ = true;
         TickRecord r{};
         r.phase = host_controls_[0].phase;
         r.level = host_controls_[0].level;
@@ -973,6 +1008,7 @@ void Batch::run_timed(KernelTimers* timers, std::vector<float>* query_ms, std::v
     }
     cudaEventDestroy(tick_begin);
     cudaEventDestroy(tick_end);
+    tail_on_ = false;
     finish();
 }
 

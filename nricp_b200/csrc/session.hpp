@@ -120,6 +120,22 @@ private:
     WrapControl* host_controls_ = nullptr;
     TickShape shape_{};
     cudaGraphExec_t graph_exec_ = nullptr;
+    // Solve launch fields of `shape` for the cluster setting `cluster` (as
+    // set_pcg_cluster takes it), its class lists in `index` (device, made
+    // here when needed); `cls` (if given) receives each wrap's cluster size.
+    void solve_shape(int cluster, TickShape& shape, int*& index, std::vector<int>* cls);
+    cudaGraphExec_t capture(const TickShape& shape);
+    // The batch's tail.  With halved classes, once the wraps still running
+    // would fit on the SMs in one round at one halving less, their ticks run
+    // with that shape: few wraps left, each gets more CTAs.  Results do not
+    // depend on the cluster size.
+    bool tail_due() const;
+    TickShape tail_shape_{};
+    int* tail_index_ = nullptr;
+    std::vector<int> tail_cls_;
+    bool tail_ready_ = false, tail_on_ = false;
+    cudaGraphExec_t tail_graph_ = nullptr;
+    int sms_ = 148;
     std::vector<TickRecord> records_;
     long ticks_ = 0;
     long launches_ = 0;
