@@ -195,7 +195,7 @@ struct WrapDev {
     float* pcg_u;                 // N x 6: u = M^-1 r, every node
     // reductions
     double* partials;             // energy_blocks x kPartialStride
-    double* edge_partials;        // edge blocks x 1 (smoothness energy)
+    double* edge_partials;        // edges: each edge's smoothness energy (the decision kernel sums them)
     double* node_partials;        // N: each node's anchor energy (the decision kernel sums them)
     int* counts;                  // stats scratch
     // report

@@ -344,7 +344,7 @@ size_t prepare_device(Wrap& w, WrapControl* control, cudaStream_t stream, bool p
     const size_t o_u = a.reserve(sizeof(float) * 6 * N);
     const int vblocks = (V + 255) / 256;
     const size_t o_part = a.reserve(sizeof(double) * kPartialStride * std::max(1, vblocks));
-    const size_t o_epart = a.reserve(sizeof(double) * std::max(1, (w.max_edges + 127) / 128));
+    const size_t o_epart = a.reserve(sizeof(double) * std::max(1, w.max_edges));
     const size_t o_npart = a.reserve(sizeof(double) * N);
     const size_t o_records = a.reserve(sizeof(LevelRecord) * w.levels);
     const size_t o_lstats = a.reserve(sizeof(CorrStats) * w.levels);

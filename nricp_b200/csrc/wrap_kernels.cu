@@ -1579,13 +1579,13 @@ __device__ __forceinline__ void k_edge_assemble_body(const WrapDev& w, int part,
             }
         }
     }
-    __shared__ double scratch[33];
-    const double total = block_sum<kEdgeThreads>(energy, scratch);
-    if (threadIdx.x == 0) w.edge_partials[bx] = total;
+    // the edge's smoothness energy; the decision kernel sums them as a block
+    // sum over this block would (no block barrier here)
+    if (e < L.edge_count) w.edge_partials[e] = energy;
 }
 
 __global__ void __launch_bounds__(kEdgeThreads) k_edge_assemble(const WrapDev* __restrict__ wraps, int wrap_count, int part) {
-    over_virtual_blocks<true>(
+    over_virtual_blocks<false>(
         wraps, wrap_count,
         [&](const WrapDev& w) {
             const WrapControl c = *w.control;
@@ -1622,7 +1622,26 @@ __global__ void k_decide(const WrapDev* __restrict__ wraps, int part) {
             s1 += w.partials[(long)i * kPartialStride + 1];
             s4 += w.partials[(long)i * kPartialStride + 2];
         }
-        for (int i = threadIdx.x; i < eb; i += blockDim.x) s2 += w.edge_partials[i];
+        for (int i = threadIdx.x; i < eb; i += blockDim.x) {
+            // edge block i's smoothness energy, summed in the order of a block
+            // sum over its 128 threads: a butterfly within each warp (lane l
+            // holds edge 128i + 32j + l, zero past the last edge), then the
+            // four warps' sums, ((w0 + w2) + (w1 + w3)); the zeros the other
+            // lanes add change nothing (energies are non-negative)
+            static_assert(kEdgeThreads == 4 * 32, "four warps per edge block");
+            double warp_total[4];
+            for (int j = 0; j < 4; ++j) {
+                double x[32];
+                for (int l = 0; l < 32; ++l) {
+                    const int e = i * kEdgeThreads + j * 32 + l;
+                    x[l] = e < L.edge_count ? w.edge_partials[e] : 0.0;
+                }
+                for (int o = 16; o > 0; o >>= 1)
+                    for (int l = 0; l < o; ++l) x[l] = x[l] + x[l + o];
+                warp_total[j] = x[0];
+            }
+            s2 += (warp_total[0] + warp_total[2]) + (warp_total[1] + warp_total[3]);
+        }
         for (int i = threadIdx.x; i < nb; i += blockDim.x) {
             // node block i's anchor energy, summed in the order of a block sum
             // over its 8 warps (lane 0 of warp j holds node 8i + j; the other
